@@ -1,0 +1,388 @@
+"""Benchmark: particle-steps/s of the openECLOUD per-step particle kernels.
+
+Workload (the kernel microbench configuration): 2^24 macro-electrons, uniform
+inside a 512x512-node rectangular grid of 40x40 mm, Maxwellian velocities
+(kT = 5 eV), uniform dipole B_y = 0.5 T (Boris type 1), E from a smooth
+charge density (sum of 16 Gaussians, sigma 1-4 mm, seed 7), dt = 1e-11 s.
+One step = gather E + Boris push + move + wall test + fixed-point deposit of
+the survivors: the work of calcGridWeights + eFieldToParticles + borisPush
++ indexInside + chargeToGrid in the reference loop.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun, one rank per GPU; every rank advances its own
+2^24 particles (independent shards, no collective on the data path:
+weak scaling).  Rank 0 prints one JSON line.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+QE = 1.602176565e-19
+ME = 9.10938291e-31
+EPS0 = 8.85418781762e-12
+METRIC = "particle-steps/s"
+
+
+# ------------------------------------------------------------- workload
+def workload(n, nodes=512, seed=7):
+    """Synthetic c2 inputs: particle rows (cell-sorted) and the node E field."""
+    rng = np.random.default_rng(seed)
+    lx = ly = 0.04
+    dx = lx / (nodes - 1.)
+    nx = nodes + 2
+    lxh = (lx + 2 * dx) * 0.5
+    pd = np.empty((n, 6), np.float64)
+    pd[:, 0] = rng.uniform(-lx / 2, lx / 2, n)
+    pd[:, 1] = rng.uniform(-ly / 2, ly / 2, n)
+    sv = np.sqrt(5.0 * QE / ME)  # Maxwellian, kT = 5 eV, per component
+    pd[:, 2:5] = rng.normal(0.0, sv, (n, 3))
+    pd[:, 5] = 1e9 / n
+    # cell-sorted order (the store keeps particles grouped by cell)
+    ix = np.floor((pd[:, 0] + lxh) / dx).astype(np.int64)
+    iy = np.floor((pd[:, 1] + lxh) / dx).astype(np.int64)
+    pd = pd[np.argsort(ix + iy * nx, kind="stable")]
+    # E of 16 Gaussian line-charge blobs (free-space closed form on the nodes)
+    xm = np.linspace(-lxh, lxh, nx)
+    X, Y = np.meshgrid(xm, xm)
+    Ex = np.zeros_like(X)
+    Ey = np.zeros_like(X)
+    for _ in range(16):
+        cx, cy = rng.uniform(-0.012, 0.012, 2)
+        s = rng.uniform(1e-3, 4e-3)
+        Q = rng.uniform(-1, 1) * 1e-9
+        rx, ry = X - cx, Y - cy
+        r2 = rx * rx + ry * ry + 1e-30
+        f = Q / (2 * np.pi * EPS0) * (1 - np.exp(-r2 / (2 * s * s))) / r2
+        Ex += f * rx
+        Ey += f * ry
+    E = np.concatenate([Ex.reshape(-1), Ey.reshape(-1)])
+    return pd, E, (nodes, nodes, lx, ly)
+
+
+# --------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if self.proc is None:
+            return out
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [l.strip().split(",") for l in self.f.read().splitlines() if l.strip()]
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for k, v in zip(names, r[5:9]):
+                    if v.strip().lower() in ("active", "1"):
+                        reasons.add(k)
+            except Exception:
+                continue
+        if sm:
+            out["sm_mhz"] = float(np.median(sm))
+            out["sm_max_mhz"] = float(np.max(mx))
+        out["reasons"] = sorted(reasons)
+        out["samples"] = len(sm)
+        return out
+
+
+# ----------------------------------------------------------- CPU legs
+def _ref_modules():
+    ref = os.path.join(ROOT, "oracle", "_ref")
+    if not os.path.exists(os.path.join(ref, "ref_compat.py")):
+        return None
+    sys.path.insert(0, ref)
+    try:
+        import ref_compat  # noqa: F401
+        import grid as rgrid
+        import particles as rparticles
+        import particleBoundary as rboundary
+        return rgrid, rparticles, rboundary
+    except Exception:
+        return None
+
+
+def cpu_reference_steps(n_sample, min_seconds, max_steps, min_steps=1):
+    """Time the compiled reference's own step (weights, deposit, gather, push,
+    wall test) on a bounded sample; falls back to the C oracle port."""
+    pd, E, (nx, ny, lx, ly) = workload(n_sample, seed=11)
+    mods = _ref_modules()
+    steps = 0
+    if mods is not None:
+        rgrid, rparticles, rboundary = mods
+        g = rgrid.Grid(nx, ny, lx, ly, 0)
+        P = rparticles.Particles("electrons", "variableWeight")
+        P.setParticleData(pd.copy())
+        P.setBConst(np.array([0.0, 0.5, 0.0]))
+        bd = rboundary.AbsorbRectangular(g, P)
+        kind = "reference"
+
+        def step():
+            P.calcGridWeights(g)
+            P.chargeToGrid(g)
+            P.eFieldToParticles(g, E)
+            P.borisPush(1e-11, 1)
+            bd.indexInside()
+    else:
+        from oracle import oracle as O
+        og = O.GridGeom(nx, ny, lx, ly)
+        state = {"pd": pd.copy()}
+        kind = "port"
+        qm = -QE / ME
+
+        def step():
+            p = state["pd"]
+            O.charge_to_grid(p, og, -QE)
+            e = O.field_to_particles(p, og, E, 2)
+            state["pd"] = O.boris_push(p, e, 1e-11, qm, 1, bconst=[0.0, 0.5, 0.0])
+            O.index_inside(state["pd"], og, 0)
+    step()  # warm caches
+    t0 = time.perf_counter()
+    while steps < min_steps or (time.perf_counter() - t0 < min_seconds and steps < max_steps):
+        step()
+        steps += 1
+    dt = time.perf_counter() - t0
+    return {"value": n_sample * steps / dt, "unit": METRIC, "cores": 1, "kind": kind,
+            "sample": f"{n_sample} particles x {steps} steps of the same workload (512x512 rect, B_y=0.5 T), "
+                      f"single thread ({dt:.1f} s)"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    n_sample = 1 << 22
+    t0 = time.perf_counter()
+    res = cpu_reference_steps(n_sample, min_seconds=0.0, max_steps=args.warmup, min_steps=max(1, args.warmup))
+    res = cpu_reference_steps(n_sample, min_seconds=0.0, max_steps=args.steps, min_steps=args.steps)
+    ms = n_sample / res["value"] * 1e3
+    line = {"metric": METRIC, "value": res["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "kernel microbench: 2^24 electrons (timed on a 2^22 sample), 512x512 rect "
+                                   "40x40 mm, B_y=0.5 T, weights+deposit+gather+Boris+wall test",
+                       "inputs_vs_L2": "sample 200 MB > L2"},
+            "impl": "reference", "cpu_baseline": {k: res[k] for k in ("kind", "cores", "sample", "value")},
+            "e2e": {"value": res["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": time.perf_counter() - t0}
+    print(json.dumps(line), flush=True)
+
+
+# -------------------------------------------------------------- GPU arm
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from openecloud_b200 import _lib
+    from openecloud_b200.grid import Grid
+    from openecloud_b200.particles import Particles
+    from openecloud_b200.particleBoundary import AbsorbRectangular
+
+    torch.cuda.set_device(local_rank)
+    n = args.particles
+    pd, E, (nx, ny, lx, ly) = workload(n, seed=7 + rank)
+    g = Grid(nx, ny, lx, ly, 0)
+    P = Particles("electrons", "variableWeight", capacity=n)
+    P.setParticleData(pd)
+    P.setBConst([0.0, 0.5, 0.0])
+    bd = AbsorbRectangular(g, P)
+    et = P.fieldTable(g, E, 2)
+    dt = 1e-11
+    P.pushGatherDeposit(g, et, dt, 1, bd)  # computes the fixed-point scale once
+    torch.cuda.synchronize()
+
+    cg, cp, cb = g.c_grid(), P.c_particles(), bd.c_boundary()
+    bconst = _lib.d3([0.0, 0.5, 0.0])
+    qm = P.particleCharge / P.particleMass
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    mask, rho, wsc, st = P._mask.data_ptr(), P._rho_fix.data_ptr(), P._wscale.data_ptr(), P._status.data_ptr()
+    L = _lib.lib()
+
+    def step():
+        rc = L.oec_push_gather(cg, cp, et.data_ptr(), None, bconst, dt, qm, 1, cb, mask, rho, wsc, st, sh)
+        if rc:
+            raise _lib.OecError("oec_push_gather", rc)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for k in range(args.steps):
+        ev[k][0].record(stream)
+        step()
+        ev[k][1].record(stream)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms_total = t_start.elapsed_time(t_end)
+    ms_kernel = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    ms_step = ms_total / args.steps
+    if world > 1:
+        t = torch.tensor([ms_step, ms_kernel], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step, ms_kernel = float(t[0]), float(t[1])
+    status = P.status()
+
+    # ---------------------------------------------- end to end (host buffers)
+    e2e = None
+    if args.e2e_steps > 0:
+        host = torch.from_numpy(pd).pin_memory()
+        out = torch.empty_like(host).pin_memory()
+        stage_rows = 1 << 20
+        staging = torch.empty((stage_rows, 6), dtype=torch.float64, device="cuda")
+        hp, op_, sp = host.data_ptr(), out.data_ptr(), staging.data_ptr()
+
+        def e2e_step():
+            rc = L.oec_particles_upload_host(cg, hp, n, cp, sp, stage_rows, sh)
+            if rc:
+                raise _lib.OecError("oec_particles_upload_host", rc)
+            step()
+            rc = L.oec_particles_download_host(cg, cp, op_, n, sp, stage_rows, sh)
+            if rc:
+                raise _lib.OecError("oec_particles_download_host", rc)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms_e2e = a.elapsed_time(b) / args.e2e_steps
+        if world > 1:
+            t = torch.tensor([ms_e2e], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_e2e = float(t[0])
+        e2e = {"value": n * world / (ms_e2e * 1e-3), "unit": METRIC, "h2d_bytes_per_step": int(n * 48),
+               "d2h_bytes_per_step": int(n * 48), "ms_per_step": ms_e2e,
+               "path": "oec_particles_upload_host -> oec_push_gather -> oec_particles_download_host, "
+                       "(N,6) f64 rows in pinned host memory"}
+
+    # ----------------------------------------------------------- roofline
+    G = (nx + 2) * (ny + 2)
+    bytes_particle = 28 + 24 + 1.0 / 8  # read cell,ox,oy,vx,vy,vz,w; write cell,ox,oy,vx,vy,vz; absorbed bit
+    bytes_grid = 8 * 4 * G + 8 * G + 8 * G  # E corner table read, rho clear + accumulate
+    alg_bytes = n * bytes_particle + bytes_grid
+    achieved = alg_bytes / (ms_kernel * 1e-3) / 1e9
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        try:
+            peak = float(json.load(open(peaks_path))["hbm_gbs"])
+            peak_src = "measured"
+        except Exception:
+            pass
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic_push_gather.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_steps(1 << 21, min_seconds=10.0, max_steps=200, min_steps=3)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": n * world / (ms_step * 1e-3), "unit": METRIC, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32+i64", "data": "synthetic",
+                "config": {"workload": "kernel microbench: 2^24 macro-electrons per GPU, 512x512 rect grid "
+                                       "40x40 mm, Maxwellian 5 eV, B_y=0.5 T, fused gather+Boris+move+wall "
+                                       "test+int64 deposit, dt=1e-11 s",
+                           "particles_per_gpu": n, "grid_nodes": [nx + 2, ny + 2],
+                           "parallelism": f"{world} independent particle shards",
+                           "l2": "inputs 470 MB per step > 126 MB L2 (no flush needed)"},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": traffic,
+                             "kernel": "k_push_gather<1,rect,deposit>", "kernel_ms": ms_kernel,
+                             "alg_bytes_per_launch": alg_bytes, "peak_source": peak_src},
+                "clocks": clk, "e2e": e2e, "gpu_launches": 1 * args.steps,
+                "status": {k: v for k, v in status.items() if v}}
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--particles", type=int, default=1 << 24)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

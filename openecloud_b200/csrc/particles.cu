@@ -1,0 +1,1021 @@
+// particles.cu -- particle store conversions, CIC weights, field gather,
+// Boris push and the fused gather+push+inside-test+deposit hot kernel.
+//
+// Reference: particles.pyx (openECLOUD).  Layout and precision choices:
+//  * particles are SoA FP32 with the position held as (cell index, in-cell
+//    offset); the offset keeps ~6e-8 cell resolution anywhere on the grid,
+//    where an absolute FP32 coordinate would keep only ~2e-5 cell on a
+//    512-cell grid;
+//  * field tables are cell-centric float4 corner quadruples so one gather is
+//    two (E) or three (B) 16-byte loads;
+//  * the deposit is an int64 fixed-point sum, so the grid is independent of
+//    particle order and the total charge is conserved exactly.
+#include <math.h>
+
+#include "oec_common.cuh"
+
+namespace oec {
+
+int sm_count() {
+    static int cached = 0;
+    if (cached == 0) {
+        int dev = 0, n = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 148;
+        cached = n > 0 ? n : 148;
+    }
+    return cached;
+}
+
+namespace {
+
+constexpr int kThreads = 256;           // threads per CTA
+constexpr int kPer = 4;                 // particles per thread (one float4)
+constexpr int kChunk = kThreads * kPer; // particles per CTA iteration
+constexpr float kBelowOne = 0x1.fffffep-1f;
+
+// ------------------------------------------------------------------ A1
+
+__global__ void k_from_aos(const double *__restrict__ aos, int64_t n, oec_particles_t p, int nx,
+                           int ny, double dxi, double dyi, double lxh, double lyh) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) *p.count = (int32_t)n;
+    if (i >= n) return;
+    const double *r = aos + 6 * i;
+    // particles.pyx:408-413: normalised coordinate, truncating cast, remainder.
+    double ux = (r[0] + lxh) * dxi;
+    double uy = (r[1] + lyh) * dyi;
+    double fx = floor(ux), fy = floor(uy);
+    int ix = (int)fmax(fmin(fx, (double)(nx - 2)), 0.0);
+    int iy = (int)fmax(fmin(fy, (double)(ny - 2)), 0.0);
+    float ox = (float)(ux - (double)ix);
+    float oy = (float)(uy - (double)iy);
+    ox = fminf(fmaxf(ox, 0.0f), kBelowOne);
+    oy = fminf(fmaxf(oy, 0.0f), kBelowOne);
+    p.cell[i] = ix + iy * nx;
+    p.ox[i] = ox;
+    p.oy[i] = oy;
+    p.vx[i] = (float)r[2];
+    p.vy[i] = (float)r[3];
+    p.vz[i] = (float)r[4];
+    p.w[i] = (float)r[5];
+}
+
+__global__ void k_to_aos(oec_particles_t p, double *__restrict__ aos, int64_t max_rows, int nx,
+                         float inv_nx, double dx, double dy, double lxh, double lyh) {
+    int64_t n = *p.count;
+    if (n > max_rows) n = max_rows;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        int ix, iy;
+        split_cell(p.cell[i], nx, inv_nx, ix, iy);
+        double *r = aos + 6 * i;
+        r[0] = abs_coord(ix, p.ox[i], dx, lxh);
+        r[1] = abs_coord(iy, p.oy[i], dy, lyh);
+        r[2] = (double)p.vx[i];
+        r[3] = (double)p.vy[i];
+        r[4] = (double)p.vz[i];
+        r[5] = (double)p.w[i];
+    }
+}
+
+// ------------------------------------------------------------------ A2
+
+__global__ void k_calc_weights(oec_particles_t p, uint32_t *__restrict__ in_cell,
+                               double *__restrict__ w00, double *__restrict__ w10,
+                               double *__restrict__ w01, double *__restrict__ w11) {
+    int64_t n = *p.count;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double fx = (double)p.ox[i], fy = (double)p.oy[i];
+        in_cell[i] = (uint32_t)p.cell[i];
+        w00[i] = (1.0 - fx) * (1.0 - fy);
+        w10[i] = fx * (1.0 - fy);
+        w01[i] = (1.0 - fx) * fy;
+        w11[i] = fx * fy;
+    }
+}
+
+// ---------------------------------------------------------- field tables
+
+__global__ void k_field_prepare(const double *__restrict__ f, int ncomp, int nx, int G,
+                                float4 *__restrict__ out) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < G; c += gridDim.x * blockDim.x) {
+        for (int k = 0; k < ncomp; ++k) {
+            const double *fk = f + (int64_t)k * G;
+            float4 q;
+            q.x = (float)fk[c];
+            q.y = (c + 1 < G) ? (float)fk[c + 1] : 0.0f;
+            q.z = (c + nx < G) ? (float)fk[c + nx] : 0.0f;
+            q.w = (c + nx + 1 < G) ? (float)fk[c + nx + 1] : 0.0f;
+            out[(int64_t)c * ncomp + k] = q;
+        }
+    }
+}
+
+__device__ __forceinline__ float corner_sum(float4 q, float w00, float w10, float w01, float w11) {
+    // particles.pyx:363-372 accumulation order.
+    float s = w00 * q.x;
+    s += w10 * q.y;
+    s += w01 * q.z;
+    s += w11 * q.w;
+    return s;
+}
+
+__global__ void k_gather(oec_particles_t p, const float4 *__restrict__ tab, int ncomp, int ncell,
+                         double *__restrict__ out) {
+    int64_t n = *p.count;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        int c = p.cell[i];
+        if ((unsigned)c >= (unsigned)ncell) {
+            for (int k = 0; k < ncomp; ++k) out[i * ncomp + k] = 0.0;
+            continue;
+        }
+        float fx = p.ox[i], fy = p.oy[i];
+        float w00 = (1.0f - fx) * (1.0f - fy), w10 = fx * (1.0f - fy);
+        float w01 = (1.0f - fx) * fy, w11 = fx * fy;
+        for (int k = 0; k < ncomp; ++k)
+            out[i * ncomp + k] = (double)corner_sum(__ldg(&tab[(int64_t)c * ncomp + k]), w00, w10, w01, w11);
+    }
+}
+
+// ------------------------------------------------------------- A5-A7
+
+struct PushConst {
+    int type_b;
+    float qm_dt;             // type 0: q/m*dt ; types 1,2: q/(2m)*dt
+    float t0, t1, t2;        // type 1 rotation vector
+    float s0, s1, s2;        // type 1: 2t/(1+t.t)
+    float dtdxi, dtdyi;      // dt/dx, dt/dy (cell units per m/s)
+};
+
+// One Boris step on (vx,vy,vz) with E (and B for type 2): particles.pyx:272-333.
+template <int TB>
+__device__ __forceinline__ void boris(const PushConst &k, float ex, float ey, float bx, float by,
+                                      float bz, float &vx, float &vy, float &vz) {
+    if (TB == 0) {
+        vx += k.qm_dt * ex;
+        vy += k.qm_dt * ey;
+    } else {
+        float t0, t1, t2, s0, s1, s2;
+        if (TB == 1) {
+            t0 = k.t0; t1 = k.t1; t2 = k.t2;
+            s0 = k.s0; s1 = k.s1; s2 = k.s2;
+        } else {
+            t0 = k.qm_dt * bx; t1 = k.qm_dt * by; t2 = k.qm_dt * bz;
+            float f = 2.0f / (1.0f + t0 * t0 + t1 * t1 + t2 * t2);
+            s0 = t0 * f; s1 = t1 * f; s2 = t2 * f;
+        }
+        float hx = k.qm_dt * ex, hy = k.qm_dt * ey;
+        vx += hx;
+        vy += hy;
+        float w0 = vx + vy * t2 - vz * t1;
+        float w1 = vy + vz * t0 - vx * t2;
+        float w2 = vz + vx * t1 - vy * t0;
+        vx += w1 * s2 - w2 * s1 + hx;
+        vy += w2 * s0 - w0 * s2 + hy;
+        vz += w0 * s1 - w1 * s0;
+    }
+}
+
+// ----------------------------------------------------- boundary geometry
+
+struct BoundaryConst {
+    int kind;
+    double rx, ry;           // rect: lx/2, ly/2
+    double ex, ey;           // ellipse: 4/lx^2, 4/ly^2
+    const uint16_t *faces;   // cut-cell
+    const double *bpts;
+    const int32_t *cpi;
+    float clip_lo;           // cut-cell clip, cell units (1e-6)
+};
+
+// Inside predicates of particleBoundary.pyx evaluated in FP64 with explicit
+// round-to-nearest operations (no FMA contraction) so that the decision is
+// bit-identical to the FP64 reference for the same stored position.
+__device__ __forceinline__ bool inside_rect(const BoundaryConst &b, double x, double y) {
+    // particleBoundary.pyx:92-97: outside if x<-lx/2 or x>lx/2 or y<-ly/2 or y>ly/2.
+    return !(x < -b.rx || x > b.rx || y < -b.ry || y > b.ry);
+}
+
+__device__ __forceinline__ bool inside_ellipse(const BoundaryConst &b, double x, double y) {
+    // particleBoundary.pyx:238-242: outside if x^2*4/lx^2 + y^2*4/ly^2 >= 1.
+    double r = __dadd_rn(__dmul_rn(__dmul_rn(x, x), b.ex), __dmul_rn(__dmul_rn(y, y), b.ey));
+    return !(r >= 1.0);
+}
+
+__device__ __forceinline__ bool inside_cutcell(const BoundaryConst &b, int cell, double x, double y) {
+    // particleBoundary.pyx:358-370.
+    unsigned f = b.faces[cell];
+    if (f == 8) return true;
+    if (f == 0) return false;
+    int i0 = b.cpi[2 * cell], i1 = b.cpi[2 * cell + 1];
+    if (i0 < 0 || i1 < 0) return false;
+    double a = __dmul_rn(__dsub_rn(b.bpts[2 * i0], x), __dsub_rn(b.bpts[2 * i1 + 1], y));
+    double c = __dmul_rn(__dsub_rn(b.bpts[2 * i1], x), __dsub_rn(b.bpts[2 * i0 + 1], y));
+    return a > c;
+}
+
+// ----------------------------------------------------------- deposit
+
+// Quantised corner charges of one particle; the four parts sum exactly to
+// llrint(w * wscale) so the deposited total is independent of splitting.
+__device__ __forceinline__ void corner_charges(float w, float fx, float fy, double wscale,
+                                               long long v[4]) {
+    long long q = llrint((double)w * wscale);
+    double qd = (double)q;
+    double gx = (double)fx, gy = (double)fy;
+    double hx = 1.0 - gx, hy = 1.0 - gy;
+    v[0] = llrint(qd * (hx * hy));   // LowXLowY  -> node c
+    v[1] = llrint(qd * (gx * hy));   // UpXLowY   -> node c+1
+    v[2] = llrint(qd * (hx * gy));   // LowXUpY   -> node c+nx
+    v[3] = q - v[0] - v[1] - v[2];   // UpXUpY    -> node c+nx+1
+}
+
+// Warp-cooperative deposit of one particle per lane (key < 0: nothing).
+__device__ __forceinline__ void deposit_warp(int key, long long v[4], unsigned long long *rho, int nx) {
+    if (!__any_sync(kFullMask, key >= 0)) return;
+    bool head = warp_segment_sum4(key, v);
+    if (head && key >= 0) {
+        atomicAdd(rho + key, (unsigned long long)v[0]);
+        atomicAdd(rho + key + 1, (unsigned long long)v[1]);
+        atomicAdd(rho + key + nx, (unsigned long long)v[2]);
+        atomicAdd(rho + key + nx + 1, (unsigned long long)v[3]);
+    }
+}
+
+// ------------------------------------------------------- fused kernel
+
+struct FusedArgs {
+    int32_t *cell;
+    float *ox, *oy, *vx, *vy, *vz;
+    const float *w;
+    const int32_t *count;
+    const float4 *etab;      // 2 float4 per cell
+    const float4 *btab;      // 3 float4 per cell (type 2)
+    PushConst k;
+    BoundaryConst b;
+    int nx, ny;
+    int ncell;               // cells with all four corners on the grid: G - nx - 1
+    float inv_nx;
+    double dx, dy, lxh, lyh;
+    uint32_t *mask;
+    unsigned long long *rho;
+    const double *wscale;
+    oec_status_t *status;
+    int64_t capacity;
+};
+
+template <int TB, int KIND, bool DEP>
+__global__ void __launch_bounds__(kThreads) k_push_gather(FusedArgs a) {
+    const int n = *a.count;
+    const int lane = threadIdx.x & 31;
+    const int nchunks = (n + kChunk - 1) / kChunk;
+    const double wscale = DEP ? *a.wscale : 0.0;
+    int absorbed_local = 0, nonfinite_local = 0, clipped_local = 0;
+
+    for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+        const int q = chunk * kThreads + threadIdx.x;  // float4 group index
+        const int base = q * kPer;
+        int4 c4 = reinterpret_cast<const int4 *>(a.cell)[q];
+        float4 fx4 = reinterpret_cast<const float4 *>(a.ox)[q];
+        float4 fy4 = reinterpret_cast<const float4 *>(a.oy)[q];
+        float4 vx4 = reinterpret_cast<const float4 *>(a.vx)[q];
+        float4 vy4 = reinterpret_cast<const float4 *>(a.vy)[q];
+        float4 vz4 = reinterpret_cast<const float4 *>(a.vz)[q];
+        float4 w4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (DEP) w4 = reinterpret_cast<const float4 *>(a.w)[q];
+
+        int cc[4] = {c4.x, c4.y, c4.z, c4.w};
+        float fx[4] = {fx4.x, fx4.y, fx4.z, fx4.w};
+        float fy[4] = {fy4.x, fy4.y, fy4.z, fy4.w};
+        float vx[4] = {vx4.x, vx4.y, vx4.z, vx4.w};
+        float vy[4] = {vy4.x, vy4.y, vy4.z, vy4.w};
+        float vz[4] = {vz4.x, vz4.y, vz4.z, vz4.w};
+        float ww[4] = {w4.x, w4.y, w4.z, w4.w};
+        unsigned nib = 0;
+        int key[4];
+
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            key[j] = -1;
+            if (base + j >= n) continue;
+            const int c = cc[j];
+            if ((unsigned)c >= (unsigned)a.ncell) {  // not a valid interpolation cell
+                nib |= 1u << j;
+                ++nonfinite_local;
+                continue;
+            }
+            // --- gather at the current position (particles.pyx:354-372)
+            float gx = fx[j], gy = fy[j];
+            float w00 = (1.0f - gx) * (1.0f - gy), w10 = gx * (1.0f - gy);
+            float w01 = (1.0f - gx) * gy, w11 = gx * gy;
+            float4 qx = __ldg(&a.etab[2 * c]);
+            float4 qy = __ldg(&a.etab[2 * c + 1]);
+            float ex = corner_sum(qx, w00, w10, w01, w11);
+            float ey = corner_sum(qy, w00, w10, w01, w11);
+            float bx = 0.f, by = 0.f, bz = 0.f;
+            if (TB == 2) {
+                bx = corner_sum(__ldg(&a.btab[3 * c]), w00, w10, w01, w11);
+                by = corner_sum(__ldg(&a.btab[3 * c + 1]), w00, w10, w01, w11);
+                bz = corner_sum(__ldg(&a.btab[3 * c + 2]), w00, w10, w01, w11);
+            }
+            // --- push
+            boris<TB>(a.k, ex, ey, bx, by, bz, vx[j], vy[j], vz[j]);
+            // --- move in cell units and carry whole cells into the index
+            float nxo = gx + a.k.dtdxi * vx[j];
+            float nyo = gy + a.k.dtdyi * vy[j];
+            int ix, iy;
+            split_cell(c, a.nx, a.inv_nx, ix, iy);
+            bool finite = isfinite(nxo) && isfinite(nyo);
+            bool out = false;
+            if (!finite) {
+                ++nonfinite_local;
+                out = true;
+            } else {
+                float sx = floorf(fminf(fmaxf(nxo, -1048576.f), 1048576.f));
+                float sy = floorf(fminf(fmaxf(nyo, -1048576.f), 1048576.f));
+                nxo -= sx;
+                nyo -= sy;
+                ix += (int)sx;
+                iy += (int)sy;
+                if (nxo >= 1.0f) { nxo = 0.0f; ix += 1; }
+                if (nyo >= 1.0f) { nyo = 0.0f; iy += 1; }
+                if (KIND == OEC_BOUNDARY_CUTCELL) {
+                    // _clipParticleDataToGrid (particleBoundary.pyx:485-508):
+                    // keep the point 1e-6 cells inside the extended grid.
+                    bool clip = false;
+                    if (ix < 0 || (ix == 0 && nxo < a.b.clip_lo)) { ix = 0; nxo = a.b.clip_lo; clip = true; }
+                    if (ix > a.nx - 2) { ix = a.nx - 2; nxo = 1.0f - a.b.clip_lo; clip = true; }
+                    if (ix == a.nx - 2 && nxo > 1.0f - a.b.clip_lo) { nxo = 1.0f - a.b.clip_lo; clip = true; }
+                    if (iy < 0 || (iy == 0 && nyo < a.b.clip_lo)) { iy = 0; nyo = a.b.clip_lo; clip = true; }
+                    if (iy > a.ny - 2) { iy = a.ny - 2; nyo = 1.0f - a.b.clip_lo; clip = true; }
+                    if (iy == a.ny - 2 && nyo > 1.0f - a.b.clip_lo) { nyo = 1.0f - a.b.clip_lo; clip = true; }
+                    clipped_local += clip ? 1 : 0;
+                } else {
+                    // Outside the extended grid means outside any rect/ellipse wall.
+                    out = (ix < 0 || iy < 0 || ix > a.nx - 2 || iy > a.ny - 2);
+                }
+                fx[j] = nxo;
+                fy[j] = nyo;
+                cc[j] = ix + iy * a.nx;
+                if (!out) {
+                    double x = abs_coord(ix, nxo, a.dx, a.lxh);
+                    double y = abs_coord(iy, nyo, a.dy, a.lyh);
+                    bool in;
+                    if (KIND == OEC_BOUNDARY_RECT)
+                        in = inside_rect(a.b, x, y);
+                    else if (KIND == OEC_BOUNDARY_ELLIPSE)
+                        in = inside_ellipse(a.b, x, y);
+                    else
+                        in = inside_cutcell(a.b, cc[j], x, y);
+                    out = !in;
+                }
+            }
+            if (out) {
+                nib |= 1u << j;
+            } else if (DEP) {
+                key[j] = cc[j];
+            }
+        }
+
+        // --- write back (invalid tail slots are rewritten unchanged)
+        reinterpret_cast<int4 *>(a.cell)[q] = make_int4(cc[0], cc[1], cc[2], cc[3]);
+        reinterpret_cast<float4 *>(a.ox)[q] = make_float4(fx[0], fx[1], fx[2], fx[3]);
+        reinterpret_cast<float4 *>(a.oy)[q] = make_float4(fy[0], fy[1], fy[2], fy[3]);
+        reinterpret_cast<float4 *>(a.vx)[q] = make_float4(vx[0], vx[1], vx[2], vx[3]);
+        reinterpret_cast<float4 *>(a.vy)[q] = make_float4(vy[0], vy[1], vy[2], vy[3]);
+        reinterpret_cast<float4 *>(a.vz)[q] = make_float4(vz[0], vz[1], vz[2], vz[3]);
+
+        // --- absorbed bits: 8 lanes x 4 particles = one 32-bit word
+        unsigned word = nib << (4 * (lane & 7));
+        word |= __shfl_xor_sync(kFullMask, word, 1);
+        word |= __shfl_xor_sync(kFullMask, word, 2);
+        word |= __shfl_xor_sync(kFullMask, word, 4);
+        if ((lane & 7) == 0) a.mask[q >> 3] = word;
+        absorbed_local += __popc(nib);
+
+        // --- deposit of the surviving particles at their new position
+        if (DEP) {
+#pragma unroll
+            for (int j = 0; j < kPer; ++j) {
+                long long v[4] = {0, 0, 0, 0};
+                if (key[j] >= 0) corner_charges(ww[j], fx[j], fy[j], wscale, v);
+                deposit_warp(key[j], v, a.rho, a.nx);
+            }
+        }
+    }
+    int s = __reduce_add_sync(kFullMask, absorbed_local);
+    if (lane == 0 && s) atomicAdd(&a.status->n_absorbed, s);
+    s = __reduce_add_sync(kFullMask, nonfinite_local);
+    if (lane == 0 && s) atomicAdd(&a.status->n_nonfinite, s);
+    if (KIND == OEC_BOUNDARY_CUTCELL) {
+        s = __reduce_add_sync(kFullMask, clipped_local);
+        if (lane == 0 && s) atomicAdd(&a.status->n_clipped, s);
+    }
+}
+
+// ------------------------------------------------------ standalone deposit
+
+__global__ void __launch_bounds__(kThreads)
+    k_deposit(const int32_t *__restrict__ cell, const float *__restrict__ ox,
+              const float *__restrict__ oy, const float *__restrict__ w, const int32_t *count, int nx,
+              int ncell, unsigned long long *rho, const double *wscale_p) {
+    const int n = *count;
+    const double wscale = *wscale_p;
+    const int nchunks = (n + kChunk - 1) / kChunk;
+    for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+        const int q = chunk * kThreads + threadIdx.x;
+        const int base = q * kPer;
+        int4 c4 = reinterpret_cast<const int4 *>(cell)[q];
+        float4 fx4 = reinterpret_cast<const float4 *>(ox)[q];
+        float4 fy4 = reinterpret_cast<const float4 *>(oy)[q];
+        float4 w4 = reinterpret_cast<const float4 *>(w)[q];
+        int cc[4] = {c4.x, c4.y, c4.z, c4.w};
+        float fx[4] = {fx4.x, fx4.y, fx4.z, fx4.w};
+        float fy[4] = {fy4.x, fy4.y, fy4.z, fy4.w};
+        float ww[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            long long v[4] = {0, 0, 0, 0};
+            int key = (base + j < n && (unsigned)cc[j] < (unsigned)ncell) ? cc[j] : -1;
+            if (key >= 0) corner_charges(ww[j], fx[j], fy[j], wscale, v);
+            deposit_warp(key, v, rho, nx);
+        }
+    }
+}
+
+__global__ void k_deposit_finalize(const long long *__restrict__ fix, int G, const double *wscale_p,
+                                   double charge, double *__restrict__ out) {
+    double f = charge / *wscale_p;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < G; i += gridDim.x * blockDim.x)
+        out[i] = (double)fix[i] * f;
+}
+
+// wscale = 2^(bits - ceil(log2 max|w|)): integer charge units of a particle
+// stay below 2^bits.  `bits` is fixed by the host from the capacity so that
+// no node can leave the int64 range even if every particle met in one node.
+// Pass 1: grid-wide max of |w| as float bits (monotone for |w| >= 0) into the
+// first word of the output; pass 2: the scale, in place.
+__global__ void k_wmax(const float *__restrict__ w, const int32_t *count, int *maxbits) {
+    int n = *count;
+    float m = 0.0f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        m = fmaxf(m, fabsf(w[i]));
+    for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(kFullMask, m, off));
+    if ((threadIdx.x & 31) == 0 && m > 0.0f) atomicMax(maxbits, __float_as_int(m));
+}
+
+__global__ void k_wscale(double *out, int bits) {
+    float m = __int_as_float(*reinterpret_cast<const int *>(out));
+    int e = 0;
+    if (m > 0.0f && isfinite(m)) frexp((double)m, &e);  // m = f*2^e, f in [0.5,1): ceil(log2 m) <= e
+    *out = ldexp(1.0, bits - e);
+}
+
+// ------------------------------------------------------- inside test only
+
+template <int KIND>
+__global__ void __launch_bounds__(kThreads) k_index_inside(FusedArgs a) {
+    const int n = *a.count;
+    const int lane = threadIdx.x & 31;
+    const int nchunks = (n + kChunk - 1) / kChunk;
+    int absorbed_local = 0, clipped_local = 0;
+    for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+        const int q = chunk * kThreads + threadIdx.x;
+        const int base = q * kPer;
+        int4 c4 = reinterpret_cast<const int4 *>(a.cell)[q];
+        float4 fx4 = reinterpret_cast<const float4 *>(a.ox)[q];
+        float4 fy4 = reinterpret_cast<const float4 *>(a.oy)[q];
+        int cc[4] = {c4.x, c4.y, c4.z, c4.w};
+        float fx[4] = {fx4.x, fx4.y, fx4.z, fx4.w};
+        float fy[4] = {fy4.x, fy4.y, fy4.z, fy4.w};
+        unsigned nib = 0;
+        bool changed = false;
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            if (base + j >= n) continue;
+            if ((unsigned)cc[j] >= (unsigned)a.ncell) {
+                nib |= 1u << j;
+                continue;
+            }
+            int ix, iy;
+            split_cell(cc[j], a.nx, a.inv_nx, ix, iy);
+            if (KIND == OEC_BOUNDARY_CUTCELL) {
+                float lo = a.b.clip_lo, hi = 1.0f - a.b.clip_lo;
+                bool clip = false;
+                if (ix == 0 && fx[j] < lo) { fx[j] = lo; clip = true; }
+                if (ix == a.nx - 2 && fx[j] > hi) { fx[j] = hi; clip = true; }
+                if (iy == 0 && fy[j] < lo) { fy[j] = lo; clip = true; }
+                if (iy == a.ny - 2 && fy[j] > hi) { fy[j] = hi; clip = true; }
+                clipped_local += clip ? 1 : 0;
+                changed |= clip;
+            }
+            double x = abs_coord(ix, fx[j], a.dx, a.lxh);
+            double y = abs_coord(iy, fy[j], a.dy, a.lyh);
+            bool in;
+            if (KIND == OEC_BOUNDARY_RECT)
+                in = inside_rect(a.b, x, y);
+            else if (KIND == OEC_BOUNDARY_ELLIPSE)
+                in = inside_ellipse(a.b, x, y);
+            else
+                in = inside_cutcell(a.b, cc[j], x, y);
+            if (!in) nib |= 1u << j;
+        }
+        if (KIND == OEC_BOUNDARY_CUTCELL && changed) {
+            reinterpret_cast<float4 *>(a.ox)[q] = make_float4(fx[0], fx[1], fx[2], fx[3]);
+            reinterpret_cast<float4 *>(a.oy)[q] = make_float4(fy[0], fy[1], fy[2], fy[3]);
+        }
+        unsigned word = nib << (4 * (lane & 7));
+        word |= __shfl_xor_sync(kFullMask, word, 1);
+        word |= __shfl_xor_sync(kFullMask, word, 2);
+        word |= __shfl_xor_sync(kFullMask, word, 4);
+        if ((lane & 7) == 0) a.mask[q >> 3] = word;
+        absorbed_local += __popc(nib);
+    }
+    int s = __reduce_add_sync(kFullMask, absorbed_local);
+    if (lane == 0 && s) atomicAdd(&a.status->n_absorbed, s);
+    if (KIND == OEC_BOUNDARY_CUTCELL) {
+        s = __reduce_add_sync(kFullMask, clipped_local);
+        if (lane == 0 && s) atomicAdd(&a.status->n_clipped, s);
+    }
+}
+
+}  // namespace
+}  // namespace oec
+
+using namespace oec;
+
+// =================================================================== C ABI
+
+static bool valid_particles(const oec_particles_t *p) {
+    return p && p->cell && p->ox && p->oy && p->vx && p->vy && p->vz && p->w && p->count &&
+           p->capacity > 0 && (p->capacity % kChunk) == 0;
+}
+
+static bool valid_grid(const oec_grid_t *g) {
+    return g && g->nx >= 3 && g->ny >= 3 && g->dx > 0 && g->dy > 0 &&
+           (int64_t)g->nx * g->ny < (1 << 23);
+}
+
+static int64_t cap_chunks(const oec_particles_t *p) { return p->capacity / kChunk; }
+
+static PushConst make_push_const(const GridConst &gc, const double bconst[3], double dt, double qm,
+                                 int type_b) {
+    PushConst k{};
+    k.type_b = type_b;
+    if (type_b == 0) {
+        k.qm_dt = (float)(qm * dt);
+    } else {
+        double h = 0.5 * qm * dt;
+        k.qm_dt = (float)h;
+        if (type_b == 1) {
+            double t0 = h * bconst[0], t1 = h * bconst[1], t2 = h * bconst[2];
+            double f = 2.0 / (1.0 + t0 * t0 + t1 * t1 + t2 * t2);
+            k.t0 = (float)t0; k.t1 = (float)t1; k.t2 = (float)t2;
+            k.s0 = (float)(t0 * f); k.s1 = (float)(t1 * f); k.s2 = (float)(t2 * f);
+        }
+    }
+    k.dtdxi = (float)(dt * gc.dxi);
+    k.dtdyi = (float)(dt * gc.dyi);
+    return k;
+}
+
+static int make_boundary_const(const oec_boundary_t *bd, const GridConst &gc, BoundaryConst &b) {
+    b = BoundaryConst{};
+    b.kind = bd ? bd->kind : OEC_BOUNDARY_RECT;
+    b.rx = gc.lx * 0.5;
+    b.ry = gc.ly * 0.5;
+    b.ex = 4.0 / (gc.lx * gc.lx);
+    b.ey = 4.0 / (gc.ly * gc.ly);
+    b.clip_lo = 1e-6f;
+    if (b.kind == OEC_BOUNDARY_CUTCELL) {
+        if (!bd->inside_faces_dev || !bd->boundary_points_dev || !bd->cut_cell_points_ind_dev)
+            return OEC_ERR_INVALID;
+        b.faces = bd->inside_faces_dev;
+        b.bpts = bd->boundary_points_dev;
+        b.cpi = bd->cut_cell_points_ind_dev;
+    } else if (b.kind != OEC_BOUNDARY_RECT && b.kind != OEC_BOUNDARY_ELLIPSE) {
+        return OEC_ERR_INVALID;
+    }
+    return OEC_OK;
+}
+
+extern "C" int oec_particles_from_aos(const oec_grid_t *grid, const double *aos_dev, int64_t n,
+                                      oec_particles_t *p, void *stream) {
+    if (!valid_grid(grid) || !valid_particles(p) || n < 0 || (n > 0 && !aos_dev)) return OEC_ERR_INVALID;
+    if (n > p->capacity) return OEC_ERR_CAPACITY;
+    GridConst gc = make_grid_const(*grid);
+    int64_t blocks = (n + 255) / 256;
+    if (blocks < 1) blocks = 1;
+    k_from_aos<<<(unsigned)blocks, 256, 0, as_stream(stream)>>>(aos_dev, n, *p, gc.nx, gc.ny, gc.dxi,
+                                                                gc.dyi, gc.lxh, gc.lyh);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int oec_particles_to_aos(const oec_grid_t *grid, const oec_particles_t *p, double *aos_dev,
+                                    int64_t max_rows, void *stream) {
+    if (!valid_grid(grid) || !valid_particles(p) || !aos_dev || max_rows < 0) return OEC_ERR_INVALID;
+    GridConst gc = make_grid_const(*grid);
+    k_to_aos<<<persistent_grid((max_rows + 255) / 256, 8), 256, 0, as_stream(stream)>>>(
+        *p, aos_dev, max_rows, gc.nx, 1.0f / (float)gc.nx, gc.dx, gc.dy, gc.lxh, gc.lyh);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int oec_calc_grid_weights(const oec_grid_t *grid, const oec_particles_t *p,
+                                     uint32_t *in_cell_dev, double *w00_dev, double *w10_dev,
+                                     double *w01_dev, double *w11_dev, void *stream) {
+    if (!valid_grid(grid) || !valid_particles(p) || !in_cell_dev || !w00_dev || !w10_dev || !w01_dev ||
+        !w11_dev)
+        return OEC_ERR_INVALID;
+    k_calc_weights<<<persistent_grid(cap_chunks(p) * 4, 8), 256, 0, as_stream(stream)>>>(
+        *p, in_cell_dev, w00_dev, w10_dev, w01_dev, w11_dev);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int oec_field_prepare(const oec_grid_t *grid, const double *node_field_dev, int32_t ncomp,
+                                 float *cell_field_dev, void *stream) {
+    if (!valid_grid(grid) || !node_field_dev || !cell_field_dev || (ncomp != 2 && ncomp != 3))
+        return OEC_ERR_INVALID;
+    if (((uintptr_t)cell_field_dev & 15u) != 0) return OEC_ERR_INVALID;
+    int G = grid->nx * grid->ny;
+    k_field_prepare<<<persistent_grid((G + 255) / 256, 8), 256, 0, as_stream(stream)>>>(
+        node_field_dev, ncomp, grid->nx, G, reinterpret_cast<float4 *>(cell_field_dev));
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int oec_gather(const oec_grid_t *grid, const oec_particles_t *p, const float *cell_field_dev,
+                          int32_t ncomp, double *out_dev, void *stream) {
+    if (!valid_grid(grid) || !valid_particles(p) || !cell_field_dev || !out_dev ||
+        (ncomp != 2 && ncomp != 3))
+        return OEC_ERR_INVALID;
+    k_gather<<<persistent_grid(cap_chunks(p) * 4, 8), 256, 0, as_stream(stream)>>>(
+        *p, reinterpret_cast<const float4 *>(cell_field_dev), ncomp, grid->nx * grid->ny - grid->nx - 1,
+        out_dev);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+namespace oec {
+namespace {
+// Standalone push (API path): velocity update then move with carry.
+__global__ void k_boris_push_move(oec_particles_t p, const double *__restrict__ e_at,
+                                  const double *__restrict__ b_at, PushConst k, int nx) {
+    int64_t n = *p.count;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        float vx = p.vx[i], vy = p.vy[i], vz = p.vz[i];
+        float ex = (float)e_at[2 * i], ey = (float)e_at[2 * i + 1];
+        if (k.type_b == 0)
+            boris<0>(k, ex, ey, 0.f, 0.f, 0.f, vx, vy, vz);
+        else if (k.type_b == 1)
+            boris<1>(k, ex, ey, 0.f, 0.f, 0.f, vx, vy, vz);
+        else
+            boris<2>(k, ex, ey, (float)b_at[3 * i], (float)b_at[3 * i + 1], (float)b_at[3 * i + 2], vx,
+                     vy, vz);
+        p.vx[i] = vx;
+        p.vy[i] = vy;
+        p.vz[i] = vz;
+        float ox = p.ox[i] + k.dtdxi * vx;
+        float oy = p.oy[i] + k.dtdyi * vy;
+        if (!(isfinite(ox) && isfinite(oy))) continue;  // left for the inside test to absorb
+        float fx = floorf(fminf(fmaxf(ox, -1048576.f), 1048576.f));
+        float fy = floorf(fminf(fmaxf(oy, -1048576.f), 1048576.f));
+        ox -= fx;
+        oy -= fy;
+        int cx = (int)fx, cy = (int)fy;
+        if (ox >= 1.0f) { ox = 0.0f; cx += 1; }
+        if (oy >= 1.0f) { oy = 0.0f; cy += 1; }
+        p.ox[i] = ox;
+        p.oy[i] = oy;
+        p.cell[i] += cx + cy * nx;
+    }
+}
+}  // namespace
+}  // namespace oec
+
+extern "C" int oec_boris_push(const oec_grid_t *grid, oec_particles_t *p, const double *e_at_particles_dev,
+                              const double *b_at_particles_dev, const double bconst[3], double dt,
+                              double charge_over_mass, int32_t type_b_field, void *stream) {
+    if (!valid_grid(grid) || !valid_particles(p) || !e_at_particles_dev) return OEC_ERR_INVALID;
+    if (type_b_field < 0 || type_b_field > 2) return OEC_ERR_INVALID;
+    if (type_b_field == 1 && !bconst) return OEC_ERR_INVALID;
+    if (type_b_field == 2 && !b_at_particles_dev) return OEC_ERR_INVALID;
+    GridConst gc = make_grid_const(*grid);
+    double zero[3] = {0, 0, 0};
+    PushConst k = make_push_const(gc, bconst ? bconst : zero, dt, charge_over_mass, type_b_field);
+    k_boris_push_move<<<persistent_grid(cap_chunks(p) * 4, 8), 256, 0, as_stream(stream)>>>(
+        *p, e_at_particles_dev, b_at_particles_dev, k, gc.nx);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+static int deposit_bits(const oec_particles_t *p) {
+    // A node sums at most `capacity` particles of at most 2^bits units:
+    // capacity * 2^bits <= 2^62 keeps every node inside int64.
+    int lc = 0;
+    while ((int64_t(1) << lc) < p->capacity) ++lc;
+    int bits = 62 - lc;
+    return bits > 40 ? 40 : bits;
+}
+
+extern "C" int oec_deposit_scale(const oec_particles_t *p, double *wscale_dev, void *stream) {
+    if (!valid_particles(p) || !wscale_dev) return OEC_ERR_INVALID;
+    cudaStream_t s = as_stream(stream);
+    OEC_CUDA_TRY(cudaMemsetAsync(wscale_dev, 0, sizeof(double), s));
+    k_wmax<<<persistent_grid(cap_chunks(p), 4), kThreads, 0, s>>>(p->w, p->count,
+                                                                   reinterpret_cast<int *>(wscale_dev));
+    OEC_LAUNCH_CHECK();
+    k_wscale<<<1, 1, 0, s>>>(wscale_dev, deposit_bits(p));
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+template <int TB, int KIND, bool DEP>
+static void launch_fused(const FusedArgs &a, int grid_unused, cudaStream_t s) {
+    (void)grid_unused;
+    static int per_sm = 0;  // resident CTAs per SM for this instantiation
+    if (per_sm == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_push_gather<TB, KIND, DEP>, kThreads, 0) !=
+                cudaSuccess ||
+            per_sm < 1)
+            per_sm = 1;
+    }
+    int64_t chunks = ((int64_t)a.capacity + kChunk - 1) / kChunk;
+    k_push_gather<TB, KIND, DEP><<<persistent_grid(chunks, per_sm), kThreads, 0, s>>>(a);
+}
+
+template <int TB, int KIND>
+static void launch_fused_dep(const FusedArgs &a, bool dep, int grid, cudaStream_t s) {
+    if (dep)
+        launch_fused<TB, KIND, true>(a, grid, s);
+    else
+        launch_fused<TB, KIND, false>(a, grid, s);
+}
+
+template <int TB>
+static void launch_fused_kind(const FusedArgs &a, int kind, bool dep, int grid, cudaStream_t s) {
+    if (kind == OEC_BOUNDARY_RECT)
+        launch_fused_dep<TB, OEC_BOUNDARY_RECT>(a, dep, grid, s);
+    else if (kind == OEC_BOUNDARY_ELLIPSE)
+        launch_fused_dep<TB, OEC_BOUNDARY_ELLIPSE>(a, dep, grid, s);
+    else
+        launch_fused_dep<TB, OEC_BOUNDARY_CUTCELL>(a, dep, grid, s);
+}
+
+static FusedArgs make_fused_args(const GridConst &gc, oec_particles_t *p) {
+    FusedArgs a{};
+    a.cell = p->cell;
+    a.ox = p->ox;
+    a.oy = p->oy;
+    a.vx = p->vx;
+    a.vy = p->vy;
+    a.vz = p->vz;
+    a.w = p->w;
+    a.count = p->count;
+    a.capacity = p->capacity;
+    a.nx = gc.nx;
+    a.ny = gc.ny;
+    a.ncell = gc.G - gc.nx - 1;
+    a.inv_nx = 1.0f / (float)gc.nx;
+    a.dx = gc.dx;
+    a.dy = gc.dy;
+    a.lxh = gc.lxh;
+    a.lyh = gc.lyh;
+    return a;
+}
+
+extern "C" int oec_push_gather(const oec_grid_t *grid, oec_particles_t *p, const float *e_cell_dev,
+                               const float *b_cell_dev, const double bconst[3], double dt,
+                               double charge_over_mass, int32_t type_b_field,
+                               const oec_boundary_t *boundary, uint32_t *absorbed_mask_dev,
+                               int64_t *rho_fix_dev, const double *wscale_dev,
+                               oec_status_t *status_dev, void *stream) {
+    if (!valid_grid(grid) || !valid_particles(p) || !e_cell_dev || !absorbed_mask_dev || !status_dev)
+        return OEC_ERR_INVALID;
+    if (type_b_field < 0 || type_b_field > 2) return OEC_ERR_INVALID;
+    if (type_b_field == 1 && !bconst) return OEC_ERR_INVALID;
+    if (type_b_field == 2 && !b_cell_dev) return OEC_ERR_INVALID;
+    if (rho_fix_dev && !wscale_dev) return OEC_ERR_INVALID;
+    GridConst gc = make_grid_const(*grid);
+    double zero[3] = {0, 0, 0};
+    FusedArgs a = make_fused_args(gc, p);
+    a.k = make_push_const(gc, bconst ? bconst : zero, dt, charge_over_mass, type_b_field);
+    int rc = make_boundary_const(boundary, gc, a.b);
+    if (rc != OEC_OK) return rc;
+    a.etab = reinterpret_cast<const float4 *>(e_cell_dev);
+    a.btab = reinterpret_cast<const float4 *>(b_cell_dev);
+    a.mask = absorbed_mask_dev;
+    a.rho = reinterpret_cast<unsigned long long *>(rho_fix_dev);
+    a.wscale = wscale_dev;
+    a.status = status_dev;
+    cudaStream_t s = as_stream(stream);
+    OEC_CUDA_TRY(cudaMemsetAsync(&status_dev->n_absorbed, 0, sizeof(int32_t), s));
+    if (rho_fix_dev)
+        OEC_CUDA_TRY(cudaMemsetAsync(rho_fix_dev, 0, sizeof(int64_t) * (size_t)gc.G, s));
+    int g = persistent_grid(cap_chunks(p), 8);
+    bool dep = rho_fix_dev != nullptr;
+    if (type_b_field == 0)
+        launch_fused_kind<0>(a, a.b.kind, dep, g, s);
+    else if (type_b_field == 1)
+        launch_fused_kind<1>(a, a.b.kind, dep, g, s);
+    else
+        launch_fused_kind<2>(a, a.b.kind, dep, g, s);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int oec_deposit(const oec_grid_t *grid, const oec_particles_t *p, int64_t *rho_fix_dev,
+                           const double *wscale_dev, int32_t zero_first, oec_status_t *status_dev,
+                           void *stream) {
+    (void)status_dev;
+    if (!valid_grid(grid) || !valid_particles(p) || !rho_fix_dev || !wscale_dev) return OEC_ERR_INVALID;
+    cudaStream_t s = as_stream(stream);
+    int G = grid->nx * grid->ny;
+    if (zero_first) OEC_CUDA_TRY(cudaMemsetAsync(rho_fix_dev, 0, sizeof(int64_t) * (size_t)G, s));
+    k_deposit<<<persistent_grid(cap_chunks(p), 8), kThreads, 0, s>>>(
+        p->cell, p->ox, p->oy, p->w, p->count, grid->nx, G - grid->nx - 1,
+        reinterpret_cast<unsigned long long *>(rho_fix_dev),
+        wscale_dev);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int oec_deposit_finalize(const oec_grid_t *grid, const int64_t *rho_fix_dev,
+                                    const double *wscale_dev, double particle_charge, double *rho_dev,
+                                    void *stream) {
+    if (!valid_grid(grid) || !rho_fix_dev || !wscale_dev || !rho_dev) return OEC_ERR_INVALID;
+    int G = grid->nx * grid->ny;
+    k_deposit_finalize<<<persistent_grid((G + 255) / 256, 8), 256, 0, as_stream(stream)>>>(
+        reinterpret_cast<const long long *>(rho_fix_dev), G, wscale_dev, particle_charge, rho_dev);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int oec_index_inside(const oec_grid_t *grid, oec_particles_t *p, const oec_boundary_t *boundary,
+                                uint32_t *absorbed_mask_dev, oec_status_t *status_dev, void *stream) {
+    if (!valid_grid(grid) || !valid_particles(p) || !absorbed_mask_dev || !status_dev || !boundary)
+        return OEC_ERR_INVALID;
+    GridConst gc = make_grid_const(*grid);
+    FusedArgs a = make_fused_args(gc, p);
+    int rc = make_boundary_const(boundary, gc, a.b);
+    if (rc != OEC_OK) return rc;
+    a.mask = absorbed_mask_dev;
+    a.status = status_dev;
+    cudaStream_t s = as_stream(stream);
+    OEC_CUDA_TRY(cudaMemsetAsync(&status_dev->n_absorbed, 0, sizeof(int32_t), s));
+    int g = persistent_grid(cap_chunks(p), 8);
+    if (a.b.kind == OEC_BOUNDARY_RECT)
+        k_index_inside<OEC_BOUNDARY_RECT><<<g, kThreads, 0, s>>>(a);
+    else if (a.b.kind == OEC_BOUNDARY_ELLIPSE)
+        k_index_inside<OEC_BOUNDARY_ELLIPSE><<<g, kThreads, 0, s>>>(a);
+    else
+        k_index_inside<OEC_BOUNDARY_CUTCELL><<<g, kThreads, 0, s>>>(a);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+// ============================================ host round trip (end-to-end)
+
+namespace oec {
+namespace {
+
+__global__ void k_from_aos_rows(const double *__restrict__ aos, int64_t row0, int64_t rows, oec_particles_t p,
+                                int nx, int ny, double dxi, double dyi, double lxh, double lyh) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= rows) return;
+    int64_t i = row0 + k;
+    const double *r = aos + 6 * k;
+    double ux = (r[0] + lxh) * dxi;
+    double uy = (r[1] + lyh) * dyi;
+    int ix = (int)fmax(fmin(floor(ux), (double)(nx - 2)), 0.0);
+    int iy = (int)fmax(fmin(floor(uy), (double)(ny - 2)), 0.0);
+    float ox = fminf(fmaxf((float)(ux - (double)ix), 0.0f), kBelowOne);
+    float oy = fminf(fmaxf((float)(uy - (double)iy), 0.0f), kBelowOne);
+    p.cell[i] = ix + iy * nx;
+    p.ox[i] = ox;
+    p.oy[i] = oy;
+    p.vx[i] = (float)r[2];
+    p.vy[i] = (float)r[3];
+    p.vz[i] = (float)r[4];
+    p.w[i] = (float)r[5];
+}
+
+__global__ void k_to_aos_rows(oec_particles_t p, int64_t row0, int64_t rows, double *__restrict__ aos, int nx,
+                              float inv_nx, double dx, double dy, double lxh, double lyh) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= rows) return;
+    int64_t i = row0 + k;
+    int ix, iy;
+    split_cell(p.cell[i], nx, inv_nx, ix, iy);
+    double *r = aos + 6 * k;
+    r[0] = abs_coord(ix, p.ox[i], dx, lxh);
+    r[1] = abs_coord(iy, p.oy[i], dy, lyh);
+    r[2] = (double)p.vx[i];
+    r[3] = (double)p.vy[i];
+    r[4] = (double)p.vz[i];
+    r[5] = (double)p.w[i];
+}
+
+// Two-slot pipeline: the copy of chunk k+1 overlaps the conversion of chunk k.
+struct Pipe {
+    cudaStream_t copy = nullptr;
+    cudaEvent_t copied[2] = {nullptr, nullptr};
+    cudaEvent_t used[2] = {nullptr, nullptr};
+    bool ready = false;
+    int init() {
+        if (ready) return OEC_OK;
+        OEC_CUDA_TRY(cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking));
+        for (int s = 0; s < 2; ++s) {
+            OEC_CUDA_TRY(cudaEventCreateWithFlags(&copied[s], cudaEventDisableTiming));
+            OEC_CUDA_TRY(cudaEventCreateWithFlags(&used[s], cudaEventDisableTiming));
+        }
+        ready = true;
+        return OEC_OK;
+    }
+};
+
+Pipe &pipe() {
+    static Pipe p;
+    return p;
+}
+
+}  // namespace
+}  // namespace oec
+
+extern "C" int oec_particles_upload_host(const oec_grid_t *grid, const double *aos_host, int64_t n,
+                                         oec_particles_t *p, double *staging_dev, int64_t staging_rows,
+                                         void *stream) {
+    if (!valid_grid(grid) || !valid_particles(p) || n < 0 || (n > 0 && (!aos_host || !staging_dev)) ||
+        staging_rows < 2)
+        return OEC_ERR_INVALID;
+    if (n > p->capacity) return OEC_ERR_CAPACITY;
+    Pipe &pp = pipe();
+    int rc = pp.init();
+    if (rc != OEC_OK) return rc;
+    cudaStream_t s = as_stream(stream);
+    GridConst gc = make_grid_const(*grid);
+    int64_t half = staging_rows / 2;
+    // the copy stream must not run ahead of work already queued on `s`
+    OEC_CUDA_TRY(cudaEventRecord(pp.used[0], s));
+    OEC_CUDA_TRY(cudaEventRecord(pp.used[1], s));
+    int k = 0;
+    for (int64_t row0 = 0; row0 < n; row0 += half, ++k) {
+        int slot = k & 1;
+        int64_t rows = (n - row0 < half) ? (n - row0) : half;
+        double *buf = staging_dev + 6 * half * slot;
+        OEC_CUDA_TRY(cudaStreamWaitEvent(pp.copy, pp.used[slot], 0));
+        OEC_CUDA_TRY(cudaMemcpyAsync(buf, aos_host + 6 * row0, sizeof(double) * 6 * rows, cudaMemcpyHostToDevice,
+                                     pp.copy));
+        OEC_CUDA_TRY(cudaEventRecord(pp.copied[slot], pp.copy));
+        OEC_CUDA_TRY(cudaStreamWaitEvent(s, pp.copied[slot], 0));
+        k_from_aos_rows<<<(unsigned)((rows + 255) / 256), 256, 0, s>>>(buf, row0, rows, *p, gc.nx, gc.ny, gc.dxi,
+                                                                       gc.dyi, gc.lxh, gc.lyh);
+        OEC_LAUNCH_CHECK();
+        OEC_CUDA_TRY(cudaEventRecord(pp.used[slot], s));
+    }
+    int32_t cnt = (int32_t)n;
+    OEC_CUDA_TRY(cudaMemcpyAsync(p->count, &cnt, sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    OEC_CUDA_TRY(cudaStreamSynchronize(s));  // `cnt` lives on this stack frame
+    return OEC_OK;
+}
+
+extern "C" int oec_particles_download_host(const oec_grid_t *grid, const oec_particles_t *p, double *aos_host,
+                                           int64_t n, double *staging_dev, int64_t staging_rows, void *stream) {
+    if (!valid_grid(grid) || !valid_particles(p) || n < 0 || (n > 0 && (!aos_host || !staging_dev)) ||
+        staging_rows < 2 || n > p->capacity)
+        return OEC_ERR_INVALID;
+    Pipe &pp = pipe();
+    int rc = pp.init();
+    if (rc != OEC_OK) return rc;
+    cudaStream_t s = as_stream(stream);
+    GridConst gc = make_grid_const(*grid);
+    int64_t half = staging_rows / 2;
+    OEC_CUDA_TRY(cudaEventRecord(pp.used[0], pp.copy));
+    OEC_CUDA_TRY(cudaEventRecord(pp.used[1], pp.copy));
+    int k = 0;
+    for (int64_t row0 = 0; row0 < n; row0 += half, ++k) {
+        int slot = k & 1;
+        int64_t rows = (n - row0 < half) ? (n - row0) : half;
+        double *buf = staging_dev + 6 * half * slot;
+        OEC_CUDA_TRY(cudaStreamWaitEvent(s, pp.used[slot], 0));  // previous copy out of this slot finished
+        k_to_aos_rows<<<(unsigned)((rows + 255) / 256), 256, 0, s>>>(*p, row0, rows, buf, gc.nx,
+                                                                     1.0f / (float)gc.nx, gc.dx, gc.dy, gc.lxh,
+                                                                     gc.lyh);
+        OEC_LAUNCH_CHECK();
+        OEC_CUDA_TRY(cudaEventRecord(pp.copied[slot], s));
+        OEC_CUDA_TRY(cudaStreamWaitEvent(pp.copy, pp.copied[slot], 0));
+        OEC_CUDA_TRY(cudaMemcpyAsync(aos_host + 6 * row0, buf, sizeof(double) * 6 * rows, cudaMemcpyDeviceToHost,
+                                     pp.copy));
+        OEC_CUDA_TRY(cudaEventRecord(pp.used[slot], pp.copy));
+    }
+    // make `stream` wait for the last host copies so its users see the data
+    OEC_CUDA_TRY(cudaEventRecord(pp.copied[0], pp.copy));
+    OEC_CUDA_TRY(cudaStreamWaitEvent(s, pp.copied[0], 0));
+    return OEC_OK;
+}

@@ -1,0 +1,186 @@
+"""Generate golden fixtures by running the compiled openECLOUD reference.
+
+Requires the reference modules built by ``python oracle/build_ref.py`` into
+``oracle/_ref`` (which needs the reference source tree; it exists only where
+the fixtures are generated).  Writes small ``.npz`` files next to this script;
+the fixtures are committed, the reference is not.
+
+Every array is produced by calling the reference's own public methods on
+seeded inputs; the seeds and shapes are recorded in each file.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REF = os.path.join(REPO, "oracle", "_ref")
+
+
+def _import_reference():
+    if not os.path.isdir(REF):
+        raise SystemExit("oracle/_ref missing: run python oracle/build_ref.py first")
+    sys.path.insert(0, REF)
+    import ref_compat  # noqa: F401  (scipy aliases used by beam.py)
+    import grid, particles, particleBoundary, poissonSolver, randomGen  # noqa: E401
+    return grid, particles, particleBoundary, poissonSolver, randomGen
+
+
+GRIDS = {
+    # name: (nx, ny, lx, ly, boundType)
+    "rect_24x20": (24, 20, 0.03, 0.02, 0),
+    "circle_32": (32, 32, 0.04, 0.04, 1),
+    "ellipse_40x24": (40, 24, 0.09, 0.036, 1),
+    "circle_128": (128, 128, 0.04, 0.04, 1),
+}
+
+
+def grid_arrays(g):
+    out = {}
+    for name in ["XMesh", "YMesh", "Ds", "Dst"]:
+        out[name] = np.asarray(getattr(g, "get" + name)())
+    out["Dsi"] = np.asarray(g.getDsi())
+    out["Da"] = np.asarray(g.getDa())
+    out["Dai"] = np.asarray(g.getDai())
+    out["Dat"] = np.asarray(g.getDat())
+    out["Dati"] = np.asarray(g.getDati())
+    out["insidePoints"] = np.asarray(g.getInsidePoints())
+    out["insideEdges"] = np.asarray(g.getInsideEdges())
+    out["insideFaces"] = np.asarray(g.getInsideFaces())
+    e2n = g.getEdgeToNode().tocsr()
+    e2n.sort_indices()
+    out["e2n_indptr"], out["e2n_indices"], out["e2n_data"] = e2n.indptr, e2n.indices, e2n.data
+    for name in ["BoundaryPoints", "BoundaryPointsInd", "CutCellPointsInd", "CutCellNormalVectors",
+                 "CutCellCenter"]:
+        try:
+            out[name[0].lower() + name[1:]] = np.asarray(getattr(g, "get" + name)())
+        except Exception:
+            pass
+    return out
+
+
+def random_inside(rng, n, lx, ly, kind):
+    pts = []
+    while sum(len(p) for p in pts) < n:
+        x = (rng.random(4 * n) - 0.5) * lx
+        y = (rng.random(4 * n) - 0.5) * ly
+        if kind == 1:
+            ok = x * x * 4 / lx ** 2 + y * y * 4 / ly ** 2 < 0.999
+        else:
+            ok = np.ones_like(x, bool)
+        pts.append(np.stack([x[ok], y[ok]], 1))
+    return np.concatenate(pts)[:n]
+
+
+def make_particles(rng, n, lx, ly, kind, vscale):
+    xy = random_inside(rng, n, lx, ly, kind)
+    pd = np.empty((n, 6))
+    pd[:, :2] = xy
+    pd[:, 2:5] = rng.normal(0.0, vscale, (n, 3))
+    pd[:, 5] = rng.uniform(0.5, 1.5, n) * 1e5
+    return pd
+
+
+def main():
+    grid, particles, particleBoundary, poissonSolver, randomGen = _import_reference()
+    rng = np.random.default_rng(20240611)
+    for gname, (nx, ny, lx, ly, bt) in GRIDS.items():
+        g = grid.Grid(nx, ny, lx, ly, bt)
+        arrays = grid_arrays(g)
+        arrays["params"] = np.array([nx, ny, lx, ly, bt], np.float64)
+        # Poisson: random smooth charge, reference solve.
+        ps = poissonSolver.PoissonSolver(g)
+        xm, ym = arrays["XMesh"], arrays["YMesh"]
+        X, Y = np.meshgrid(xm, ym)
+        q = np.zeros_like(X)
+        for _ in range(4):
+            cx, cy = rng.uniform(-0.3, 0.3) * lx, rng.uniform(-0.3, 0.3) * ly
+            s = rng.uniform(0.05, 0.15) * min(lx, ly)
+            q += rng.uniform(-1, 1) * 1e-9 * np.exp(-((X - cx) ** 2 + (Y - cy) ** 2) / (2 * s * s))
+        q = q.reshape(-1)
+        E = np.asarray(ps.solve(q)).copy()
+        arrays["poisson_q"] = q
+        arrays["poisson_phi"] = np.asarray(ps.getPhi()).copy()
+        arrays["poisson_E"] = E
+        # Particle kernels on this grid.
+        if gname != "circle_128":
+            n = 600
+            pd = make_particles(rng, n, lx, ly, bt, 2e6)
+            P = particles.Particles("electrons", "variableWeight")
+            P.setParticleData(pd.copy())
+            P.calcGridWeights(g)
+            arrays["pd_in"] = pd
+            arrays["inCell"] = np.asarray(P.getInCell()).copy()
+            arrays["w00"] = np.asarray(P.getWeightLowXLowY()).copy()
+            arrays["w10"] = np.asarray(P.getWeightUpXLowY()).copy()
+            arrays["w01"] = np.asarray(P.getWeightLowXUpY()).copy()
+            arrays["w11"] = np.asarray(P.getWeightUpXUpY()).copy()
+            P.chargeToGrid(g)
+            arrays["chargeOnGrid"] = np.asarray(P.getChargeOnGrid()).copy()
+            P.eFieldToParticles(g, E)
+            arrays["eAtParticles"] = np.asarray(P.getEAtParticles()).copy()
+            B = rng.normal(0, 0.3, 3 * g.getNpExt())
+            P.bFieldToParticles(g, B)
+            arrays["B_nodes"] = B
+            arrays["bAtParticles"] = np.asarray(P.getBAtParticles())[:n].copy()
+            dt = 2e-11
+            for tb in (0, 1, 2):
+                Q = particles.Particles("electrons", "variableWeight")
+                Q.setParticleData(pd.copy())
+                Q.setBConst(np.array([0.01, 0.5, -0.2]))
+                Q.calcGridWeights(g)
+                Q.eFieldToParticles(g, E)
+                Q.bFieldToParticles(g, B)
+                Q.borisPush(dt, tb)
+                arrays[f"push{tb}"] = np.asarray(Q.getParticleData()).copy()
+            arrays["push_dt"] = np.array(dt)
+            arrays["bconst"] = np.array([0.01, 0.5, -0.2])
+            # Boundary: particles near the wall moved outward by one push
+            # (zero field), so about half cross the wall within one cell.
+            dtb = 1e-11
+            pb = make_particles(rng, n, lx, ly, bt, 1.0)
+            scale = rng.uniform(0.95, 0.9995, n)
+            if bt == 1:
+                rho = np.sqrt(pb[:, 0] ** 2 * 4 / lx ** 2 + pb[:, 1] ** 2 * 4 / ly ** 2)
+            else:
+                rho = np.maximum(np.abs(pb[:, 0]) / (0.5 * lx), np.abs(pb[:, 1]) / (0.5 * ly))
+            pb[:, 0] *= scale / np.maximum(rho, 1e-12)
+            pb[:, 1] *= scale / np.maximum(rho, 1e-12)
+            r = np.sqrt(pb[:, 0] ** 2 + pb[:, 1] ** 2) + 1e-30
+            step = rng.uniform(0.2, 0.8, n) * min(lx / (nx - 1), ly / (ny - 1))
+            ang = rng.uniform(-0.6, 0.6, n)
+            ux, uy = pb[:, 0] / r, pb[:, 1] / r
+            vx = (ux * np.cos(ang) - uy * np.sin(ang)) * step / dtb
+            vy = (ux * np.sin(ang) + uy * np.cos(ang)) * step / dtb
+            pb[:, 2], pb[:, 3] = vx, vy
+            pb[:, 4] = rng.normal(0, 1e5, n)
+            arrays["bnd_in"] = pb.copy()
+            arrays["bnd_dt"] = np.array(dtb)
+            zeroE = np.zeros(2 * g.getNpExt())
+            kinds = [("rect", particleBoundary.AbsorbRectangular)] if bt == 0 else \
+                [("ell", particleBoundary.AbsorbElliptical), ("cc", particleBoundary.AbsorbArbitraryCutCell)]
+            for tag, cls in kinds:
+                R = particles.Particles("electrons", "variableWeight")
+                R.setParticleData(pb.copy())
+                R.calcGridWeights(g)
+                R.eFieldToParticles(g, zeroE)
+                R.borisPush(dtb, 0)
+                bd = cls(g, R)
+                bd.indexInside()
+                arrays[f"{tag}_moved"] = np.asarray(R.getParticleData()).copy()
+                arrays[f"{tag}_isInside"] = np.asarray(R.getIsInside()).copy()
+                bd.saveAbsorbed()
+                arrays[f"{tag}_absorbed"] = np.asarray(bd.getAbsorbedParticles()).copy()
+                if bd.getAbsorbedMacroParticleCount() > 0:
+                    bd.calculateInteractionPoint()
+                    bd.calculateNormalVectors()
+                    arrays[f"{tag}_wall"] = np.asarray(bd.getAbsorbedParticles()).copy()
+                    arrays[f"{tag}_normals"] = np.asarray(bd.getNormalVectors()).copy()
+        path = os.path.join(HERE, f"grid_{gname}.npz")
+        np.savez_compressed(path, **arrays)
+        print("wrote", path, os.path.getsize(path))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,34 @@
+"""liboec.so loads on the CPU host and exports every symbol include/*.h declares."""
+import glob
+import os
+import re
+
+from conftest import ROOT
+
+
+def declared_symbols():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names.update(re.findall(r"\bint\s+(oec_\w+)\s*\(", text))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = declared_symbols()
+    assert "oec_push_gather" in names and "oec_deposit" in names
+    assert len(names) >= 10
+
+
+def test_library_exports_all_declared_symbols():
+    from openecloud_b200 import _lib
+    L = _lib.lib()  # loads without a GPU: no CUDA call happens at load time
+    missing = [n for n in declared_symbols() if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_python_signatures_cover_header():
+    from openecloud_b200 import _lib
+    missing = [n for n in declared_symbols() if n not in _lib.SIGNATURES]
+    assert not missing, missing
