@@ -170,12 +170,24 @@ def cpu_reference_steps(n_sample, min_seconds, max_steps, min_steps=1):
             e = O.field_to_particles(p, og, E, 2)
             state["pd"] = O.boris_push(p, e, 1e-11, qm, 1, bconst=[0.0, 0.5, 0.0])
             O.index_inside(state["pd"], og, 0)
+    # Every timed step starts from the same in-grid sample: the reference
+    # indexes its grid unchecked (particles.pyx:410-411), so particles may not
+    # be left to drift out of the extended grid over many steps.
+    def reload():
+        if mods is not None:
+            P.setParticleData(pd.copy())
+        else:
+            state["pd"] = pd.copy()
+    reload()
     step()  # warm caches
-    t0 = time.perf_counter()
-    while steps < min_steps or (time.perf_counter() - t0 < min_seconds and steps < max_steps):
+    dt = 0.0
+    t_all = time.perf_counter()
+    while steps < min_steps or (time.perf_counter() - t_all < min_seconds and steps < max_steps):
+        reload()
+        t0 = time.perf_counter()
         step()
+        dt += time.perf_counter() - t0
         steps += 1
-    dt = time.perf_counter() - t0
     return {"value": n_sample * steps / dt, "unit": METRIC, "cores": 1, "kind": kind,
             "sample": f"{n_sample} particles x {steps} steps of the same workload (512x512 rect, B_y=0.5 T), "
                       f"single thread ({dt:.1f} s)"}
@@ -222,6 +234,7 @@ def run_ours(args, rank, world, local_rank):
     dt = 1e-11
     P.pushGatherDeposit(g, et, dt, 1, bd)  # computes the fixed-point scale once
     torch.cuda.synchronize()
+    _log(f"setup done: {n} particles, capacity {P._cap}")
 
     cg, cp, cb = g.c_grid(), P.c_particles(), bd.c_boundary()
     bconst = _lib.d3([0.0, 0.5, 0.0])
@@ -268,6 +281,7 @@ def run_ours(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_step, ms_kernel = float(t[0]), float(t[1])
     status = P.status()
+    _log(f"timed: {ms_step:.4f} ms/step, kernel {ms_kernel:.4f} ms, clocks {clk}")
 
     # ---------------------------------------------- end to end (host buffers)
     e2e = None
@@ -329,6 +343,8 @@ def run_ours(args, rank, world, local_rank):
         except Exception:
             traffic = None
 
+    if e2e is not None:
+        _log(f"e2e: {e2e['ms_per_step']:.3f} ms/step")
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_steps(1 << 21, min_seconds=10.0, max_steps=200, min_steps=3)
@@ -352,6 +368,10 @@ def run_ours(args, rank, world, local_rank):
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
+
+
+def _log(msg):
+    print(f"[bench] {msg}", file=sys.stderr, flush=True)
 
 
 def main():

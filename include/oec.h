@@ -51,7 +51,8 @@ typedef struct oec_status {
     int32_t n_wait_timeout;    /* bounded device waits that gave up */
     int32_t warn_derm;         /* delta_E+delta_R >= cap (particleEmitter.pyx:201-206) */
     int32_t warn_tsprime;      /* delta_TS' >= m (particleEmitter.pyx:209-214) */
-    int32_t reserved[6];
+    int32_t n_out_of_grid;     /* particles that left the extended grid (absorbed) */
+    int32_t reserved[5];
 } oec_status_t;
 
 /* ------------------------------------------------------------ types */
@@ -130,9 +131,10 @@ int oec_boris_push(const oec_grid_t *grid, oec_particles_t *p, const double *e_a
                    double charge_over_mass, int32_t type_b_field, void *stream);
 
 /* Fixed-point deposit scale: charge of a particle of weight w is stored as
- * llrint(w * wscale) integer units, wscale = 2^(40 - ceil(log2(wmax))).
- * Computes wscale on the device from the particles' max |w|; bits is 40, or
- * fewer when the capacity exceeds 2^22 so that capacity * 2^bits <= 2^62. */
+ * llrint(w * wscale) integer units, wscale = 2^(bits - ceil(log2(wmax))).
+ * Computes wscale on the device from the particles' max |w|; bits =
+ * min(50, 62 - ceil(log2(capacity))), so capacity * 2^bits <= 2^62 and no
+ * node can leave the int64 range whatever the particle distribution. */
 int oec_deposit_scale(const oec_particles_t *p, double *wscale_dev, void *stream);
 
 /* THE HOT PATH.  One pass over all particles:
@@ -171,6 +173,63 @@ int oec_deposit_finalize(const oec_grid_t *grid, const int64_t *rho_fix_dev,
  * kind the positions are first clipped to the grid (:485-508). */
 int oec_index_inside(const oec_grid_t *grid, oec_particles_t *p, const oec_boundary_t *boundary,
                      uint32_t *absorbed_mask_dev, oec_status_t *status_dev, void *stream);
+
+/* ------------------------------------------- grid geometry (A11-A14, host) */
+
+/* Boundary function of the grid (grid.pyx:88-105). */
+#define OEC_BOUND_RECT 0      /* p0 = lx/2, p1 = ly/2 (grid.pyx:1437) */
+#define OEC_BOUND_ELLIPSE 1   /* p0 = 4/lx^2, p1 = 4/ly^2 (grid.pyx:1443) */
+#define OEC_BOUND_POLYGON 2   /* poly: quadrant polygon, winding test of |x|,|y| */
+#define OEC_BOUND_CALLBACK 3  /* fn(x, y, ctx) -> 0/1 (a user boundFunc) */
+typedef int (*oec_bound_fn)(double x, double y, void *ctx);
+
+typedef struct oec_geom_in {
+    int32_t nx, ny;            /* nxExt, nyExt */
+    double dx, dy;
+    const double *x_mesh;      /* [nx] */
+    const double *y_mesh;      /* [ny] */
+    double scan_around_point;  /* relative probe offset (grid.pyx:49) */
+    double cut_cell_acc;       /* bisection accuracy (cut-cell only) */
+    int32_t cut_cell;          /* 0: staircase (grid.pyx:166), 1: cut-cell (:468) */
+    int32_t bound_kind;        /* OEC_BOUND_* */
+    double p0, p1;
+    const double *poly;
+    int32_t n_poly;
+    oec_bound_fn fn;
+    void *ctx;
+} oec_geom_in_t;
+
+/* Caller-allocated outputs; G = nx*ny.  Capacities: boundary points
+ * cap_boundary_points (<= 2G), each COO stage cap_coo (8G is enough). */
+typedef struct oec_geom_out {
+    uint16_t *inside_points;   /* [G] */
+    uint16_t *inside_edges;    /* [2G] x-edges then y-edges */
+    uint16_t *inside_faces;    /* [G] */
+    double *ds, *dsi;          /* [2G] */
+    double *da, *dai;          /* [G] */
+    double *dst, *dsti;        /* [2G] */
+    double *dat, *dati;        /* [G] */
+    double *boundary_points;   /* [cap_boundary_points*2] */
+    uint32_t *boundary_points_ind;
+    int32_t cap_boundary_points;
+    int32_t n_boundary_points; /* out */
+    int32_t *cut_cell_points_ind;  /* [G*2], -1 where unused */
+    double *cut_cell_center;       /* [G*2] */
+    double *cut_cell_normals;      /* [G*2] */
+    int64_t cap_coo;
+    int32_t *r1, *c1; double *v1; int64_t n1;  /* edge average (grid.pyx:390 / :900) */
+    int32_t *r2, *c2; double *v2; int64_t n2;  /* boundary extrapolation (:432 / :1133) */
+    int32_t *r3, *c3; double *v3; int64_t n3;  /* triangle cells (:1206); n3 = -1 if absent */
+} oec_geom_out_t;
+
+/* computeStaircaseGridGeom / computeCutCellGridGeom (grid.pyx:166-1330). */
+int oec_grid_geometry(const oec_geom_in_t *in, oec_geom_out_t *out);
+
+/* pointInPolygon (grid.pyx:108-120): 1 if (|x|,|y|) is inside. Not a status. */
+int oec_point_in_polygon(const double *poly, int32_t n, double x, double y);
+
+/* prepareBoundFuncPoints (grid.pyx:123-159): drop collinear vertices. */
+int oec_polygon_prepare(const double *pts, int32_t n, double *out, int32_t *n_out);
 
 #ifdef __cplusplus
 }

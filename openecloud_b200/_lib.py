@@ -40,7 +40,8 @@ class Boundary_t(ctypes.Structure):
 
 
 STATUS_FIELDS = ["n_absorbed", "n_secondaries", "n_nonfinite", "n_clipped", "n_not_found",
-                 "n_capacity_drop", "deposit_overflow", "n_wait_timeout", "warn_derm", "warn_tsprime"]
+                 "n_capacity_drop", "deposit_overflow", "n_wait_timeout", "warn_derm", "warn_tsprime",
+                 "n_out_of_grid"]
 STATUS_WORDS = 16
 
 _P = ctypes.c_void_p
@@ -70,6 +71,9 @@ SIGNATURES = {
 }
 
 _lib = None
+# entry points whose ctypes signatures live next to their Python users
+# (structure arguments defined there); registered at import of that module
+OTHER_DECLARED = set()
 
 
 def lib():

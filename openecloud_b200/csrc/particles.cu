@@ -245,6 +245,39 @@ __device__ __forceinline__ void deposit_warp(int key, long long v[4], unsigned l
     }
 }
 
+// Deposit of a thread's four consecutive particles.  Cell-sorted storage
+// makes them share one or two cells: the first two distinct cells are summed
+// in registers and reduced across the warp (two rounds at most); any further
+// cell, rare for sorted data, is added directly.
+__device__ __forceinline__ void deposit_thread4(const int key[4], const float w[4], const float fx[4],
+                                                const float fy[4], double wscale, unsigned long long *rho,
+                                                int nx) {
+    long long a0[4] = {0, 0, 0, 0}, a1[4] = {0, 0, 0, 0};
+    int k0 = -1, k1 = -1;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (key[j] < 0) continue;
+        long long v[4];
+        corner_charges(w[j], fx[j], fy[j], wscale, v);
+        if (k0 < 0 || key[j] == k0) {
+            k0 = key[j];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) a0[t] += v[t];
+        } else if (k1 < 0 || key[j] == k1) {
+            k1 = key[j];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) a1[t] += v[t];
+        } else {
+            atomicAdd(rho + key[j], (unsigned long long)v[0]);
+            atomicAdd(rho + key[j] + 1, (unsigned long long)v[1]);
+            atomicAdd(rho + key[j] + nx, (unsigned long long)v[2]);
+            atomicAdd(rho + key[j] + nx + 1, (unsigned long long)v[3]);
+        }
+    }
+    deposit_warp(k0, a0, rho, nx);
+    deposit_warp(k1, a1, rho, nx);
+}
+
 // ------------------------------------------------------- fused kernel
 
 struct FusedArgs {
@@ -273,7 +306,7 @@ __global__ void __launch_bounds__(kThreads) k_push_gather(FusedArgs a) {
     const int lane = threadIdx.x & 31;
     const int nchunks = (n + kChunk - 1) / kChunk;
     const double wscale = DEP ? *a.wscale : 0.0;
-    int absorbed_local = 0, nonfinite_local = 0, clipped_local = 0;
+    int absorbed_local = 0, nonfinite_local = 0, clipped_local = 0, outgrid_local = 0;
 
     for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
         const int q = chunk * kThreads + threadIdx.x;  // float4 group index
@@ -304,7 +337,7 @@ __global__ void __launch_bounds__(kThreads) k_push_gather(FusedArgs a) {
             const int c = cc[j];
             if ((unsigned)c >= (unsigned)a.ncell) {  // not a valid interpolation cell
                 nib |= 1u << j;
-                ++nonfinite_local;
+                ++outgrid_local;
                 continue;
             }
             // --- gather at the current position (particles.pyx:354-372)
@@ -333,6 +366,8 @@ __global__ void __launch_bounds__(kThreads) k_push_gather(FusedArgs a) {
             if (!finite) {
                 ++nonfinite_local;
                 out = true;
+                fx[j] = nxo;
+                fy[j] = nyo;
             } else {
                 float sx = floorf(fminf(fmaxf(nxo, -1048576.f), 1048576.f));
                 float sy = floorf(fminf(fmaxf(nyo, -1048576.f), 1048576.f));
@@ -353,13 +388,20 @@ __global__ void __launch_bounds__(kThreads) k_push_gather(FusedArgs a) {
                     if (iy > a.ny - 2) { iy = a.ny - 2; nyo = 1.0f - a.b.clip_lo; clip = true; }
                     if (iy == a.ny - 2 && nyo > 1.0f - a.b.clip_lo) { nyo = 1.0f - a.b.clip_lo; clip = true; }
                     clipped_local += clip ? 1 : 0;
-                } else {
-                    // Outside the extended grid means outside any rect/ellipse wall.
-                    out = (ix < 0 || iy < 0 || ix > a.nx - 2 || iy > a.ny - 2);
+                } else if (ix < 0 || iy < 0 || ix > a.nx - 2 || iy > a.ny - 2) {
+                    // Left the extended grid: outside any rect/ellipse wall.
+                    // Keep the old (valid) cell and the unfloored offset so
+                    // the absolute position stays exact for the wall
+                    // intersection and no packed index wraps around.
+                    out = true;
+                    ++outgrid_local;
+                    nxo = gx + a.k.dtdxi * vx[j];
+                    nyo = gy + a.k.dtdyi * vy[j];
+                    ix = -1;
                 }
                 fx[j] = nxo;
                 fy[j] = nyo;
-                cc[j] = ix + iy * a.nx;
+                if (ix >= 0) cc[j] = ix + iy * a.nx;
                 if (!out) {
                     double x = abs_coord(ix, nxo, a.dx, a.lxh);
                     double y = abs_coord(iy, nyo, a.dy, a.lyh);
@@ -397,19 +439,14 @@ __global__ void __launch_bounds__(kThreads) k_push_gather(FusedArgs a) {
         absorbed_local += __popc(nib);
 
         // --- deposit of the surviving particles at their new position
-        if (DEP) {
-#pragma unroll
-            for (int j = 0; j < kPer; ++j) {
-                long long v[4] = {0, 0, 0, 0};
-                if (key[j] >= 0) corner_charges(ww[j], fx[j], fy[j], wscale, v);
-                deposit_warp(key[j], v, a.rho, a.nx);
-            }
-        }
+        if (DEP) deposit_thread4(key, ww, fx, fy, wscale, a.rho, a.nx);
     }
     int s = __reduce_add_sync(kFullMask, absorbed_local);
     if (lane == 0 && s) atomicAdd(&a.status->n_absorbed, s);
     s = __reduce_add_sync(kFullMask, nonfinite_local);
     if (lane == 0 && s) atomicAdd(&a.status->n_nonfinite, s);
+    s = __reduce_add_sync(kFullMask, outgrid_local);
+    if (lane == 0 && s) atomicAdd(&a.status->n_out_of_grid, s);
     if (KIND == OEC_BOUNDARY_CUTCELL) {
         s = __reduce_add_sync(kFullMask, clipped_local);
         if (lane == 0 && s) atomicAdd(&a.status->n_clipped, s);
@@ -436,13 +473,10 @@ __global__ void __launch_bounds__(kThreads)
         float fx[4] = {fx4.x, fx4.y, fx4.z, fx4.w};
         float fy[4] = {fy4.x, fy4.y, fy4.z, fy4.w};
         float ww[4] = {w4.x, w4.y, w4.z, w4.w};
+        int key[4];
 #pragma unroll
-        for (int j = 0; j < kPer; ++j) {
-            long long v[4] = {0, 0, 0, 0};
-            int key = (base + j < n && (unsigned)cc[j] < (unsigned)ncell) ? cc[j] : -1;
-            if (key >= 0) corner_charges(ww[j], fx[j], fy[j], wscale, v);
-            deposit_warp(key, v, rho, nx);
-        }
+        for (int j = 0; j < kPer; ++j) key[j] = (base + j < n && (unsigned)cc[j] < (unsigned)ncell) ? cc[j] : -1;
+        deposit_thread4(key, ww, fx, fy, wscale, rho, nx);
     }
 }
 
@@ -665,7 +699,7 @@ namespace oec {
 namespace {
 // Standalone push (API path): velocity update then move with carry.
 __global__ void k_boris_push_move(oec_particles_t p, const double *__restrict__ e_at,
-                                  const double *__restrict__ b_at, PushConst k, int nx) {
+                                  const double *__restrict__ b_at, PushConst k, int nx, int ny, float inv_nx) {
     int64_t n = *p.count;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -686,9 +720,17 @@ __global__ void k_boris_push_move(oec_particles_t p, const double *__restrict__ 
         if (!(isfinite(ox) && isfinite(oy))) continue;  // left for the inside test to absorb
         float fx = floorf(fminf(fmaxf(ox, -1048576.f), 1048576.f));
         float fy = floorf(fminf(fmaxf(oy, -1048576.f), 1048576.f));
+        int cx = (int)fx, cy = (int)fy;
+        int ix, iy;
+        split_cell(p.cell[i], nx, inv_nx, ix, iy);
+        if (ix + cx < 0 || iy + cy < 0 || ix + cx > nx - 2 || iy + cy > ny - 2) {
+            // left the extended grid: keep the valid cell, unfloored offset
+            p.ox[i] = ox;
+            p.oy[i] = oy;
+            continue;
+        }
         ox -= fx;
         oy -= fy;
-        int cx = (int)fx, cy = (int)fy;
         if (ox >= 1.0f) { ox = 0.0f; cx += 1; }
         if (oy >= 1.0f) { oy = 0.0f; cy += 1; }
         p.ox[i] = ox;
@@ -710,18 +752,19 @@ extern "C" int oec_boris_push(const oec_grid_t *grid, oec_particles_t *p, const 
     double zero[3] = {0, 0, 0};
     PushConst k = make_push_const(gc, bconst ? bconst : zero, dt, charge_over_mass, type_b_field);
     k_boris_push_move<<<persistent_grid(cap_chunks(p) * 4, 8), 256, 0, as_stream(stream)>>>(
-        *p, e_at_particles_dev, b_at_particles_dev, k, gc.nx);
+        *p, e_at_particles_dev, b_at_particles_dev, k, gc.nx, gc.ny, 1.0f / (float)gc.nx);
     OEC_LAUNCH_CHECK();
     return OEC_OK;
 }
 
 static int deposit_bits(const oec_particles_t *p) {
     // A node sums at most `capacity` particles of at most 2^bits units:
-    // capacity * 2^bits <= 2^62 keeps every node inside int64.
+    // capacity * 2^bits <= 2^62 keeps every node inside int64.  At most 50
+    // bits so that the f64 corner products stay exact to well below a unit.
     int lc = 0;
     while ((int64_t(1) << lc) < p->capacity) ++lc;
     int bits = 62 - lc;
-    return bits > 40 ? 40 : bits;
+    return bits > 50 ? 50 : bits;
 }
 
 extern "C" int oec_deposit_scale(const oec_particles_t *p, double *wscale_dev, void *stream) {
