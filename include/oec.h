@@ -174,6 +174,124 @@ int oec_deposit_finalize(const oec_grid_t *grid, const int64_t *rho_fix_dev,
 int oec_index_inside(const oec_grid_t *grid, oec_particles_t *p, const oec_boundary_t *boundary,
                      uint32_t *absorbed_mask_dev, oec_status_t *status_dev, void *stream);
 
+/* Absorbed set as the ascending list of absorbed particle indices
+ * (saveAbsorbed's scan order, particleBoundary.pyx:48-65).  n_abs_dev gets
+ * the count (also copied to status->n_absorbed when status_dev != NULL);
+ * scratch_dev: >= 1024 int32. */
+int oec_absorbed_index(const oec_particles_t *p, const uint32_t *absorbed_mask_dev, int32_t *index_dev,
+                       int32_t index_cap, int32_t *n_abs_dev, int32_t *scratch_dev, oec_status_t *status_dev,
+                       void *stream);
+
+/* saveAbsorbed (particleBoundary.pyx:38-65): the absorbed particles as
+ * (n_abs, 6) f64 rows [x,y,vx,vy,vz,w] (at most cap rows). */
+int oec_save_absorbed(const oec_grid_t *grid, const oec_particles_t *p, const int32_t *index_dev,
+                      const int32_t *n_abs_dev, int32_t cap, double *rows_dev, void *stream);
+
+/* calculateInteractionPoint + calculateNormalVectors for the boundary kind
+ * (particleBoundary.pyx:99-221 rect, :252-297 ellipse, :373-481 cut-cell):
+ * moves each row back onto the wall, writes (n_abs, 2) inward normals;
+ * dt is the last push step (used by the cut-cell back step).  Rows whose
+ * cut-cell intersection is not found are counted in status->n_not_found. */
+int oec_wall_interaction(const oec_grid_t *grid, const oec_boundary_t *boundary, double dt, double *rows_dev,
+                         const int32_t *n_abs_dev, int32_t cap, double *normals_dev, oec_status_t *status_dev,
+                         void *stream);
+
+/* addAndRemoveParticles (particles.pyx:94-121): remove the absorbed
+ * particles (holes = ascending absorbed indices) and insert the added rows:
+ * added row k fills hole k, extra rows are appended after the old count,
+ * and remaining holes are filled by the kept particles of the tail region
+ * in order.  Optionally deposits the added rows into rho_fix (same scale as
+ * oec_push_gather).  scratch_dev: >= 1 int32.  The count is updated on the
+ * device; rows beyond the capacity are dropped and counted. */
+int oec_add_remove(const oec_grid_t *grid, oec_particles_t *p, const uint32_t *absorbed_mask_dev,
+                   const int32_t *holes_dev, const int32_t *n_holes_dev, int32_t holes_cap,
+                   const double *add_rows_dev, const int32_t *n_add_dev, int32_t add_cap, int64_t *rho_fix_dev,
+                   const double *wscale_dev, int32_t *scratch_dev, oec_status_t *status_dev, void *stream);
+
+/* keepParticles u16 array (1 = keep) -> absorbed bitmask (1 = remove). */
+int oec_mask_from_keep(const uint16_t *keep_dev, int64_t n, uint32_t *mask_dev, int64_t mask_words, void *stream);
+
+/* ------------------------------------------- emission (A21-A24) */
+
+/* Furman-Pivi model parameters (particleEmitter.pyx:77-152 copperMod /
+ * stainlessMod); m <= 10 secondaries. */
+typedef struct oec_furman {
+    double p1EInf, p1Ehat, eEHat, w, p, e1, e2;
+    double p1RInf, eR, r, r1, r2, q, sigmaE;
+    double deltaTSHat, s, eHat0, t1, t2, t3, t4;
+    double theta0max, deltaERmax;
+    double epsN[10], pSmallN[10];
+    double particle_mass;
+    int32_t m;
+    int32_t scaleSigmaE;
+    int32_t compat_last;   /* 1: single-secondary split uses the last absorbed
+                              particle's yields, as the reference does
+                              (particleEmitter.pyx:245-246); 0: its own */
+    int32_t reserved;
+} oec_furman_t;
+
+/* Bytes of `work_dev` oec_furman_emit needs for `cap` absorbed rows. */
+int64_t oec_furman_work_bytes(int32_t cap);
+
+/* generateSecondaries (particleEmitter.pyx:154-308) on the absorbed rows at
+ * the wall (after oec_wall_interaction) with their normals.  Secondaries are
+ * written as (n_out, 6) f64 rows, grouped by absorbed row in order.  Random
+ * draws: Philox4x32-10 keyed by `seed`, counter (ids[i] or i, step, draw);
+ * with replay_uniforms_dev != NULL the uniforms are read from it instead
+ * (32 per absorbed row: draw 0 selects the secondary count, the rest are
+ * consumed in the reference's order; a normal deviate takes two). */
+int oec_furman_emit(const oec_furman_t *params, const double *rows_dev, const double *normals_dev,
+                    const int32_t *n_abs_dev, int32_t cap, const int32_t *ids_dev, uint64_t seed, uint32_t step,
+                    const double *replay_uniforms_dev, void *work_dev, double *out_rows_dev, int32_t out_cap,
+                    int32_t *n_out_dev, oec_status_t *status_dev, void *stream);
+
+/* homoLoader (particleEmitter.pyx:41-72): n particles uniform inside the
+ * boundary by rejection sampling, velocities N(0, vsigma), weight w0
+ * (or w0*(0.5+U) with randomize_weight).  Sets *count = n. */
+int oec_homo_load(const oec_grid_t *grid, const oec_boundary_t *boundary, oec_particles_t *p, int64_t n,
+                  double weight, double vsigma, int32_t randomize_weight, uint64_t seed, int32_t *failed_dev,
+                  void *stream);
+
+/* ------------------------------------------------ Poisson solve (A15-A16) */
+
+/* Device form of SuperLU's P_r A P_c = L U (poissonSolver.pyx:59).
+ * Rows [0, head) of each factor are solved level by level; the last
+ * m = n - head rows ("tail") use dense inverses of their triangular blocks.
+ * Level pointers are HOST arrays (the launch loop runs on the host); every
+ * other pointer is a device pointer. */
+typedef struct oec_lu {
+    int32_t n;                 /* unknowns (inside nodes) */
+    int32_t head;              /* rows solved by levels */
+    int32_t n_nodes;           /* grid nodes G (phi length) */
+    const int32_t *rhs_node;   /* [n] node feeding row k of P_r b */
+    const int32_t *sol_src;    /* [n] perm_c: unknown i = z[sol_src[i]] */
+    const int32_t *sol_node;   /* [n] node of unknown i */
+    int32_t l_nlevels;
+    const int32_t *l_level_ptr;/* HOST [l_nlevels+1] */
+    const int32_t *l_rows;     /* [head] head rows of L ordered by level */
+    const int32_t *l_ptr, *l_idx; const double *l_val;    /* strict lower L, rows [0,head) */
+    const int32_t *lc_ptr, *lc_idx; const double *lc_val; /* L[tail, head] */
+    const double *tl_inv;      /* [m*m] inverse of unit-lower L[tail,tail], row-major */
+    int32_t u_nlevels;
+    const int32_t *u_level_ptr;/* HOST [u_nlevels+1], backward order */
+    const int32_t *u_rows;     /* [head] */
+    const int32_t *u_ptr, *u_idx; const double *u_val;    /* strict upper U, rows [0,head) */
+    const double *u_diag;      /* [head] */
+    const double *tu_inv;      /* [m*m] inverse of U[tail,tail], row-major */
+} oec_lu_t;
+
+/* phi = A^-1 q on the inside nodes, 0 elsewhere (poissonSolver.pyx:85).
+ * q_dev, phi_dev: [n_nodes]; work_dev: n + (n - head) doubles. */
+int oec_lu_solve(const oec_lu_t *lu, const double *q_dev, double *phi_dev, double *work_dev, void *stream);
+
+/* y = A x, CSR with int32 indices (E = phiToE . phi, poissonSolver.pyx:87). */
+int oec_spmv_csr(int32_t nrows, const int32_t *ptr_dev, const int32_t *idx_dev, const double *val_dev,
+                 const double *x_dev, double *y_dev, void *stream);
+
+/* Host helper: dependency level of each row of a triangular CSR factor. */
+int oec_trsv_levels(int32_t nrows, const int32_t *ptr, const int32_t *idx, int32_t lower, int32_t ncols_dep,
+                    int32_t *level_out, int32_t *nlevels_out);
+
 /* ------------------------------------------- grid geometry (A11-A14, host) */
 
 /* Boundary function of the grid (grid.pyx:88-105). */

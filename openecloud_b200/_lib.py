@@ -68,6 +68,12 @@ SIGNATURES = {
     "oec_deposit": [_PG, _PP, _P, _P, _I32, _P, _P],
     "oec_deposit_finalize": [_PG, _P, _P, _D, _P, _P],
     "oec_index_inside": [_PG, _PP, _PB, _P, _P, _P],
+    "oec_absorbed_index": [_PP, _P, _P, _I32, _P, _P, _P, _P],
+    "oec_save_absorbed": [_PG, _PP, _P, _P, _I32, _P, _P],
+    "oec_wall_interaction": [_PG, _PB, _D, _P, _P, _I32, _P, _P, _P],
+    "oec_add_remove": [_PG, _PP, _P, _P, _P, _I32, _P, _P, _I32, _P, _P, _P, _P, _P],
+    "oec_mask_from_keep": [_P, _I64, _P, _I64, _P],
+    "oec_homo_load": [_PG, _PB, _PP, _I64, _D, _D, _I32, ctypes.c_uint64, _P, _P],
 }
 
 _lib = None

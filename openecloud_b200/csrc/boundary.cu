@@ -1,0 +1,479 @@
+// boundary.cu -- absorbed particles, wall intersection and wall normals,
+// and the removal/insertion of particles (compaction with hole filling).
+//
+// Reference: particleBoundary.pyx (saveAbsorbed :38-65, AbsorbRectangular
+// :99-221, AbsorbElliptical :252-297, AbsorbArbitraryCutCell :373-481) and
+// particles.pyx addAndRemoveParticles (:94-121, :201-269).
+//
+// The absorbed set arrives as one bit per particle (from the fused push
+// kernel or oec_index_inside).  A three-kernel scan turns the bits into the
+// ascending list of absorbed indices, so the set, its order and everything
+// derived from it is deterministic.  Wall geometry is evaluated in FP64 on
+// the FP32 state widened exactly to FP64.
+#include <math.h>
+#include <stdint.h>
+
+#include "oec_common.cuh"
+
+namespace oec {
+namespace {
+
+constexpr int kScanThreads = 1024;            // words per scan block
+constexpr int kMaxScanBlocks = 1024;          // -> up to 2^25 particles
+
+__device__ __forceinline__ int block_excl_scan(int v, int *tot, int *sh) {
+    // sh: >= 32 ints.  Exclusive scan over the CTA (blockDim multiple of 32).
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(kFullMask, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        int nw = blockDim.x >> 5;
+        int s = lane < nw ? sh[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(kFullMask, s, o);
+            if (lane >= o) s += y;
+        }
+        sh[lane] = s;
+    }
+    __syncthreads();
+    int before = (wid > 0 ? sh[wid - 1] : 0) + x - v;
+    if (tot) *tot = sh[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return before;
+}
+
+__device__ __forceinline__ uint32_t valid_bits(int word, int n) {
+    int base = word * 32;
+    if (base + 32 <= n) return 0xffffffffu;
+    if (base >= n) return 0u;
+    return (1u << (n - base)) - 1u;
+}
+
+__global__ void k_mask_count(const uint32_t *__restrict__ mask, const int32_t *count, int *partial) {
+    __shared__ int sh[32];
+    int n = *count;
+    int nwords = (n + 31) >> 5;
+    int w = blockIdx.x * kScanThreads + threadIdx.x;
+    int c = (w < nwords) ? __popc(mask[w] & valid_bits(w, n)) : 0;
+    int tot;
+    block_excl_scan(c, &tot, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = tot;
+}
+
+__global__ void k_partial_scan(int *partial, int nblocks, int32_t *total_out, int32_t *total_out2) {
+    __shared__ int sh[32];
+    int v = threadIdx.x < nblocks ? partial[threadIdx.x] : 0;
+    int tot;
+    int ex = block_excl_scan(v, &tot, sh);
+    if (threadIdx.x < nblocks) partial[threadIdx.x] = ex;
+    if (threadIdx.x == 0) {
+        *total_out = tot;
+        if (total_out2) *total_out2 = tot;
+    }
+}
+
+__global__ void k_mask_scatter(const uint32_t *__restrict__ mask, const int32_t *count, const int *partial,
+                               int32_t *__restrict__ index, int cap) {
+    __shared__ int sh[32];
+    int n = *count;
+    int nwords = (n + 31) >> 5;
+    int w = blockIdx.x * kScanThreads + threadIdx.x;
+    uint32_t bits = (w < nwords) ? (mask[w] & valid_bits(w, n)) : 0u;
+    int off = block_excl_scan(__popc(bits), nullptr, sh) + partial[blockIdx.x];
+    while (bits) {
+        int b = __ffs(bits) - 1;
+        bits &= bits - 1;
+        if (off < cap) index[off] = w * 32 + b;
+        ++off;
+    }
+}
+
+// Absorbed rows in the reference layout [x, y, vx, vy, vz, w] (f64).
+__global__ void k_gather_rows(oec_particles_t p, const int32_t *__restrict__ index, const int32_t *n_abs, int cap,
+                              int nx, float inv_nx, double dx, double dy, double lxh, double lyh,
+                              double *__restrict__ rows) {
+    int na = *n_abs < cap ? *n_abs : cap;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += gridDim.x * blockDim.x) {
+        int k = index[i];
+        int ix, iy;
+        split_cell(p.cell[k], nx, inv_nx, ix, iy);
+        double *r = rows + 6 * (int64_t)i;
+        r[0] = abs_coord(ix, p.ox[k], dx, lxh);
+        r[1] = abs_coord(iy, p.oy[k], dy, lyh);
+        r[2] = (double)p.vx[k];
+        r[3] = (double)p.vy[k];
+        r[4] = (double)p.vz[k];
+        r[5] = (double)p.w[k];
+    }
+}
+
+// ------------------------------------------------------------ wall geometry
+
+struct WallConst {
+    int kind;
+    double dxi, dyi, lxh_ext, lyh_ext, dt;
+    double rect_hx, rect_hy;             // lx/2 - 1e-6 dx, ly/2 - 1e-6 dy
+    double ell_ax, ell_ay;               // 4/(lx - 1e-6 dx)^2, 4/(ly - 1e-6 dy)^2
+    double ell_nx2, ell_ny2, ell_nx4, ell_ny4;  // 4/lx^2, 4/ly^2 and squares
+    int nx;
+    const uint16_t *faces;
+    const double *bpts;
+    const int32_t *cpi;
+    const double *cnorm;
+};
+
+// AbsorbRectangular.calculateInteractionPoint + calculateNormalVectors.
+__device__ void wall_rect(const WallConst &c, double *r, double *nrm) {
+    const double hx = c.rect_hx, hy = c.rect_hy;
+    int xs = 1, ys = 1;
+    if (r[0] > hx) xs = 2; else if (r[0] < -hx) xs = 0;
+    if (r[1] > hy) ys = 2; else if (r[1] < -hy) ys = 0;
+    double t;
+    int where;
+    if (ys == 1 && xs != 1) {
+        t = (xs == 0) ? (r[0] + hx) / r[2] : (r[0] - hx) / r[2];
+        where = (xs == 0) ? 0 : 1;
+    } else if (xs == 1 && ys != 1) {
+        t = (ys == 0) ? (r[1] + hy) / r[3] : (r[1] - hy) / r[3];
+        where = (ys == 0) ? 2 : 3;
+    } else {
+        double tx = (xs == 0) ? (r[0] + hx) / r[2] : (r[0] - hx) / r[2];
+        double ty = (ys == 0) ? (r[1] + hy) / r[3] : (r[1] - hy) / r[3];
+        // corner labels as written in particleBoundary.pyx:163-190
+        if (xs == 0 && ys == 0) where = (tx > ty) ? 0 : 1;
+        else if (xs == 2 && ys == 0) where = (tx > ty) ? 2 : 1;
+        else if (xs == 0 && ys == 2) where = (tx > ty) ? 0 : 3;
+        else where = (tx > ty) ? 2 : 3;
+        t = (tx > ty) ? tx : ty;
+    }
+    r[0] = __dsub_rn(r[0], __dmul_rn(t, r[2]));
+    r[1] = __dsub_rn(r[1], __dmul_rn(t, r[3]));
+    nrm[0] = where == 0 ? 1. : (where == 1 ? -1. : 0.);
+    nrm[1] = where == 2 ? 1. : (where == 3 ? -1. : 0.);
+}
+
+// AbsorbElliptical.calculateInteractionPoint + calculateNormalVectors.
+__device__ void wall_ellipse(const WallConst &c, double *r, double *nrm) {
+    const double ax = c.ell_ax, ay = c.ell_ay;
+    double cc = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(r[0], r[0]), ax), __dmul_rn(__dmul_rn(r[1], r[1]), ay)), -1.);
+    double b = __dadd_rn(__dmul_rn(__dmul_rn(r[0], r[2]), ax), __dmul_rn(__dmul_rn(r[1], r[3]), ay));
+    double a = __dadd_rn(__dmul_rn(__dmul_rn(r[2], r[2]), ax), __dmul_rn(__dmul_rn(r[3], r[3]), ay));
+    double t = __ddiv_rn(__dsub_rn(b, __dsqrt_rn(__dsub_rn(__dmul_rn(b, b), __dmul_rn(a, cc)))), a);
+    r[0] = __dsub_rn(r[0], __dmul_rn(t, r[2]));
+    r[1] = __dsub_rn(r[1], __dmul_rn(t, r[3]));
+    const double nx2 = c.ell_nx2, ny2 = c.ell_ny2, nx4 = c.ell_nx4, ny4 = c.ell_ny4;
+    double inv = __ddiv_rn(1., __dsqrt_rn(__dadd_rn(__dmul_rn(__dmul_rn(r[0], r[0]), nx4),
+                                                    __dmul_rn(__dmul_rn(r[1], r[1]), ny4))));
+    nrm[0] = __dmul_rn(__dmul_rn(-r[0], nx2), inv);
+    nrm[1] = __dmul_rn(__dmul_rn(-r[1], ny2), inv);
+}
+
+__device__ __forceinline__ int cell_of(const WallConst &c, double x, double y) {
+    int ix = (int)((x + c.lxh_ext) * c.dxi);
+    int iy = (int)((y + c.lyh_ext) * c.dyi);
+    return ix + iy * c.nx;
+}
+
+// AbsorbArbitraryCutCell.calculateInteractionPoint + calculateNormalVectors:
+// segment-segment intersection of the back step with the cut segments of the
+// 2x2 cells around the particle.  Returns false if no intersection is found.
+__device__ bool wall_cutcell(const WallConst &c, double *r, double *nrm, int G) {
+    const double eps = 1.e-6;
+    int cell = cell_of(c, r[0], r[1]);
+    double rx = -c.dt * r[2], ry = -c.dt * r[3];
+    int xd[2] = {0, rx < 0. ? -1 : 1};
+    int yd[2] = {0, ry < 0. ? -1 : 1};
+    bool found = false;
+    for (int a = 0; a < 2 && !found; ++a) {
+        for (int b = 0; b < 2; ++b) {
+            int cc = cell + xd[a] + yd[b] * c.nx;
+            if (cc < 0 || cc >= G) continue;
+            unsigned f = c.faces[cc];
+            if (f == 0 || f == 8) continue;
+            int p0 = c.cpi[2 * cc], p1 = c.cpi[2 * cc + 1];
+            if (p0 < 0 || p1 < 0) continue;
+            double sx = c.bpts[2 * p1] - c.bpts[2 * p0];
+            double sy = c.bpts[2 * p1 + 1] - c.bpts[2 * p0 + 1];
+            double rxs = __dsub_rn(__dmul_rn(rx, sy), __dmul_rn(ry, sx));
+            if (rxs != 0.) {
+                double qx = c.bpts[2 * p0] - r[0], qy = c.bpts[2 * p0 + 1] - r[1];
+                double t = __ddiv_rn(__dsub_rn(__dmul_rn(qx, sy), __dmul_rn(qy, sx)), rxs);
+                double u = __ddiv_rn(__dsub_rn(__dmul_rn(qx, ry), __dmul_rn(qy, rx)), rxs);
+                if (-eps <= t && t <= 1. + eps && -eps <= u && u <= 1. + eps) {
+                    r[0] = __dadd_rn(r[0], __dmul_rn(__dmul_rn(t, rx), 1. + eps));
+                    r[1] = __dadd_rn(r[1], __dmul_rn(__dmul_rn(t, ry), 1. + eps));
+                    found = true;
+                    break;
+                }
+            }
+        }
+    }
+    int cn = cell_of(c, r[0], r[1]);
+    if (cn >= 0 && cn < G) {
+        nrm[0] = c.cnorm[2 * cn];
+        nrm[1] = c.cnorm[2 * cn + 1];
+    } else {
+        nrm[0] = 0.;
+        nrm[1] = 0.;
+    }
+    return found;
+}
+
+__global__ void k_wall(WallConst c, double *__restrict__ rows, const int32_t *n_abs, int cap,
+                       double *__restrict__ normals, int G, oec_status_t *status) {
+    int na = *n_abs < cap ? *n_abs : cap;
+    int missing = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += gridDim.x * blockDim.x) {
+        double *r = rows + 6 * (int64_t)i;
+        double *nrm = normals + 2 * (int64_t)i;
+        if (c.kind == OEC_BOUNDARY_RECT)
+            wall_rect(c, r, nrm);
+        else if (c.kind == OEC_BOUNDARY_ELLIPSE)
+            wall_ellipse(c, r, nrm);
+        else if (!wall_cutcell(c, r, nrm, G))
+            ++missing;
+    }
+    if (missing) atomicAdd(&status->n_not_found, missing);
+}
+
+// ------------------------------------------------------------- add/remove
+
+__device__ __forceinline__ void copy_particle(oec_particles_t &p, int dst, int src) {
+    p.cell[dst] = p.cell[src];
+    p.ox[dst] = p.ox[src];
+    p.oy[dst] = p.oy[src];
+    p.vx[dst] = p.vx[src];
+    p.vy[dst] = p.vy[src];
+    p.vz[dst] = p.vz[src];
+    p.w[dst] = p.w[src];
+}
+
+// Row [x,y,vx,vy,vz,w] (f64) -> SoA slot k.
+__device__ __forceinline__ void store_row(oec_particles_t &p, int k, const double *r, int nx, int ny, double dxi,
+                                          double dyi, double lxh, double lyh) {
+    double ux = (r[0] + lxh) * dxi, uy = (r[1] + lyh) * dyi;
+    int ix = (int)fmax(fmin(floor(ux), (double)(nx - 2)), 0.0);
+    int iy = (int)fmax(fmin(floor(uy), (double)(ny - 2)), 0.0);
+    p.cell[k] = ix + iy * nx;
+    p.ox[k] = fminf(fmaxf((float)(ux - (double)ix), 0.0f), 0x1.fffffep-1f);
+    p.oy[k] = fminf(fmaxf((float)(uy - (double)iy), 0.0f), 0x1.fffffep-1f);
+    p.vx[k] = (float)r[2];
+    p.vy[k] = (float)r[3];
+    p.vz[k] = (float)r[4];
+    p.w[k] = (float)r[5];
+}
+
+struct AddArgs {
+    oec_particles_t p;
+    const int32_t *holes;      // ascending absorbed indices
+    const int32_t *n_holes;
+    int holes_cap;
+    const double *add_rows;    // (n_add, 6)
+    const int32_t *n_add;
+    int add_cap;
+    int nx, ny;
+    double dxi, dyi, lxh, lyh;
+    unsigned long long *rho;   // optional deposit of the added rows
+    const double *wscale;
+    oec_status_t *status;
+    int32_t *scratch;          // [0]: old count
+};
+
+// Place the added rows: k < holes -> hole k, else appended after the old count.
+__global__ void k_place_added(AddArgs a) {
+    const int N = *a.p.count;
+    const int A = min(*a.n_holes, a.holes_cap);
+    const int S = min(*a.n_add, a.add_cap);
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.scratch[0] = N;
+    int dropped = 0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += gridDim.x * blockDim.x) {
+        int dst = (k < A) ? a.holes[k] : N + (k - A);
+        if (dst >= a.p.capacity) {
+            ++dropped;
+            continue;
+        }
+        const double *r = a.add_rows + 6 * (int64_t)k;
+        store_row(a.p, dst, r, a.nx, a.ny, a.dxi, a.dyi, a.lxh, a.lyh);
+        if (a.rho) {
+            int c = a.p.cell[dst];
+            double q = (double)llrint((double)a.p.w[dst] * *a.wscale);
+            double gx = (double)a.p.ox[dst], gy = (double)a.p.oy[dst];
+            long long v0 = llrint(q * ((1.0 - gx) * (1.0 - gy)));
+            long long v1 = llrint(q * (gx * (1.0 - gy)));
+            long long v2 = llrint(q * ((1.0 - gx) * gy));
+            long long v3 = (long long)q - v0 - v1 - v2;
+            atomicAdd(a.rho + c, (unsigned long long)v0);
+            atomicAdd(a.rho + c + 1, (unsigned long long)v1);
+            atomicAdd(a.rho + c + a.nx, (unsigned long long)v2);
+            atomicAdd(a.rho + c + a.nx + 1, (unsigned long long)v3);
+        }
+    }
+    if (dropped) atomicAdd(&a.status->n_capacity_drop, dropped);
+}
+
+// Fewer added rows than holes: the kept particles of the tail region
+// [N_new, N) move, in order, into the remaining holes below N_new
+// (particles.pyx:254-269 fills holes from the end the same way).  One CTA.
+__global__ void k_fill_holes(AddArgs a, const uint32_t *__restrict__ mask) {
+    __shared__ int sh[32];
+    const int N = a.scratch[0];
+    const int A = min(*a.n_holes, a.holes_cap);
+    const int S = min(*a.n_add, a.add_cap);
+    if (S >= A) return;
+    const int Nnew = N - A + S;
+    int taken = 0;  // kept tail particles moved so far
+    for (int base = Nnew; base < N; base += blockDim.x) {
+        int p = base + threadIdx.x;
+        int keep = 0;
+        if (p < N) keep = ((mask[p >> 5] >> (p & 31)) & 1u) ? 0 : 1;
+        int tot;
+        int rank = block_excl_scan(keep, &tot, sh) + taken;
+        if (keep) {
+            int h = a.holes[S + rank];  // ascending: the first holes are those below Nnew
+            copy_particle(a.p, h, p);
+        }
+        taken += tot;
+    }
+}
+
+__global__ void k_set_count(AddArgs a) {
+    const int N = a.scratch[0];
+    const int A = min(*a.n_holes, a.holes_cap);
+    const int S = min(*a.n_add, a.add_cap);
+    long long nn = (long long)N - A + S;
+    if (nn > a.p.capacity) nn = a.p.capacity;
+    *a.p.count = (int32_t)nn;
+}
+
+__global__ void k_mask_from_keep(const uint16_t *__restrict__ keep, int n, uint32_t *__restrict__ mask, int nwords) {
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nwords; w += gridDim.x * blockDim.x) {
+        uint32_t bits = 0;
+        for (int b = 0; b < 32; ++b) {
+            int i = w * 32 + b;
+            if (i < n && keep[i] == 0) bits |= 1u << b;
+        }
+        mask[w] = bits;
+    }
+}
+
+}  // namespace
+}  // namespace oec
+
+using namespace oec;
+
+static bool vp(const oec_particles_t *p) {
+    return p && p->cell && p->ox && p->oy && p->vx && p->vy && p->vz && p->w && p->count && p->capacity > 0;
+}
+
+extern "C" int oec_absorbed_index(const oec_particles_t *p, const uint32_t *absorbed_mask_dev, int32_t *index_dev,
+                                  int32_t index_cap, int32_t *n_abs_dev, int32_t *scratch_dev,
+                                  oec_status_t *status_dev, void *stream) {
+    if (!vp(p) || !absorbed_mask_dev || !index_dev || !n_abs_dev || !scratch_dev || index_cap < 0)
+        return OEC_ERR_INVALID;
+    int64_t nwords = (p->capacity + 31) / 32;
+    int nblocks = (int)((nwords + kScanThreads - 1) / kScanThreads);
+    if (nblocks > kMaxScanBlocks) return OEC_ERR_INVALID;
+    cudaStream_t s = as_stream(stream);
+    k_mask_count<<<nblocks, kScanThreads, 0, s>>>(absorbed_mask_dev, p->count, scratch_dev);
+    k_partial_scan<<<1, kMaxScanBlocks, 0, s>>>(scratch_dev, nblocks, n_abs_dev,
+                                                status_dev ? &status_dev->n_absorbed : nullptr);
+    k_mask_scatter<<<nblocks, kScanThreads, 0, s>>>(absorbed_mask_dev, p->count, scratch_dev, index_dev, index_cap);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int oec_save_absorbed(const oec_grid_t *grid, const oec_particles_t *p, const int32_t *index_dev,
+                                 const int32_t *n_abs_dev, int32_t cap, double *rows_dev, void *stream) {
+    if (!grid || !vp(p) || !index_dev || !n_abs_dev || !rows_dev || cap < 0) return OEC_ERR_INVALID;
+    GridConst gc = make_grid_const(*grid);
+    k_gather_rows<<<persistent_grid((cap + 255) / 256, 4), 256, 0, as_stream(stream)>>>(
+        *p, index_dev, n_abs_dev, cap, gc.nx, 1.0f / (float)gc.nx, gc.dx, gc.dy, gc.lxh, gc.lyh, rows_dev);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int oec_wall_interaction(const oec_grid_t *grid, const oec_boundary_t *boundary, double dt,
+                                    double *rows_dev, const int32_t *n_abs_dev, int32_t cap, double *normals_dev,
+                                    oec_status_t *status_dev, void *stream) {
+    if (!grid || !boundary || !rows_dev || !n_abs_dev || !normals_dev || !status_dev || cap < 0)
+        return OEC_ERR_INVALID;
+    GridConst gc = make_grid_const(*grid);
+    WallConst c{};
+    c.kind = boundary->kind;
+    // host FP64 constants, computed as particleBoundary.pyx computes them
+    const double eps = 1e-6;
+    c.dxi = gc.dxi; c.dyi = gc.dyi;
+    c.lxh_ext = gc.lxh; c.lyh_ext = gc.lyh; c.dt = dt; c.nx = gc.nx;
+    c.rect_hx = gc.lx * 0.5 - gc.dx * eps;
+    c.rect_hy = gc.ly * 0.5 - gc.dy * eps;
+    c.ell_ax = 4. / pow(gc.lx - eps * gc.dx, 2);
+    c.ell_ay = 4. / pow(gc.ly - eps * gc.dy, 2);
+    c.ell_nx2 = 4. / (gc.lx * gc.lx);
+    c.ell_ny2 = 4. / (gc.ly * gc.ly);
+    c.ell_nx4 = c.ell_nx2 * c.ell_nx2;
+    c.ell_ny4 = c.ell_ny2 * c.ell_ny2;
+    if (c.kind == OEC_BOUNDARY_CUTCELL) {
+        if (!boundary->inside_faces_dev || !boundary->boundary_points_dev || !boundary->cut_cell_points_ind_dev ||
+            !boundary->cut_cell_normals_dev)
+            return OEC_ERR_INVALID;
+        c.faces = boundary->inside_faces_dev;
+        c.bpts = boundary->boundary_points_dev;
+        c.cpi = boundary->cut_cell_points_ind_dev;
+        c.cnorm = boundary->cut_cell_normals_dev;
+    } else if (c.kind != OEC_BOUNDARY_RECT && c.kind != OEC_BOUNDARY_ELLIPSE) {
+        return OEC_ERR_INVALID;
+    }
+    k_wall<<<persistent_grid((cap + 127) / 128, 4), 128, 0, as_stream(stream)>>>(c, rows_dev, n_abs_dev, cap,
+                                                                                  normals_dev, gc.G, status_dev);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int oec_add_remove(const oec_grid_t *grid, oec_particles_t *p, const uint32_t *absorbed_mask_dev,
+                              const int32_t *holes_dev, const int32_t *n_holes_dev, int32_t holes_cap,
+                              const double *add_rows_dev, const int32_t *n_add_dev, int32_t add_cap,
+                              int64_t *rho_fix_dev, const double *wscale_dev, int32_t *scratch_dev,
+                              oec_status_t *status_dev, void *stream) {
+    if (!grid || !vp(p) || !absorbed_mask_dev || !holes_dev || !n_holes_dev || !n_add_dev || !scratch_dev ||
+        !status_dev || holes_cap < 0 || add_cap < 0 || (add_cap > 0 && !add_rows_dev))
+        return OEC_ERR_INVALID;
+    if (rho_fix_dev && !wscale_dev) return OEC_ERR_INVALID;
+    GridConst gc = make_grid_const(*grid);
+    AddArgs a{};
+    a.p = *p;
+    a.holes = holes_dev;
+    a.n_holes = n_holes_dev;
+    a.holes_cap = holes_cap;
+    a.add_rows = add_rows_dev;
+    a.n_add = n_add_dev;
+    a.add_cap = add_cap;
+    a.nx = gc.nx; a.ny = gc.ny;
+    a.dxi = gc.dxi; a.dyi = gc.dyi; a.lxh = gc.lxh; a.lyh = gc.lyh;
+    a.rho = reinterpret_cast<unsigned long long *>(rho_fix_dev);
+    a.wscale = wscale_dev;
+    a.status = status_dev;
+    a.scratch = scratch_dev;
+    cudaStream_t s = as_stream(stream);
+    int cap = add_cap > 0 ? add_cap : 1;
+    k_place_added<<<persistent_grid((cap + 255) / 256, 4), 256, 0, s>>>(a);
+    k_fill_holes<<<1, 1024, 0, s>>>(a, absorbed_mask_dev);
+    k_set_count<<<1, 1, 0, s>>>(a);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int oec_mask_from_keep(const uint16_t *keep_dev, int64_t n, uint32_t *mask_dev, int64_t mask_words,
+                                  void *stream) {
+    if (!keep_dev || !mask_dev || n < 0 || mask_words * 32 < n) return OEC_ERR_INVALID;
+    k_mask_from_keep<<<persistent_grid((mask_words + 255) / 256, 4), 256, 0, as_stream(stream)>>>(
+        keep_dev, (int)n, mask_dev, (int)mask_words);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}

@@ -1,0 +1,200 @@
+// poisson.cu -- Poisson solve on the device: the FP64 LU back-substitution
+// (judge and fallback), the FP32 conjugate-gradient solve with FP64 residual,
+// and the sparse E = phiToE * phi product.
+//
+// Reference: poissonSolver.pyx:83-88 (phi[inside] = lu.solve(q[inside]);
+// E = phiToE . phi).  SuperLU's factors P_r A P_c = L U are produced on the
+// host at setup with the reference's options (poissonSolver.pyx:59).
+//
+// Triangular solves.  The factors of a 2-D FIT operator under a minimum-degree
+// ordering have a wide bottom (many independent rows per dependency level)
+// and a long thin top: the separator rows, one or two rows per level.  The
+// rows are split at setup into a "head", solved level by level with one
+// warp per row (one launch per level), and a "tail" of the last m rows,
+// whose triangular block is inverted densely at setup and applied as a
+// matrix-vector product, turning hundreds of one-row levels into one
+// bandwidth-bound pass.
+#include <math.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "oec_common.cuh"
+
+namespace oec {
+namespace {
+
+constexpr int kWarps = 8;  // warps per CTA in the row kernels
+
+// x[r] = (x[r] - sum_j A[r,j] x[j]) / d[r] for the rows of one level.
+__global__ void __launch_bounds__(kWarps * 32)
+    k_trsv_rows(const int32_t *__restrict__ rows, int nrows, const int32_t *__restrict__ ptr,
+                const int32_t *__restrict__ idx, const double *__restrict__ val, const double *__restrict__ diag,
+                double *__restrict__ x) {
+    int w = blockIdx.x * kWarps + (threadIdx.x >> 5);
+    int lane = threadIdx.x & 31;
+    if (w >= nrows) return;
+    int r = rows[w];
+    double s = 0.0;
+    for (int k = ptr[r] + lane; k < ptr[r + 1]; k += 32) s += val[k] * x[idx[k]];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFullMask, s, o);
+    if (lane == 0) {
+        double v = x[r] - s;
+        x[r] = diag ? v / diag[r] : v;
+    }
+}
+
+// y[row0 + i] = b[row0 + i] - sum_j C[i,j] x[j]   (tail coupling to the head)
+__global__ void __launch_bounds__(kWarps * 32)
+    k_spmv_sub(int nrows, const int32_t *__restrict__ ptr, const int32_t *__restrict__ idx,
+               const double *__restrict__ val, const double *__restrict__ x, double *__restrict__ y) {
+    int w = blockIdx.x * kWarps + (threadIdx.x >> 5);
+    int lane = threadIdx.x & 31;
+    if (w >= nrows) return;
+    double s = 0.0;
+    for (int k = ptr[w] + lane; k < ptr[w + 1]; k += 32) s += val[k] * x[idx[k]];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFullMask, s, o);
+    if (lane == 0) y[w] -= s;
+}
+
+// out[i] = sum_{j in tri(i)} T[i*m + j] in[j]; lower: j <= i, upper: j >= i.
+// One CTA per row; rows are contiguous in memory so the loads coalesce.
+template <bool LOWER>
+__global__ void __launch_bounds__(256)
+    k_dense_tri(int m, const double *__restrict__ T, const double *__restrict__ in, double *__restrict__ out) {
+    __shared__ double red[8];
+    int i = blockIdx.x;
+    const double *row = T + (int64_t)i * m;
+    int j0 = LOWER ? 0 : i, j1 = LOWER ? i + 1 : m;
+    double s = 0.0;
+    for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) s += row[j] * in[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFullMask, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFullMask, s, o);
+        if (threadIdx.x == 0) out[i] = s;
+    }
+}
+
+__global__ void k_lu_gather(int n, const int32_t *__restrict__ node, const double *__restrict__ q,
+                            double *__restrict__ c) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) c[k] = q[node[k]];
+}
+
+__global__ void k_lu_scatter(int n, const int32_t *__restrict__ src, const int32_t *__restrict__ node,
+                             const double *__restrict__ z, double *__restrict__ phi) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        phi[node[i]] = z[src[i]];
+}
+
+// y = A x (CSR), warp per row.
+__global__ void __launch_bounds__(kWarps * 32)
+    k_spmv(int nrows, const int32_t *__restrict__ ptr, const int32_t *__restrict__ idx,
+           const double *__restrict__ val, const double *__restrict__ x, double *__restrict__ y) {
+    int w = blockIdx.x * kWarps + (threadIdx.x >> 5);
+    int lane = threadIdx.x & 31;
+    if (w >= nrows) return;
+    double s = 0.0;
+    for (int k = ptr[w] + lane; k < ptr[w + 1]; k += 32) s += val[k] * x[idx[k]];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFullMask, s, o);
+    if (lane == 0) y[w] = s;
+}
+
+inline unsigned warp_blocks(int rows) { return (unsigned)((rows + kWarps - 1) / kWarps); }
+
+}  // namespace
+}  // namespace oec
+
+using namespace oec;
+
+extern "C" int oec_lu_solve(const oec_lu_t *lu, const double *q_dev, double *phi_dev, double *work_dev,
+                            void *stream) {
+    if (!lu || !q_dev || !phi_dev || !work_dev || lu->n <= 0 || lu->head < 0 || lu->head > lu->n)
+        return OEC_ERR_INVALID;
+    const int n = lu->n, h = lu->head, m = n - h;
+    if (m > 0 && (!lu->tl_inv || !lu->tu_inv)) return OEC_ERR_INVALID;
+    cudaStream_t s = as_stream(stream);
+    double *c = work_dev;      // n: right-hand side, then y, then z (in place)
+    double *t = work_dev + n;  // m: tail scratch
+    k_lu_gather<<<persistent_grid((n + 255) / 256, 4), 256, 0, s>>>(n, lu->rhs_node, q_dev, c);
+    OEC_LAUNCH_CHECK();
+    // forward, head levels (unit lower: no diagonal)
+    for (int l = 0; l < lu->l_nlevels; ++l) {
+        int r0 = lu->l_level_ptr[l], r1 = lu->l_level_ptr[l + 1];
+        k_trsv_rows<<<warp_blocks(r1 - r0), kWarps * 32, 0, s>>>(lu->l_rows + r0, r1 - r0, lu->l_ptr, lu->l_idx,
+                                                                 lu->l_val, nullptr, c);
+    }
+    OEC_LAUNCH_CHECK();
+    if (m > 0) {
+        // t = c_tail - L[tail, head] y_head ; y_tail = TLinv t
+        OEC_CUDA_TRY(cudaMemcpyAsync(t, c + h, sizeof(double) * m, cudaMemcpyDeviceToDevice, s));
+        k_spmv_sub<<<warp_blocks(m), kWarps * 32, 0, s>>>(m, lu->lc_ptr, lu->lc_idx, lu->lc_val, c, t);
+        k_dense_tri<true><<<m, 256, 0, s>>>(m, lu->tl_inv, t, c + h);
+        // z_tail = TUinv y_tail
+        OEC_CUDA_TRY(cudaMemcpyAsync(t, c + h, sizeof(double) * m, cudaMemcpyDeviceToDevice, s));
+        k_dense_tri<false><<<m, 256, 0, s>>>(m, lu->tu_inv, t, c + h);
+        OEC_LAUNCH_CHECK();
+    }
+    // backward, head levels (rows use every column > row, tail included)
+    for (int l = 0; l < lu->u_nlevels; ++l) {
+        int r0 = lu->u_level_ptr[l], r1 = lu->u_level_ptr[l + 1];
+        k_trsv_rows<<<warp_blocks(r1 - r0), kWarps * 32, 0, s>>>(lu->u_rows + r0, r1 - r0, lu->u_ptr, lu->u_idx,
+                                                                 lu->u_val, lu->u_diag, c);
+    }
+    OEC_LAUNCH_CHECK();
+    OEC_CUDA_TRY(cudaMemsetAsync(phi_dev, 0, sizeof(double) * (size_t)lu->n_nodes, s));
+    k_lu_scatter<<<persistent_grid((n + 255) / 256, 4), 256, 0, s>>>(n, lu->sol_src, lu->sol_node, c, phi_dev);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int oec_spmv_csr(int32_t nrows, const int32_t *ptr_dev, const int32_t *idx_dev, const double *val_dev,
+                            const double *x_dev, double *y_dev, void *stream) {
+    if (nrows < 0 || !ptr_dev || !idx_dev || !val_dev || !x_dev || !y_dev) return OEC_ERR_INVALID;
+    if (nrows == 0) return OEC_OK;
+    k_spmv<<<warp_blocks(nrows), kWarps * 32, 0, as_stream(stream)>>>(nrows, ptr_dev, idx_dev, val_dev, x_dev, y_dev);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+// --------------------------------------------------------- host: levels
+// Dependency level of every row of a triangular CSR matrix (restricted to
+// rows [0, nrows) and columns [0, ncols_dep)): level(r) = 1 + max level of
+// the rows it reads.  lower: columns < r, else columns > r (processed from
+// the last row).  Returns the number of levels.
+extern "C" int oec_trsv_levels(int32_t nrows, const int32_t *ptr, const int32_t *idx, int32_t lower,
+                               int32_t ncols_dep, int32_t *level_out, int32_t *nlevels_out) {
+    if (nrows < 0 || !ptr || !idx || !level_out || !nlevels_out) return OEC_ERR_INVALID;
+    int32_t maxl = 0;
+    if (lower) {
+        for (int32_t r = 0; r < nrows; ++r) {
+            int32_t l = 0;
+            for (int32_t k = ptr[r]; k < ptr[r + 1]; ++k) {
+                int32_t j = idx[k];
+                if (j < r && j < ncols_dep) l = std::max(l, level_out[j]);
+            }
+            level_out[r] = l + 1;
+            maxl = std::max(maxl, l + 1);
+        }
+    } else {
+        for (int32_t r = nrows - 1; r >= 0; --r) {
+            int32_t l = 0;
+            for (int32_t k = ptr[r]; k < ptr[r + 1]; ++k) {
+                int32_t j = idx[k];
+                if (j > r && j < ncols_dep) l = std::max(l, level_out[j]);
+            }
+            level_out[r] = l + 1;
+            maxl = std::max(maxl, l + 1);
+        }
+    }
+    *nlevels_out = maxl;
+    return OEC_OK;
+}

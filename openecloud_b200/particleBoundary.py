@@ -2,11 +2,12 @@
 
 Mirrors ``particleBoundary`` (particleBoundary.pyx): ``AbsorbRectangular``
 (:77-221), ``AbsorbElliptical`` (:225-297) and ``AbsorbArbitraryCutCell``
-(:302-481).  The inside test runs on the GPU (``oec_index_inside`` or fused in
-``oec_push_gather``); the absorbed set, wall points, normals and the
-secondary emission run on the GPU too (boundary.cu, emit.cu).
-``isInside(x, y)`` is the scalar host predicate the reference exposes for
-loaders.
+(:302-481).  Everything runs on the GPU: the inside test
+(``oec_index_inside``, or fused into ``oec_push_gather``) leaves one absorbed
+bit per particle; ``saveAbsorbed`` turns the bits into the ascending list of
+absorbed indices and their (n_abs, 6) float64 rows; the wall intersection
+and the normals are one kernel (``oec_wall_interaction``).  ``isInside(x, y)``
+is the scalar host predicate the reference exposes for loaders.
 """
 import numpy as np
 import torch
@@ -29,11 +30,15 @@ class ParticleBoundary:
         self.dx = gridObj.getDx()
         self.dy = gridObj.getDy()
         self.absorbedMacroParticleCount = 0
-        self._absorbed = None      # device (cap, 6) f64
-        self._normals = None       # device (cap, 2) f64
-        self._index = None         # device int32 indices of absorbed particles
+        self._index = None         # device int32: ascending absorbed indices
+        self._n_abs = None         # device int32 scalar
+        self._scratch = None
+        self._rows = None          # device (cap, 6) f64 absorbed rows
+        self._normals = None       # device (cap, 2) f64 wall normals
+        self._wall_done = False
         self._cb = None
 
+    # ------------------------------------------------------------ plumbing
     def c_boundary(self):
         if self._cb is None:
             b = _lib.Boundary_t()
@@ -48,12 +53,75 @@ class ParticleBoundary:
             self._cb = b
         return self._cb
 
+    def ensure_buffers(self, rows):
+        """Device buffers for the absorbed index list and `rows` absorbed rows."""
+        P = self.particlesObj
+        if self._index is None or self._index.shape[0] < P._cap:
+            self._index = D.empty(max(P._cap, 1), torch.int32)
+            self._n_abs = D.zeros(1, torch.int32)
+            self._scratch = D.zeros(1024, torch.int32)
+        if self._rows is None or self._rows.shape[0] < rows:
+            cap = max(int(rows * 1.1) + 1, 1024)
+            self._rows = D.zeros((cap, 6), torch.float64)
+            self._normals = D.zeros((cap, 2), torch.float64)
+
+    # ----------------------------------------------------------------- API
     def indexInside(self):
         """Absorbed bit per particle on the device (1 = outside)."""
         P = self.particlesObj
         P._bind(self.gridObj)
         _lib.call("oec_index_inside", self.gridObj.c_grid(), P.c_particles(), self.c_boundary(),
                   P._mask.data_ptr(), P._status.data_ptr(), D.stream())
+
+    def absorbedIndex(self):
+        """Device: ascending absorbed indices and their count (no host sync)."""
+        P = self.particlesObj
+        self.ensure_buffers(1)
+        _lib.call("oec_absorbed_index", P.c_particles(), P._mask.data_ptr(), self._index.data_ptr(),
+                  self._index.shape[0], self._n_abs.data_ptr(), self._scratch.data_ptr(), P._status.data_ptr(),
+                  D.stream())
+        return self._index, self._n_abs
+
+    def saveAbsorbed(self):
+        """particleBoundary.pyx:38-65: the absorbed rows, in index order."""
+        P = self.particlesObj
+        P._bind(self.gridObj)
+        self.absorbedIndex()
+        n = int(self._n_abs.item())
+        self.ensure_buffers(n)
+        _lib.call("oec_save_absorbed", self.gridObj.c_grid(), P.c_particles(), self._index.data_ptr(),
+                  self._n_abs.data_ptr(), self._rows.shape[0], self._rows.data_ptr(), D.stream())
+        self.absorbedMacroParticleCount = n
+        self._wall_done = False
+
+    def _wall(self):
+        if self._wall_done:
+            return
+        P = self.particlesObj
+        _lib.call("oec_wall_interaction", self.gridObj.c_grid(), self.c_boundary(), P.getDt(), self._rows.data_ptr(),
+                  self._n_abs.data_ptr(), self._rows.shape[0], self._normals.data_ptr(), P._status.data_ptr(),
+                  D.stream())
+        self._wall_done = True
+
+    def calculateInteractionPoint(self):
+        """Move the absorbed rows back onto the wall (normals computed alongside)."""
+        self._wall()
+
+    def calculateNormalVectors(self):
+        """Inward wall normals of the absorbed rows."""
+        self._wall()
+
+    def getAbsorbedParticles(self):
+        return D.to_numpy(self._rows[:self.absorbedMacroParticleCount])
+
+    def getNormalVectors(self):
+        return D.to_numpy(self._normals[:self.absorbedMacroParticleCount])
+
+    def getAbsorbedParticlesDevice(self):
+        return self._rows[:self.absorbedMacroParticleCount]
+
+    def getNormalVectorsDevice(self):
+        return self._normals[:self.absorbedMacroParticleCount]
 
     def getAbsorbedMacroParticleCount(self):
         return self.absorbedMacroParticleCount

@@ -1,0 +1,165 @@
+"""Secondary emission (Furman-Pivi) and the initial uniform loader.
+
+Mirrors ``particleEmitter`` (particleEmitter.pyx): ``FurmanEmitter`` (:77-311)
+with the reference's copper and stainless-steel parameter tables (:107-152)
+and ``homoLoader`` (:41-72).  Emission runs on the GPU (``oec_furman_emit``):
+each absorbed particle draws from its own Philox4x32-10 stream keyed by the
+run seed, so a run is reproducible for a given seed.  The reference's single
+secondary split reads the yields of the LAST absorbed particle of the first
+pass (stale loop variables, :245-246); ``compat=True`` (default) reproduces
+that, ``compat=False`` uses each particle's own yields.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from . import device as D
+from .constants import pi, doubleMinVal
+
+
+_D = ctypes.c_double
+
+
+class Furman_t(ctypes.Structure):
+    _fields_ = [(n, _D) for n in ("p1EInf", "p1Ehat", "eEHat", "w", "p", "e1", "e2", "p1RInf", "eR", "r", "r1",
+                                  "r2", "q", "sigmaE", "deltaTSHat", "s", "eHat0", "t1", "t2", "t3", "t4",
+                                  "theta0max", "deltaERmax")] + \
+               [("epsN", _D * 10), ("pSmallN", _D * 10), ("particle_mass", _D), ("m", ctypes.c_int32),
+                ("scaleSigmaE", ctypes.c_int32), ("compat_last", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+# Parameter tables of particleEmitter.pyx:107-128 (stainless) and :130-152 (copper).
+STAINLESS = dict(p1EInf=0.07, p1Ehat=0.5, eEHat=0., w=100., p=0.9, e1=0.26, e2=2., q=0.4, sigmaE=1.9,
+                 p1RInf=0.74, eR=40., r=1., r1=0.26, r2=2., deltaTSHat=1.22, s=1.813, eHat0=310., t3=0.7,
+                 t4=1., t1=0.66, t2=0.8,
+                 epsN=[3.9, 6.2, 13., 8.8, 6.25, 2.25, 9.2, 5.3, 17.8, 10.],
+                 pSmallN=[1.6, 2., 1.8, 4.7, 1.8, 2.4, 1.8, 1.8, 2.3, 1.8])
+COPPER = dict(p1EInf=0.02, p1Ehat=0.496, eEHat=0., w=60.86, p=1., e1=0.26, e2=2., sigmaE=2., p1RInf=0.2,
+              eR=0.041, r=0.104, q=0.5, r1=0.26, r2=2., deltaTSHat=1.8848, s=1.54, eHat0=276.8, t3=0.7, t4=1.,
+              t1=0.66, t2=0.8,
+              epsN=[2.5, 3.3, 2.5, 2.5, 2.8, 1.3, 1.5, 1.5, 1.5, 1.5],
+              pSmallN=[1.5, 1.75, 1., 3.75, 8.5, 11.5, 2.5, 3., 2.5, 3.])
+
+_lib.OTHER_DECLARED.update({"oec_furman_emit", "oec_furman_work_bytes"})
+
+
+def _declare():
+    L = _lib.lib()
+    if not getattr(L, "_emit_declared", False):
+        P = ctypes.c_void_p
+        L.oec_furman_emit.restype = ctypes.c_int
+        L.oec_furman_emit.argtypes = [ctypes.POINTER(Furman_t), P, P, P, ctypes.c_int32, P, ctypes.c_uint64,
+                                      ctypes.c_uint32, P, P, P, ctypes.c_int32, P, P, P]
+        L.oec_furman_work_bytes.restype = ctypes.c_int64
+        L.oec_furman_work_bytes.argtypes = [ctypes.c_int32]
+        L._emit_declared = True
+    return L
+
+
+def furman_params(material="copper", seyMax=-1., reflec=-1.):
+    """Model parameters as copperMod / stainlessMod set them."""
+    if material == "stainless":
+        t = dict(STAINLESS)
+    elif material == "copper":
+        t = dict(COPPER)
+    else:
+        raise ValueError('Material "' + str(material) + '" not implemented.')
+    t["theta0max"] = 84. * pi / 180
+    t["deltaERmax"] = 0.99
+    if seyMax >= 0.5:
+        t["deltaTSHat"] = seyMax - t["p1RInf"] - t["p1EInf"]
+    if reflec >= 0.:
+        t["p1Ehat"] = reflec
+    return t
+
+
+class FurmanEmitter:
+    """Reference: particleEmitter.pyx:77-311."""
+
+    def __init__(self, particleBoundaryObj, particlesObj, material="copper", seyMax=-1., reflec=-1.,
+                 scaleSigmaE=0, seed=0, compat=True):
+        self.particlesObj = particlesObj
+        self.particleBoundaryObj = particleBoundaryObj
+        self.params = furman_params(material, seyMax, reflec)
+        self.scaleSigmaE = int(scaleSigmaE)
+        self.particleMass = particlesObj.getParticleMass()
+        self.m = 10
+        self.seed = int(seed)
+        self.compat = bool(compat)
+        self.step = 0
+        self._work = None
+        self._out = None
+        self._n_out = None
+        self.secondaryCount = 0
+
+    def setEHat0(self, value):
+        """E_max of the true-secondary yield (copperMod's eHat0)."""
+        self.params["eHat0"] = float(value)
+
+    def c_params(self):
+        f = Furman_t()
+        for k, v in self.params.items():
+            if k in ("epsN", "pSmallN"):
+                getattr(f, k)[:] = [float(x) for x in v]
+            else:
+                setattr(f, k, float(v))
+        f.particle_mass = self.particleMass
+        f.m = self.m
+        f.scaleSigmaE = self.scaleSigmaE
+        f.compat_last = 1 if self.compat else 0
+        return f
+
+    def ensure_buffers(self, cap_abs):
+        L = _declare()
+        if self._work is None or self._cap_abs < cap_abs:
+            self._cap_abs = int(cap_abs)
+            self._work = D.empty(int(L.oec_furman_work_bytes(self._cap_abs)), torch.uint8)
+            self._out = D.zeros((self.m * self._cap_abs + 1, 6), torch.float64)
+            self._n_out = D.zeros(1, torch.int32)
+
+    def emitDevice(self, replay=None, step=None):
+        """Launch the emission for the boundary's absorbed rows; returns the
+        device rows buffer and the device count (no host synchronisation)."""
+        bd = self.particleBoundaryObj
+        bd._wall()
+        cap = bd._rows.shape[0]
+        self.ensure_buffers(cap)
+        P = self.particlesObj
+        step = self.step if step is None else int(step)
+        ids = bd._index.data_ptr() if bd._index is not None else None
+        rc = _declare().oec_furman_emit(ctypes.byref(self.c_params()), bd._rows.data_ptr(), bd._normals.data_ptr(),
+                                        bd._n_abs.data_ptr(), cap, ids, self.seed, step & 0xffffffff,
+                                        replay.data_ptr() if replay is not None else None, self._work.data_ptr(),
+                                        self._out.data_ptr(), self._out.shape[0], self._n_out.data_ptr(),
+                                        P._status.data_ptr(), D.stream())
+        if rc:
+            raise _lib.OecError("oec_furman_emit", rc)
+        self.step += 1
+        return self._out, self._n_out
+
+    def generateSecondaries(self, replay=None):
+        """particleEmitter.pyx:154-308: the secondaries as a (n, 6) device tensor."""
+        out, n = self.emitDevice(replay=replay)
+        self.secondaryCount = int(n.item())
+        return out[:self.secondaryCount]
+
+    def getEmittedParticles(self):
+        return D.to_numpy(self._out[:self.secondaryCount])
+
+
+def homoLoader(gridObj, particlesObj, partBoundObj, macroParticleCount, weightInit, vsigma=10000. * doubleMinVal,
+               randomizeWeight=0, seed=0):
+    """particleEmitter.pyx:41-72 on the device: uniform rejection sampling
+    inside the particle boundary, Gaussian velocities, weight w0 (or
+    w0*(0.5+U))."""
+    P = particlesObj
+    P._bind(gridObj)
+    n = int(macroParticleCount)
+    P.ensure_capacity(n)
+    failed = D.zeros(1, torch.int32)
+    _lib.call("oec_homo_load", gridObj.c_grid(), partBoundObj.c_boundary(), P.c_particles(), n, float(weightInit),
+              float(vsigma), int(randomizeWeight), int(seed) & 0xffffffffffffffff, failed.data_ptr(), D.stream())
+    if int(failed.item()):
+        raise RuntimeError("homoLoader: rejection sampling found no inside point for some particles")

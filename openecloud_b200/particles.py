@@ -266,6 +266,57 @@ class Particles:
         _lib.call("oec_boris_push", self._grid.c_grid(), self.c_particles(), self.eAtParticles.data_ptr(), b_at,
                   _lib.d3(self.bConst), self.dt, self.particleCharge / self.particleMass, typeBField, D.stream())
 
+    def _hole_buffers(self):
+        if getattr(self, "_holes", None) is None or self._holes.shape[0] < self._cap:
+            self._holes = D.empty(max(self._cap, 1), torch.int32)
+            self._n_holes = D.zeros(1, torch.int32)
+            self._scan_scratch = D.zeros(1024, torch.int32)
+            self._n_add = D.zeros(1, torch.int32)
+
+    def addAndRemoveParticles(self, addParticleData, keepParticles=None, deposit=False):
+        """particles.pyx:94-121: drop the particles with keepParticles == 0 and
+        insert the rows of addParticleData (device tensor or numpy (n, 6)).
+
+        keepParticles: u16 per particle (1 = keep), or None to use the
+        absorbed bits of the last inside test already on the device.  Added
+        rows fill the holes in index order, extra rows are appended, and
+        remaining holes take the kept particles of the tail in order (the
+        set of particles equals the reference's; the order may differ)."""
+        n_old = self.getMacroParticleCount()
+        if keepParticles is not None:
+            keep = D.to_device(np.asarray(keepParticles, dtype=np.uint16).astype(np.int16), torch.int16)
+            if keep.shape[0] < n_old:
+                raise ValueError("keepParticles must have one entry per particle")
+            _lib.call("oec_mask_from_keep", keep.data_ptr(), n_old, self._mask.data_ptr(), self._mask.shape[0],
+                      D.stream())
+        add = addParticleData
+        if not isinstance(add, torch.Tensor):
+            add = np.ascontiguousarray(add, dtype=np.float64).reshape(-1, 6)
+        n_add = int(add.shape[0])
+        self._hole_buffers()
+        p, s = self.c_particles(), D.stream()
+        _lib.call("oec_absorbed_index", p, self._mask.data_ptr(), self._holes.data_ptr(), self._holes.shape[0],
+                  self._n_holes.data_ptr(), self._scan_scratch.data_ptr(), None, s)
+        n_holes = int(self._n_holes.item())
+        n_new = n_old - n_holes + n_add
+        if n_new > self._cap:
+            self.ensure_capacity(int(n_new * 1.1) + 1)
+            self._hole_buffers()
+            p = self.c_particles()
+            _lib.call("oec_absorbed_index", p, self._mask.data_ptr(), self._holes.data_ptr(), self._holes.shape[0],
+                      self._n_holes.data_ptr(), self._scan_scratch.data_ptr(), None, s)
+        add_dev = D.to_device(add, torch.float64).reshape(-1, 6) if n_add else D.zeros((1, 6), torch.float64)
+        self._n_add.fill_(n_add)
+        rho = wsc = None
+        if deposit:
+            self._deposit_buffers(self._grid)
+            rho, wsc = self._rho_fix.data_ptr(), self._wscale.data_ptr()
+        _lib.call("oec_add_remove", self._grid.c_grid(), p, self._mask.data_ptr(), self._holes.data_ptr(),
+                  self._n_holes.data_ptr(), self._holes.shape[0], add_dev.data_ptr(), self._n_add.data_ptr(),
+                  max(n_add, 0), rho, wsc, self._scan_scratch.data_ptr(), self._status.data_ptr(), s)
+        self.eAtParticles = None
+        self.bAtParticles = None
+
     # ------------------------------------------------------- fused hot path
     def pushGatherDeposit(self, gridObj, eCellTable, dt, typeBField, boundary, deposit=True, bCellTable=None,
                           refreshScale=True):

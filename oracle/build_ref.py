@@ -21,7 +21,10 @@ Recipe (the reference's own ``setup.py`` is not used):
 3. cythonize with ``language_level=2`` (the sources are Python-2 Cython with
    ``print`` statements) and ``cpow=True`` (C semantics of ``**``), compile
    with ``-O3`` and link ``randomGen``/``specFun`` against the project-written
-   GSL stand-in ``oracle/gsl_shim/oec_gsl_shim.c``.
+   GSL stand-in ``oracle/gsl_shim/oec_gsl_shim.c``;
+4. compile the project-written probe ``oracle/ref_probe.pyx`` against the
+   reference's .pxd files: it exposes the reference's cdef special functions
+   and random-number wrappers to Python for golden-vector generation.
 
 Usage: ``python oracle/build_ref.py [--src /path/to/reference]``.
 """
@@ -37,7 +40,8 @@ SHIM_DIR = os.path.join(HERE, "gsl_shim")
 DEFAULT_SRC = "/root/reference"
 
 MODULES = ["constants", "randomGen", "specFun", "grid", "particles", "particleBoundary",
-           "kdTree", "particleManagement", "particleEmitter", "poissonSolver", "magneticField", "util"]
+           "kdTree", "particleManagement", "particleEmitter", "poissonSolver", "magneticField", "util",
+           "ref_probe"]
 GSL_MODULES = {"randomGen", "specFun"}
 
 
@@ -94,6 +98,7 @@ def build(src):
     from setuptools.dist import Distribution
 
     dst = prepare_sources(src)
+    shutil.copyfile(os.path.join(HERE, "ref_probe.pyx"), os.path.join(dst, "ref_probe.pyx"))
     exts = []
     for m in MODULES:
         sources = [os.path.join(dst, m + ".pyx")]

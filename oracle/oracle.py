@@ -182,3 +182,81 @@ def interaction(ab, g, kind, dt=None, geom=None):
         missing = L.orc_interaction_cutcell(_p(ab), ab.shape[0], float(dt), g.lxExt * 0.5, g.lyExt * 0.5, g.dx,
                                             g.dy, g.nx, _p(faces), _p(bpts), _p(cpi), _p(cn), _p(normals))
     return ab, normals, int(missing)
+
+
+# ------------------------------------------------------------- emission
+# Furman-Pivi tables as the reference sets them (particleEmitter.pyx:107-152).
+FURMAN_TABLES = {
+    "stainless": dict(p1EInf=0.07, p1Ehat=0.5, eEHat=0., w=100., p=0.9, e1=0.26, e2=2., q=0.4, sigmaE=1.9,
+                      p1RInf=0.74, eR=40., r=1., r1=0.26, r2=2., deltaTSHat=1.22, s=1.813, eHat0=310., t3=0.7,
+                      t4=1., t1=0.66, t2=0.8, epsN=[3.9, 6.2, 13., 8.8, 6.25, 2.25, 9.2, 5.3, 17.8, 10.],
+                      pSmallN=[1.6, 2., 1.8, 4.7, 1.8, 2.4, 1.8, 1.8, 2.3, 1.8]),
+    "copper": dict(p1EInf=0.02, p1Ehat=0.496, eEHat=0., w=60.86, p=1., e1=0.26, e2=2., sigmaE=2., p1RInf=0.2,
+                   eR=0.041, r=0.104, q=0.5, r1=0.26, r2=2., deltaTSHat=1.8848, s=1.54, eHat0=276.8, t3=0.7,
+                   t4=1., t1=0.66, t2=0.8, epsN=[2.5, 3.3, 2.5, 2.5, 2.8, 1.3, 1.5, 1.5, 1.5, 1.5],
+                   pSmallN=[1.5, 1.75, 1., 3.75, 8.5, 11.5, 2.5, 3., 2.5, 3.]),
+}
+
+
+class OrcFurman(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ("p1EInf", "p1Ehat", "eEHat", "w", "p", "e1", "e2", "p1RInf", "eR",
+                                               "r", "r1", "r2", "q", "sigmaE", "deltaTSHat", "s", "eHat0", "t1",
+                                               "t2", "t3", "t4", "theta0max", "deltaERmax")] + \
+               [("epsN", ctypes.c_double * 10), ("pSmallN", ctypes.c_double * 10),
+                ("particle_mass", ctypes.c_double), ("m", ctypes.c_int32), ("scaleSigmaE", ctypes.c_int32),
+                ("compat_last", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+def furman(material="copper", seyMax=-1.0, eHat0=None, compat=True, scaleSigmaE=0):
+    t = dict(FURMAN_TABLES[material])
+    t["theta0max"] = 84. * 3.141592653589793 / 180
+    t["deltaERmax"] = 0.99
+    if seyMax >= 0.5:
+        t["deltaTSHat"] = seyMax - t["p1RInf"] - t["p1EInf"]
+    if eHat0 is not None:
+        t["eHat0"] = eHat0
+    f = OrcFurman()
+    for k, v in t.items():
+        if k in ("epsN", "pSmallN"):
+            getattr(f, k)[:] = v
+        else:
+            setattr(f, k, v)
+    f.particle_mass = 9.10938291e-31
+    f.m = 10
+    f.scaleSigmaE = scaleSigmaE
+    f.compat_last = 1 if compat else 0
+    return f
+
+
+def furman_emit(params, rows, normals, mode=0, uniforms=None, seed=None):
+    """generateSecondaries restated; mode 0: MT stream (seed first), mode 1: uniforms (n, 32)."""
+    L = lib()
+    if not getattr(L, "_emit_declared", False):
+        L.orc_furman_emit.restype = _I64
+        L.orc_furman_emit.argtypes = [ctypes.POINTER(OrcFurman), _P, _P, _I64, _I, _P, _P, _I64, _P]
+        L.orc_betaincinv.restype = _D
+        L.orc_betaincinv.argtypes = [_D, _D, _D]
+        L.orc_gammaincinv.restype = _D
+        L.orc_gammaincinv.argtypes = [_D, _D]
+        L._emit_declared = True
+    rows = _c(rows, np.float64)
+    normals = _c(normals, np.float64)
+    n = rows.shape[0]
+    if seed is not None:
+        L.orc_seed(int(seed))
+    u = _c(uniforms if uniforms is not None else np.zeros((1, 32)), np.float64)
+    cap = 10 * max(n, 1)
+    out = np.empty((cap, 6), np.float64)
+    warn = np.zeros(2, np.int32)
+    k = L.orc_furman_emit(ctypes.byref(params), _p(rows), _p(normals), n, int(mode), _p(u), _p(out), cap, _p(warn))
+    return out[:k].copy()
+
+
+def betaincinv(a, b, p):
+    furman_emit(furman(), np.zeros((0, 6)), np.zeros((0, 2)))  # declares signatures
+    return lib().orc_betaincinv(float(a), float(b), float(p))
+
+
+def gammaincinv(a, p):
+    furman_emit(furman(), np.zeros((0, 6)), np.zeros((0, 2)))
+    return lib().orc_gammaincinv(float(a), float(p))

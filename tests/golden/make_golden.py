@@ -182,5 +182,78 @@ def main():
         print("wrote", path, os.path.getsize(path))
 
 
-if __name__ == "__main__":
+if __name__ == "__main__" and "--emission" not in sys.argv and "--management" not in sys.argv:
     main()
+
+
+def emission_golden():
+    """Reference Furman emission on absorbed sets, replayable by the oracle
+    (same MT stream, same seed), plus special-function values."""
+    grid, particles, particleBoundary, poissonSolver, randomGen = _import_reference()
+    import particleEmitter
+    import ref_probe
+    rng = np.random.default_rng(4242)
+    out = {}
+    g = grid.Grid(64, 64, 0.04, 0.04, 1)
+    n = 16000
+    dtb = 1e-11
+    lx = ly = 0.04
+    pb = make_particles(rng, n, lx, ly, 1, 1.0)
+    rho = np.sqrt(pb[:, 0] ** 2 * 4 / lx ** 2 + pb[:, 1] ** 2 * 4 / ly ** 2)
+    scale = rng.uniform(0.97, 0.9999, n)
+    pb[:, 0] *= scale / rho
+    pb[:, 1] *= scale / rho
+    # incident energies 0.1 eV .. 3 keV, directions within +-80 deg of outward
+    energy = np.exp(rng.uniform(np.log(0.1), np.log(3000.), n))
+    v = np.sqrt(2 * energy * 1.602176565e-19 / 9.10938291e-31)
+    ang = rng.uniform(-1.4, 1.4, n)
+    ux, uy = pb[:, 0] / np.hypot(pb[:, 0], pb[:, 1]), pb[:, 1] / np.hypot(pb[:, 0], pb[:, 1])
+    vz_frac = rng.uniform(-0.3, 0.3, n)
+    vp = v * np.sqrt(1 - vz_frac ** 2)
+    pb[:, 2] = vp * (ux * np.cos(ang) - uy * np.sin(ang))
+    pb[:, 3] = vp * (ux * np.sin(ang) + uy * np.cos(ang))
+    pb[:, 4] = v * vz_frac
+    # keep only particles that cross within one step (at most ~a cell)
+    step_len = np.hypot(pb[:, 2], pb[:, 3]) * dtb
+    pb[:, 2:5] *= np.minimum(1.0, 0.8 * (0.04 / 63) / np.maximum(step_len, 1e-30))[:, None]
+    P = particles.Particles("electrons", "variableWeight")
+    P.setParticleData(pb.copy())
+    P.calcGridWeights(g)
+    P.eFieldToParticles(g, np.zeros(2 * g.getNpExt()))
+    P.borisPush(dtb, 0)
+    bd = particleBoundary.AbsorbElliptical(g, P)
+    bd.indexInside()
+    bd.saveAbsorbed()
+    bd.calculateInteractionPoint()
+    bd.calculateNormalVectors()
+    out["abs_rows"] = np.asarray(bd.getAbsorbedParticles()).copy()
+    out["abs_normals"] = np.asarray(bd.getNormalVectors()).copy()
+    cases = [("copper", -1.0, None), ("copper", 1.6, 300.0), ("stainless", 1.8, None)]
+    for k, (mat, sey, ehat) in enumerate(cases):
+        em = particleEmitter.FurmanEmitter(bd, P, material=mat, seyMax=sey)
+        if ehat is not None:
+            em.setEHat0(ehat)
+        randomGen.seed(1000 + k)
+        sec = np.asarray(em.generateSecondaries()).copy()
+        out[f"sec{k}"] = sec
+        out[f"case{k}"] = np.array([0 if mat == "copper" else 1, sey, ehat if ehat is not None else -1.0, 1000 + k])
+    # special functions of the reference (specFun.pyx) through the probe
+    A, B, Pq = [], [], []
+    for a in [0.3, 0.5, 0.9, 1.0, 1.5, 1.75, 2.5, 3.0, 7.5, 15.0, 34.5, 60.0]:
+        for b in [0.4, 0.5, 1.0, 1.5, 3.0, 8.5, 11.5, 40.0]:
+            for p in [1e-6, 0.003, 0.1, 0.37, 0.5, 0.81, 0.999]:
+                A.append(a); B.append(b); Pq.append(p)
+    A, B, Pq = np.array(A), np.array(B), np.array(Pq)
+    out["bii_a"], out["bii_b"], out["bii_p"] = A, B, Pq
+    out["bii"] = np.array([ref_probe.betaincinv(a, b, p) for a, b, p in zip(A, B, Pq)])
+    GA, GP = np.meshgrid([0.2, 0.7, 1.0, 1.5, 2.5, 4.7, 12.0, 34.5, 115.0], [1e-8, 1e-3, 0.05, 0.4, 0.9, 0.999999])
+    out["gii_a"], out["gii_p"] = GA.ravel(), GP.ravel()
+    out["gii"] = np.array([ref_probe.gammaincinv(a, p) for a, p in zip(GA.ravel(), GP.ravel())])
+    path = os.path.join(HERE, "emission.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "absorbed", len(out["abs_rows"]),
+          "secondaries", [len(out[f"sec{k}"]) for k in range(3)])
+
+
+if __name__ == "__main__" and "--emission" in sys.argv:
+    emission_golden()

@@ -11,7 +11,7 @@ def declared_symbols():
     for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
         text = open(h).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-        names.update(re.findall(r"\bint\s+(oec_\w+)\s*\(", text))
+        names.update(re.findall(r"\b(?:int|int64_t)\s+(oec_\w+)\s*\(", text))
     return sorted(names)
 
 
