@@ -67,12 +67,16 @@ class Particles:
             self._count = D.zeros(1, torch.int32)
             self._status = D.zeros(_lib.STATUS_WORDS, torch.int32)
             self._wscale = D.zeros(1, torch.float64)
-        self._mask = D.zeros(cap // 32, torch.int32)
+        mask = D.zeros(cap // 32, torch.int32)
+        if self._mask is not None:  # keep the absorbed bits across a regrowth
+            m = min(mask.shape[0], self._mask.shape[0])
+            mask[:m].copy_(self._mask[:m])
+        self._mask = mask
 
     def ensure_capacity(self, n):
         """Grow the device store (x1.5, like the reference's x1.1 regrowth) to hold n."""
         need = max(int(n), self._min_capacity)
-        if need > self._cap:
+        if need > self._cap or self._soa is None:
             self._alloc(max(need, int(self._cap * 1.5)))
 
     def c_particles(self):

@@ -260,3 +260,61 @@ def betaincinv(a, b, p):
 def gammaincinv(a, p):
     furman_emit(furman(), np.zeros((0, 6)), np.zeros((0, 2)))
     return lib().orc_gammaincinv(float(a), float(p))
+
+
+# ------------------------------------------------------------ management
+def _manage_declared():
+    L = lib()
+    if not getattr(L, "_manage_declared", False):
+        L.orc_quicksort_by_column.restype = None
+        L.orc_quicksort_by_column.argtypes = [_P, _I64, _I64, _I]
+        L.orc_global_random.restype = _I64
+        L.orc_global_random.argtypes = [_P, _I64, _I64, _P]
+        L.orc_local_random_ellipse.restype = _I64
+        L.orc_local_random_ellipse.argtypes = [_P, _I64, _I64, _I64, _D, _D, _D, _D, _I, _D, _D, _D, _I,
+                                               ctypes.c_uint, _P]
+        L.orc_add_and_remove.restype = _I64
+        L.orc_add_and_remove.argtypes = [_P, _I64, _I64, _P, _I64, _P]
+        L._manage_declared = True
+    return L
+
+
+def sort_by_column(pd, col=5, seed=None):
+    """sortByColumn (particles.pyx:49-50, :431-459) with the MT stream."""
+    L = _manage_declared()
+    if seed is not None:
+        L.orc_seed(int(seed))
+    a = np.array(pd, np.float64, copy=True, order="C")
+    L.orc_quicksort_by_column(_p(a), 0, a.shape[0] - 1, int(col))
+    return a
+
+
+def global_random(pd, target, seed=None):
+    """globalRandom (particleManagement.pyx:35-67) with the MT stream."""
+    L = _manage_declared()
+    if seed is not None:
+        L.orc_seed(int(seed))
+    n = pd.shape[0]
+    a = np.zeros((max(n, target), 6))
+    a[:n] = pd
+    scratch = np.zeros((max(target - n, 1), 6))
+    k = L.orc_global_random(_p(a), n, int(target), _p(scratch))
+    return a[:k].copy()
+
+
+def local_random(pd, target, g, kind=1, seed=None, threshold=2., lambda_factor=1., dis_limit=1., scheme=0,
+                 leaf=10):
+    """localRandom (particleManagement.pyx:74-238) with the MT stream; the
+    particle array starts with capacity n, as after setParticleData."""
+    L = _manage_declared()
+    if seed is not None:
+        L.orc_seed(int(seed))
+    n = pd.shape[0]
+    room = 2 * n + 10
+    a = np.zeros((room, 6))
+    a[:n] = pd
+    scratch = np.zeros((n + 10, 6))
+    k = L.orc_local_random_ellipse(_p(a), n, n, int(target), g.dx, g.dy, g.lx, g.ly, 1 if kind == 0 else 0,
+                                   float(threshold), float(lambda_factor), float(dis_limit), int(scheme),
+                                   int(leaf), _p(scratch))
+    return a[:k].copy()

@@ -257,3 +257,45 @@ def emission_golden():
 
 if __name__ == "__main__" and "--emission" in sys.argv:
     emission_golden()
+
+
+def management_golden():
+    """Reference sortByColumn, globalRandom and localRandom on seeded inputs."""
+    grid, particles, particleBoundary, poissonSolver, randomGen = _import_reference()
+    import particleManagement
+    rng = np.random.default_rng(99)
+    g = grid.Grid(64, 64, 0.04, 0.04, 1)
+    out = {}
+    n = 4000
+    pd = make_particles(rng, n, 0.04, 0.04, 1, 3e5)
+    pd[:, 5] = np.exp(rng.normal(0, 0.8, n)) * 1e5
+    out["pd"] = pd
+    # sortByColumn(5)
+    P = particles.Particles("electrons", "variableWeight")
+    P.setParticleData(pd.copy())
+    randomGen.seed(11)
+    P.sortByColumn(5)
+    out["sorted"] = np.asarray(P.getParticleData()).copy()
+    # globalRandom: kill and clone
+    for tag, target in [("kill", 3100), ("clone", 5200)]:
+        P = particles.Particles("electrons", "variableWeight")
+        P.setParticleData(pd.copy())
+        randomGen.seed(21)
+        particleManagement.globalRandom(g, P, target)
+        out[f"global_{tag}"] = np.asarray(P.getParticleData()).copy()
+    # localRandom (merge + split), ellipse boundary, both merge schemes
+    for scheme in (0, 1):
+        for tag, target in [("down", 3000), ("up", 4600)]:
+            P = particles.Particles("electrons", "variableWeight")
+            P.setParticleData(pd.copy())
+            bd = particleBoundary.AbsorbElliptical(g, P)
+            randomGen.seed(31 + scheme)
+            particleManagement.localRandom(g, P, bd, target, mergeScheme=scheme)
+            out[f"local{scheme}_{tag}"] = np.asarray(P.getParticleData()).copy()
+    path = os.path.join(HERE, "management.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), {k: v.shape for k, v in out.items()})
+
+
+if __name__ == "__main__" and "--management" in sys.argv:
+    management_golden()
