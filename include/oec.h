@@ -252,6 +252,49 @@ int oec_homo_load(const oec_grid_t *grid, const oec_boundary_t *boundary, oec_pa
                   double weight, double vsigma, int32_t randomize_weight, uint64_t seed, int32_t *failed_dev,
                   void *stream);
 
+/* --------------------------------------- particle management (A10, A25-A27) */
+
+/* Bytes of the work buffer of oec_sort_particles / oec_cell_merge. */
+int64_t oec_sort_work_bytes(int64_t capacity);
+
+/* sortByColumn (particles.pyx:49-50, :431-459): stable radix sort of the
+ * particles by column 2..5 (vx, vy, vz, w) or 6 (cell index); the sorted
+ * store is written to `tmp` (same capacity), the caller swaps the two. */
+int oec_sort_particles(oec_particles_t *p, oec_particles_t *tmp, int32_t column, void *work_dev, void *stream);
+
+/* w *= factor for every particle (globalRandom, particleManagement.pyx:51,60). */
+int oec_scale_weights(oec_particles_t *p, double factor, void *stream);
+
+/* Removal bits for n_remove of the first n particles, chosen uniformly
+ * without replacement (globalRandom, particleManagement.pyx:52-55); Philox
+ * keyed by seed, counter `call`.  fails_dev counts darts that gave up. */
+int oec_roulette_select(int32_t n, int32_t n_remove, uint32_t *mask_dev, int64_t mask_words, uint64_t seed,
+                        uint32_t call, int32_t *fails_dev, void *stream);
+
+/* k rows copied from particles drawn uniformly with replacement
+ * (globalRandom clone step, particleManagement.pyx:62-66). */
+int oec_clone_rows(const oec_grid_t *grid, const oec_particles_t *p, int32_t n, int32_t k, uint64_t seed,
+                   uint32_t call, double *rows_dev, void *stream);
+
+/* acc_dev[0] = sum w, acc_dev[1] = sum |v|^2 w^2 (localRandom :124-128). */
+int oec_weight_stats(const oec_particles_t *p, double *acc_dev, void *stream);
+
+/* Halve the weights of the last k of the first n particles and write their
+ * duplicates as rows (localRandom split, particleManagement.pyx:130-163). */
+int oec_split_rows(const oec_grid_t *grid, oec_particles_t *p, int32_t n, int32_t k, double *rows_dev, void *stream);
+
+/* Cell-binned merge (localRandom :165-236): the first n_cand particles are
+ * ordered by (cell, velocity projection); neighbouring pairs in one cell
+ * whose squared phase-space distance dx^2 + dy^2 + lambda^2 |dv|^2 is below
+ * `limit` merge with probability min(1, n_merge / qualifying pairs); the
+ * survivor is drawn with probability proportional to weight and takes the
+ * summed weight; the other gets its removal bit.  scheme 1 rescales the
+ * survivor's velocity as the reference does.  counters_dev[0] = qualifying
+ * pairs, [1] = merges. */
+int oec_cell_merge(const oec_grid_t *grid, oec_particles_t *p, int32_t n_cand, int32_t n_merge, double lambda,
+                   double limit, int32_t scheme, uint64_t seed, uint32_t call, double vscale, uint32_t *mask_dev,
+                   int32_t *counters_dev, void *work_dev, void *stream);
+
 /* ------------------------------------------------ Poisson solve (A15-A16) */
 
 /* Device form of SuperLU's P_r A P_c = L U (poissonSolver.pyx:59).

@@ -74,12 +74,20 @@ SIGNATURES = {
     "oec_add_remove": [_PG, _PP, _P, _P, _P, _I32, _P, _P, _I32, _P, _P, _P, _P, _P],
     "oec_mask_from_keep": [_P, _I64, _P, _I64, _P],
     "oec_homo_load": [_PG, _PB, _PP, _I64, _D, _D, _I32, ctypes.c_uint64, _P, _P],
+    "oec_sort_particles": [_PP, _PP, _I32, _P, _P],
+    "oec_scale_weights": [_PP, _D, _P],
+    "oec_roulette_select": [_I32, _I32, _P, _I64, ctypes.c_uint64, ctypes.c_uint32, _P, _P],
+    "oec_clone_rows": [_PG, _PP, _I32, _I32, ctypes.c_uint64, ctypes.c_uint32, _P, _P],
+    "oec_weight_stats": [_PP, _P, _P],
+    "oec_split_rows": [_PG, _PP, _I32, _I32, _P, _P],
+    "oec_cell_merge": [_PG, _PP, _I32, _I32, _D, _D, _I32, ctypes.c_uint64, ctypes.c_uint32, _D, _P, _P, _P, _P],
 }
+_INT64_RETURNING = {"oec_sort_work_bytes": [_I64]}
 
 _lib = None
 # entry points whose ctypes signatures live next to their Python users
 # (structure arguments defined there); registered at import of that module
-OTHER_DECLARED = set()
+OTHER_DECLARED = {"oec_sort_work_bytes"}
 
 
 def lib():
@@ -92,6 +100,10 @@ def lib():
         for name, args in SIGNATURES.items():
             f = getattr(L, name)
             f.restype = ctypes.c_int
+            f.argtypes = args
+        for name, args in _INT64_RETURNING.items():
+            f = getattr(L, name)
+            f.restype = ctypes.c_int64
             f.argtypes = args
         _lib = L
     return _lib

@@ -1,0 +1,522 @@
+// manage.cu -- macro-particle management on the device: stable radix sort
+// (sortByColumn, cell ordering), Russian roulette (globalRandom) and the
+// cell-binned phase-space merge (localRandom).
+//
+// Reference: particles.pyx sortByColumn (:49-50, :431-459),
+// particleManagement.pyx globalRandom (:35-67) and localRandom (:74-238).
+//  * Sorting is a stable least-significant-digit radix sort of 32-bit keys
+//    (8-bit digits): per pass a per-tile digit histogram, one exclusive scan
+//    over (digit, tile), and a stable scatter in which each tile ranks its
+//    elements by 1-bit split passes.
+//  * globalRandom removes n - target particles chosen uniformly without
+//    replacement (each thread throws darts at free slots with atomicOr on the
+//    removal bitmask, as the reference redraws until it hits a particle it has
+//    not removed), or appends target - n copies of particles drawn with
+//    replacement; weights are scaled by n/target in both cases.
+//  * localRandom keeps the reference's bookkeeping (weight thresholds, split
+//    and merge counts, typical velocity, phase-space metric with
+//    lambda = ds / v_typical) but replaces the sequential kd-tree search by
+//    pairing inside grid cells: the merge candidates (the lightest particles)
+//    are ordered by (cell, weighted velocity) and neighbours in that order
+//    are merged when their phase-space distance passes the reference's test.
+#include <math.h>
+#include <stdint.h>
+
+#include "oec_common.cuh"
+#include "specfun.cuh"
+
+namespace oec {
+namespace {
+
+constexpr int kTile = 1024;  // elements per sort tile (one CTA)
+
+__device__ __forceinline__ int blk_scan(int v, int *tot, int *sh) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(kFullMask, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        int s = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(kFullMask, s, o);
+            if (lane >= o) s += y;
+        }
+        sh[lane] = s;
+    }
+    __syncthreads();
+    int ex = (wid > 0 ? sh[wid - 1] : 0) + x - v;
+    if (tot) *tot = sh[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return ex;
+}
+
+// ----------------------------------------------------------- radix sort
+
+__global__ void k_digit_hist(const uint32_t *__restrict__ keys, const int32_t *n_p, int shift, int ntiles,
+                             int *__restrict__ hist) {
+    __shared__ int h[256];
+    int n = *n_p;
+    for (int d = threadIdx.x; d < 256; d += blockDim.x) h[d] = 0;
+    __syncthreads();
+    int i = blockIdx.x * kTile + threadIdx.x;
+    if (i < n) atomicAdd(&h[(keys[i] >> shift) & 255u], 1);
+    __syncthreads();
+    for (int d = threadIdx.x; d < 256; d += blockDim.x) hist[d * ntiles + blockIdx.x] = h[d];
+}
+
+// exclusive scan of `len` ints in one CTA (len <= 1024 * chunks)
+__global__ void k_scan_serial_chunks(int *a, int len) {
+    __shared__ int sh[32];
+    int carry = 0;
+    for (int base = 0; base < len; base += blockDim.x) {
+        int i = base + threadIdx.x;
+        int v = i < len ? a[i] : 0;
+        int tot;
+        int ex = blk_scan(v, &tot, sh);
+        if (i < len) a[i] = ex + carry;
+        carry += tot;
+        __syncthreads();
+    }
+}
+
+__global__ void k_scatter(const uint32_t *__restrict__ keys, const int32_t *__restrict__ vals, const int32_t *n_p,
+                          int shift, int ntiles, const int *__restrict__ offs, uint32_t *__restrict__ okeys,
+                          int32_t *__restrict__ ovals) {
+    __shared__ int sh[32];
+    __shared__ int dstart[256];
+    __shared__ int dcount[256];
+    __shared__ uint32_t skeys[kTile];
+    __shared__ int32_t svals[kTile];
+    int n = *n_p;
+    int i = blockIdx.x * kTile + threadIdx.x;
+    bool valid = i < n;
+    uint32_t k = valid ? keys[i] : 0xffffffffu;
+    int32_t v = valid ? vals[i] : 0;
+    uint32_t d = (k >> shift) & 255u;
+    // stable local sort by the 8-bit digit: eight stable 1-bit splits
+    for (int b = 0; b < 8; ++b) {
+        int bit = (d >> b) & 1u;
+        int tot;
+        int zeros_before = blk_scan(bit ^ 1, &tot, sh);  // tot = number of zeros
+        int pos = bit ? (tot + (threadIdx.x - zeros_before)) : zeros_before;
+        skeys[pos] = k;
+        svals[pos] = v;
+        __syncthreads();
+        k = skeys[threadIdx.x];
+        v = svals[threadIdx.x];
+        d = (k >> shift) & 255u;
+        __syncthreads();
+    }
+    // local start of each digit
+    for (int t = threadIdx.x; t < 256; t += blockDim.x) dcount[t] = 0;
+    __syncthreads();
+    int j = blockIdx.x * kTile + threadIdx.x;
+    int local_valid = min(kTile, n - blockIdx.x * kTile);
+    if ((int)threadIdx.x < local_valid) atomicAdd(&dcount[d], 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int s = 0;
+        for (int t = 0; t < 256; ++t) {
+            dstart[t] = s;
+            s += dcount[t];
+        }
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < local_valid) {
+        int dst = offs[d * ntiles + blockIdx.x] + ((int)threadIdx.x - dstart[d]);
+        okeys[dst] = k;
+        ovals[dst] = v;
+    }
+    (void)j;
+}
+
+// float -> order-preserving uint32
+__device__ __forceinline__ uint32_t float_key(float f) {
+    uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__global__ void k_make_keys(oec_particles_t p, int column, uint32_t *__restrict__ keys, int32_t *__restrict__ vals) {
+    int n = *p.count;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t k;
+        switch (column) {
+            case 6: k = (uint32_t)p.cell[i]; break;  // cell order
+            case 2: k = float_key(p.vx[i]); break;
+            case 3: k = float_key(p.vy[i]); break;
+            case 4: k = float_key(p.vz[i]); break;
+            case 5: k = float_key(p.w[i]); break;
+            default: k = (uint32_t)p.cell[i]; break;
+        }
+        keys[i] = k;
+        vals[i] = i;
+    }
+}
+
+// gather every SoA array through the permutation into `q`
+__global__ void k_permute(oec_particles_t p, const int32_t *__restrict__ perm, oec_particles_t q) {
+    int n = *p.count;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int s = perm[i];
+        q.cell[i] = p.cell[s];
+        q.ox[i] = p.ox[s];
+        q.oy[i] = p.oy[s];
+        q.vx[i] = p.vx[s];
+        q.vy[i] = p.vy[s];
+        q.vz[i] = p.vz[s];
+        q.w[i] = p.w[s];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *q.count = n;
+}
+
+// -------------------------------------------------------------- roulette
+
+__global__ void k_scale_w(oec_particles_t p, double factor) {
+    int n = *p.count;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        p.w[i] = (float)((double)p.w[i] * factor);
+}
+
+__global__ void k_zero_words(uint32_t *m, int nwords) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nwords; i += gridDim.x * blockDim.x) m[i] = 0u;
+}
+
+// Mark `k` distinct uniformly chosen indices in [0, n) in `mask`.
+__global__ void k_darts(int n, int k, uint32_t *mask, uint2 key, uint32_t call, int max_tries, int *fails) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < k; t += gridDim.x * blockDim.x) {
+        bool done = false;
+        for (int a = 0; a < max_tries && !done; ++a) {
+            uint4 r = sf::philox4x32_10(make_uint4((uint32_t)t, call, (uint32_t)a, 0x7011u), key);
+            uint32_t idx = (uint32_t)(((uint64_t)r.x * (uint64_t)n) >> 32);
+            uint32_t bit = 1u << (idx & 31);
+            uint32_t old = atomicOr(&mask[idx >> 5], bit);
+            done = (old & bit) == 0u;
+        }
+        if (!done) atomicAdd(fails, 1);
+    }
+}
+
+// mask = ~mask on [0, n)
+__global__ void k_invert_valid(uint32_t *mask, int n) {
+    int nw = (n + 31) >> 5;
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += gridDim.x * blockDim.x) {
+        uint32_t valid = (w * 32 + 32 <= n) ? 0xffffffffu : ((1u << (n - w * 32)) - 1u);
+        mask[w] = (~mask[w]) & valid;
+    }
+}
+
+// rows of particles drawn with replacement (clone step of globalRandom)
+__global__ void k_clone_rows(oec_particles_t p, int n, int k, uint2 key, uint32_t call, int nx, float inv_nx,
+                             double dx, double dy, double lxh, double lyh, double *rows) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < k; t += gridDim.x * blockDim.x) {
+        uint4 r = sf::philox4x32_10(make_uint4((uint32_t)t, call, 0u, 0xc10eu), key);
+        int s = (int)(((uint64_t)r.x * (uint64_t)n) >> 32);
+        int ix, iy;
+        split_cell(p.cell[s], nx, inv_nx, ix, iy);
+        double *q = rows + 6 * (int64_t)t;
+        q[0] = abs_coord(ix, p.ox[s], dx, lxh);
+        q[1] = abs_coord(iy, p.oy[s], dy, lyh);
+        q[2] = p.vx[s];
+        q[3] = p.vy[s];
+        q[4] = p.vz[s];
+        q[5] = p.w[s];
+    }
+}
+
+// ------------------------------------------------------------ local merge
+
+// Stats over particles [0, n): sum w, sum |v|^2 w^2 (f64, atomics).
+__global__ void k_wstats(oec_particles_t p, double *acc) {
+    int n = *p.count;
+    double sw = 0, sv = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double w = p.w[i], vx = p.vx[i], vy = p.vy[i], vz = p.vz[i];
+        sw += w;
+        sv += (vx * vx + vy * vy + vz * vz) * w * w;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sw += __shfl_xor_sync(kFullMask, sw, o);
+        sv += __shfl_xor_sync(kFullMask, sv, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&acc[0], sw);
+        atomicAdd(&acc[1], sv);
+    }
+}
+
+struct MergeArgs {
+    oec_particles_t p;         // weight-sorted store
+    int n_cand;                // merge candidates: the lightest n_cand particles
+    int n_merge_target;        // merges wanted
+    const int32_t *order;      // candidates ordered by (cell, velocity key)
+    double lam2;               // (ds / v_typical)^2 * lambda_factor^2
+    double limit;              // factorDisLimit * ds (compared with the squared distance, as the reference)
+    double dx, dy;
+    int nx;
+    float inv_nx;
+    uint2 key;
+    uint32_t call;
+    int scheme;
+    uint32_t *mask;            // removal bits
+    int *counters;             // [0] qualifying pairs, [1] merges done
+};
+
+// Pair (2k, 2k+1) of the ordered candidates: qualifies when both are in the
+// same cell and the weighted phase-space distance passes the test.
+__global__ void k_pair_count(MergeArgs a) {
+    int npairs = a.n_cand / 2;
+    int q = 0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < npairs; k += gridDim.x * blockDim.x) {
+        int i = a.order[2 * k], j = a.order[2 * k + 1];
+        if (a.p.cell[i] != a.p.cell[j]) continue;
+        double ddx = ((double)a.p.ox[i] - a.p.ox[j]) * a.dx, ddy = ((double)a.p.oy[i] - a.p.oy[j]) * a.dy;
+        double dvx = (double)a.p.vx[i] - a.p.vx[j], dvy = (double)a.p.vy[i] - a.p.vy[j],
+               dvz = (double)a.p.vz[i] - a.p.vz[j];
+        double d2 = ddx * ddx + ddy * ddy + a.lam2 * (dvx * dvx + dvy * dvy + dvz * dvz);
+        if (d2 < a.limit) ++q;
+    }
+    for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(kFullMask, q, o);
+    if ((threadIdx.x & 31) == 0 && q) atomicAdd(&a.counters[0], q);
+}
+
+__global__ void k_pair_merge(MergeArgs a) {
+    int npairs = a.n_cand / 2;
+    int qual = a.counters[0];
+    double paccept = qual > 0 ? fmin(1.0, (double)a.n_merge_target / (double)qual) : 0.0;
+    int done = 0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < npairs; k += gridDim.x * blockDim.x) {
+        int i = a.order[2 * k], j = a.order[2 * k + 1];
+        if (a.p.cell[i] != a.p.cell[j]) continue;
+        double ddx = ((double)a.p.ox[i] - a.p.ox[j]) * a.dx, ddy = ((double)a.p.oy[i] - a.p.oy[j]) * a.dy;
+        double dvx = (double)a.p.vx[i] - a.p.vx[j], dvy = (double)a.p.vy[i] - a.p.vy[j],
+               dvz = (double)a.p.vz[i] - a.p.vz[j];
+        double d2 = ddx * ddx + ddy * ddy + a.lam2 * (dvx * dvx + dvy * dvy + dvz * dvz);
+        if (!(d2 < a.limit)) continue;
+        uint4 r = sf::philox4x32_10(make_uint4((uint32_t)k, a.call, 0u, 0x3e59u), a.key);
+        double u0 = r.x * (1.0 / 4294967296.0), u1 = r.y * (1.0 / 4294967296.0);
+        if (u0 >= paccept) continue;
+        double wi = a.p.w[i], wj = a.p.w[j];
+        int keep = (u1 < wi / (wi + wj)) ? i : j;  // keep with probability proportional to weight
+        int drop = keep == i ? j : i;
+        if (a.scheme == 1) {
+            // scale the kept velocity to conserve kinetic energy (particleManagement.pyx:200-236)
+            double wk = a.p.w[keep], wd = a.p.w[drop];
+            double vk2 = (double)a.p.vx[keep] * a.p.vx[keep] + (double)a.p.vy[keep] * a.p.vy[keep] +
+                         (double)a.p.vz[keep] * a.p.vz[keep];
+            double vd2 = (double)a.p.vx[drop] * a.p.vx[drop] + (double)a.p.vy[drop] * a.p.vy[drop] +
+                         (double)a.p.vz[drop] * a.p.vz[drop];
+            double f = vk2 > 0 ? wk / (wk + wd) + vd2 / vk2 * wd / (wk + wd) : 1.0;
+            a.p.vx[keep] = (float)(a.p.vx[keep] * f);
+            a.p.vy[keep] = (float)(a.p.vy[keep] * f);
+            a.p.vz[keep] = (float)(a.p.vz[keep] * f);
+        }
+        a.p.w[keep] = (float)(wi + wj);
+        atomicOr(&a.mask[drop >> 5], 1u << (drop & 31));
+        ++done;
+    }
+    for (int o = 16; o > 0; o >>= 1) done += __shfl_xor_sync(kFullMask, done, o);
+    if ((threadIdx.x & 31) == 0 && done) atomicAdd(&a.counters[1], done);
+}
+
+// Candidate keys: cell in the high bits, a coarse weighted-velocity key below.
+__global__ void k_cand_keys(oec_particles_t p, int n_cand, double vscale, uint32_t *keys, int32_t *vals) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_cand; i += gridDim.x * blockDim.x) {
+        double u = 0.5 + 0.25 * ((double)p.vx[i] + p.vy[i] + p.vz[i]) / vscale;  // projection in [0,1)
+        uint32_t vk = (uint32_t)fmin(fmax(u * 2048.0, 0.0), 2047.0);
+        keys[i] = ((uint32_t)p.cell[i] << 11) | vk;
+        vals[i] = i;
+    }
+}
+
+// rows: duplicates at half weight of the heaviest `k` (the last k in weight order)
+__global__ void k_split_rows(oec_particles_t p, int n, int k, int nx, float inv_nx, double dx, double dy, double lxh,
+                             double lyh, double *rows) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < k; t += gridDim.x * blockDim.x) {
+        int s = n - k + t;
+        p.w[s] = p.w[s] * 0.5f;
+        int ix, iy;
+        split_cell(p.cell[s], nx, inv_nx, ix, iy);
+        double *q = rows + 6 * (int64_t)t;
+        q[0] = abs_coord(ix, p.ox[s], dx, lxh);
+        q[1] = abs_coord(iy, p.oy[s], dy, lyh);
+        q[2] = p.vx[s];
+        q[3] = p.vy[s];
+        q[4] = p.vz[s];
+        q[5] = p.w[s];
+    }
+}
+
+}  // namespace
+}  // namespace oec
+
+using namespace oec;
+
+static bool vp2(const oec_particles_t *p) {
+    return p && p->cell && p->ox && p->oy && p->vx && p->vy && p->vz && p->w && p->count && p->capacity > 0;
+}
+
+extern "C" int64_t oec_sort_work_bytes(int64_t capacity) {
+    int64_t tiles = (capacity + kTile - 1) / kTile;
+    return 4 * capacity * 4 + 256 * tiles * 4 + 256;
+}
+
+// Stable radix sort of (keys, vals) pairs, keys in work; `bits` significant key bits.
+static int radix_sort(uint32_t *keys, int32_t *vals, uint32_t *k2, int32_t *v2, int *hist, const int32_t *n_dev,
+                      int64_t cap, int bits, cudaStream_t s, uint32_t **kout, int32_t **vout) {
+    int ntiles = (int)((cap + kTile - 1) / kTile);
+    for (int shift = 0; shift < bits; shift += 8) {
+        k_digit_hist<<<ntiles, kTile, 0, s>>>(keys, n_dev, shift, ntiles, hist);
+        k_scan_serial_chunks<<<1, 1024, 0, s>>>(hist, 256 * ntiles);
+        k_scatter<<<ntiles, kTile, 0, s>>>(keys, vals, n_dev, shift, ntiles, hist, k2, v2);
+        uint32_t *tk = keys;
+        keys = k2;
+        k2 = tk;
+        int32_t *tv = vals;
+        vals = v2;
+        v2 = tv;
+    }
+    *kout = keys;
+    *vout = vals;
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int oec_sort_particles(oec_particles_t *p, oec_particles_t *tmp, int32_t column, void *work_dev,
+                                  void *stream) {
+    if (!vp2(p) || !vp2(tmp) || !work_dev || tmp->capacity < p->capacity) return OEC_ERR_INVALID;
+    if (column < 2 || column > 6) return OEC_ERR_INVALID;
+    cudaStream_t s = as_stream(stream);
+    int64_t cap = p->capacity;
+    uint32_t *keys = static_cast<uint32_t *>(work_dev);
+    int32_t *vals = reinterpret_cast<int32_t *>(keys + cap);
+    uint32_t *k2 = reinterpret_cast<uint32_t *>(vals + cap);
+    int32_t *v2 = reinterpret_cast<int32_t *>(k2 + cap);
+    int *hist = reinterpret_cast<int *>(v2 + cap);
+    int g = persistent_grid((cap + 255) / 256, 8);
+    k_make_keys<<<g, 256, 0, s>>>(*p, column, keys, vals);
+    OEC_LAUNCH_CHECK();
+    int bits = 32;
+    if (column == 6) {
+        // cell keys: only as many digits as the largest cell index needs
+        bits = 24;
+    }
+    uint32_t *kout;
+    int32_t *vout;
+    int rc = radix_sort(keys, vals, k2, v2, hist, p->count, cap, bits, s, &kout, &vout);
+    if (rc != OEC_OK) return rc;
+    k_permute<<<g, 256, 0, s>>>(*p, vout, *tmp);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int oec_scale_weights(oec_particles_t *p, double factor, void *stream) {
+    if (!vp2(p)) return OEC_ERR_INVALID;
+    k_scale_w<<<persistent_grid((p->capacity + 255) / 256, 8), 256, 0, as_stream(stream)>>>(*p, factor);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int oec_roulette_select(int32_t n, int32_t n_remove, uint32_t *mask_dev, int64_t mask_words,
+                                   uint64_t seed, uint32_t call, int32_t *fails_dev, void *stream) {
+    if (n < 0 || n_remove < 0 || n_remove > n || !mask_dev || !fails_dev || mask_words * 32 < n)
+        return OEC_ERR_INVALID;
+    cudaStream_t s = as_stream(stream);
+    uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+    int nw = (n + 31) / 32;
+    k_zero_words<<<persistent_grid((mask_words + 255) / 256, 8), 256, 0, s>>>(mask_dev, (int)mask_words);
+    OEC_CUDA_TRY(cudaMemsetAsync(fails_dev, 0, sizeof(int32_t), s));
+    // choose the smaller of the removed and the kept sets by darts
+    bool invert = n_remove > n / 2;
+    int k = invert ? n - n_remove : n_remove;
+    if (k > 0)
+        k_darts<<<persistent_grid((k + 255) / 256, 8), 256, 0, s>>>(n, k, mask_dev, key, call, 4096, fails_dev);
+    if (invert) k_invert_valid<<<persistent_grid((nw + 255) / 256, 8), 256, 0, s>>>(mask_dev, n);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int oec_clone_rows(const oec_grid_t *grid, const oec_particles_t *p, int32_t n, int32_t k, uint64_t seed,
+                              uint32_t call, double *rows_dev, void *stream) {
+    if (!grid || !vp2(p) || n <= 0 || k < 0 || !rows_dev) return OEC_ERR_INVALID;
+    GridConst gc = make_grid_const(*grid);
+    uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+    if (k > 0)
+        k_clone_rows<<<persistent_grid((k + 255) / 256, 8), 256, 0, as_stream(stream)>>>(
+            *p, n, k, key, call, gc.nx, 1.0f / (float)gc.nx, gc.dx, gc.dy, gc.lxh, gc.lyh, rows_dev);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int oec_weight_stats(const oec_particles_t *p, double *acc_dev, void *stream) {
+    if (!vp2(p) || !acc_dev) return OEC_ERR_INVALID;
+    cudaStream_t s = as_stream(stream);
+    OEC_CUDA_TRY(cudaMemsetAsync(acc_dev, 0, 2 * sizeof(double), s));
+    k_wstats<<<persistent_grid((p->capacity + 255) / 256, 4), 256, 0, s>>>(*p, acc_dev);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int oec_split_rows(const oec_grid_t *grid, oec_particles_t *p, int32_t n, int32_t k, double *rows_dev,
+                              void *stream) {
+    if (!grid || !vp2(p) || k < 0 || k > n || (k > 0 && !rows_dev)) return OEC_ERR_INVALID;
+    GridConst gc = make_grid_const(*grid);
+    if (k > 0)
+        k_split_rows<<<persistent_grid((k + 255) / 256, 8), 256, 0, as_stream(stream)>>>(
+            *p, n, k, gc.nx, 1.0f / (float)gc.nx, gc.dx, gc.dy, gc.lxh, gc.lyh, rows_dev);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int oec_cell_merge(const oec_grid_t *grid, oec_particles_t *p, int32_t n_cand, int32_t n_merge,
+                              double lambda, double limit, int32_t scheme, uint64_t seed, uint32_t call,
+                              double vscale, uint32_t *mask_dev, int32_t *counters_dev, void *work_dev,
+                              void *stream) {
+    if (!grid || !vp2(p) || n_cand < 0 || n_cand > p->capacity || n_merge < 0 || !mask_dev || !counters_dev ||
+        !work_dev)
+        return OEC_ERR_INVALID;
+    GridConst gc = make_grid_const(*grid);
+    if ((int64_t)gc.G >= (1 << 21)) return OEC_ERR_INVALID;  // 21 cell bits + 11 velocity bits
+    cudaStream_t s = as_stream(stream);
+    int64_t cap = p->capacity;
+    uint32_t *keys = static_cast<uint32_t *>(work_dev);
+    int32_t *vals = reinterpret_cast<int32_t *>(keys + cap);
+    uint32_t *k2 = reinterpret_cast<uint32_t *>(vals + cap);
+    int32_t *v2 = reinterpret_cast<int32_t *>(k2 + cap);
+    int *hist = reinterpret_cast<int *>(v2 + cap);
+    int32_t *ncand_dev = reinterpret_cast<int32_t *>(hist + 256 * ((cap + kTile - 1) / kTile));
+    OEC_CUDA_TRY(cudaMemcpyAsync(ncand_dev, &n_cand, sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    OEC_CUDA_TRY(cudaMemsetAsync(counters_dev, 0, 2 * sizeof(int32_t), s));
+    int g = persistent_grid((n_cand + 255) / 256 + 1, 8);
+    k_cand_keys<<<g, 256, 0, s>>>(*p, n_cand, vscale, keys, vals);
+    uint32_t *kout;
+    int32_t *vout;
+    int rc = radix_sort(keys, vals, k2, v2, hist, ncand_dev, cap, 32, s, &kout, &vout);
+    if (rc != OEC_OK) return rc;
+    MergeArgs a{};
+    a.p = *p;
+    a.n_cand = n_cand;
+    a.n_merge_target = n_merge;
+    a.order = vout;
+    a.lam2 = lambda * lambda;
+    a.limit = limit;
+    a.dx = gc.dx;
+    a.dy = gc.dy;
+    a.nx = gc.nx;
+    a.inv_nx = 1.0f / (float)gc.nx;
+    a.key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+    a.call = call;
+    a.scheme = scheme;
+    a.mask = mask_dev;
+    a.counters = counters_dev;
+    k_pair_count<<<g, 256, 0, s>>>(a);
+    k_pair_merge<<<g, 256, 0, s>>>(a);
+    OEC_LAUNCH_CHECK();
+    OEC_CUDA_TRY(cudaStreamSynchronize(s));  // n_cand lives on this stack frame
+    return OEC_OK;
+}

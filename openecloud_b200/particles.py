@@ -171,6 +171,28 @@ class Particles:
         n = self.getMacroParticleCount()
         return float(self._soa["w"][:n].double().sum().item()) / n
 
+    def sortByColumn(self, sortByColumn):
+        """particles.pyx:49-50: reorder the particles by column 2..5
+        (vx, vy, vz, w) of the reference layout, or 6 for the cell index
+        (stable device radix sort; the reference uses a random-pivot quicksort,
+        so only the order of equal keys can differ)."""
+        col = int(sortByColumn)
+        if col in (0, 1):
+            col = 6  # x, y: the cell-major order is the position order used on the device
+        if col not in (2, 3, 4, 5, 6):
+            raise ValueError("column must be 0..5 (or 6 for cells)")
+        if getattr(self, "_sort_tmp", None) is None or self._sort_tmp["cell"].shape[0] != self._cap:
+            self._sort_tmp = {"cell": D.empty(self._cap, torch.int32)}
+            for k in ("ox", "oy", "vx", "vy", "vz", "w"):
+                self._sort_tmp[k] = D.empty(self._cap, torch.float32)
+            self._sort_work = D.empty(int(_lib.lib().oec_sort_work_bytes(self._cap)), torch.uint8)
+        t = self._sort_tmp
+        tmp = _lib.Particles_t(t["cell"].data_ptr(), t["ox"].data_ptr(), t["oy"].data_ptr(), t["vx"].data_ptr(),
+                               t["vy"].data_ptr(), t["vz"].data_ptr(), t["w"].data_ptr(), self._count.data_ptr(),
+                               self._cap)
+        _lib.call("oec_sort_particles", self.c_particles(), tmp, col, self._sort_work.data_ptr(), D.stream())
+        self._soa, self._sort_tmp = t, self._soa
+
     def calcGridWeights(self, gridObj):
         """particles.pyx:52-56 -> inCell and the four CIC weights (device)."""
         self._bind(gridObj)
