@@ -236,14 +236,16 @@ int64_t oec_furman_work_bytes(int32_t cap);
 /* generateSecondaries (particleEmitter.pyx:154-308) on the absorbed rows at
  * the wall (after oec_wall_interaction) with their normals.  Secondaries are
  * written as (n_out, 6) f64 rows, grouped by absorbed row in order.  Random
- * draws: Philox4x32-10 keyed by `seed`, counter (ids[i] or i, step, draw);
+ * draws: Philox4x32-10 keyed by `seed`, counter (ids[i] or i, step + *step_dev
+ * (when step_dev != NULL: the device step counter of a replayed graph), draw);
  * with replay_uniforms_dev != NULL the uniforms are read from it instead
  * (32 per absorbed row: draw 0 selects the secondary count, the rest are
  * consumed in the reference's order; a normal deviate takes two). */
 int oec_furman_emit(const oec_furman_t *params, const double *rows_dev, const double *normals_dev,
                     const int32_t *n_abs_dev, int32_t cap, const int32_t *ids_dev, uint64_t seed, uint32_t step,
-                    const double *replay_uniforms_dev, void *work_dev, double *out_rows_dev, int32_t out_cap,
-                    int32_t *n_out_dev, oec_status_t *status_dev, void *stream);
+                    const int32_t *step_dev, const double *replay_uniforms_dev, void *work_dev,
+                    double *out_rows_dev, int32_t out_cap, int32_t *n_out_dev, oec_status_t *status_dev,
+                    void *stream);
 
 /* homoLoader (particleEmitter.pyx:41-72): n particles uniform inside the
  * boundary by rejection sampling, velocities N(0, vsigma), weight w0
@@ -251,6 +253,22 @@ int oec_furman_emit(const oec_furman_t *params, const double *rows_dev, const do
 int oec_homo_load(const oec_grid_t *grid, const oec_boundary_t *boundary, oec_particles_t *p, int64_t n,
                   double weight, double vsigma, int32_t randomize_weight, uint64_t seed, int32_t *failed_dev,
                   void *stream);
+
+/* ---------------------------------------- time-loop kernels (A28, histories) */
+
+/* Poisson right-hand side of step *step_dev: electron charge from the
+ * fixed-point deposit plus the beam imprint table[*step]*profile
+ * (example01_basic.py:81, beam.py:68-78); profile/table may be NULL. */
+int oec_rhs_with_beam(const oec_grid_t *grid, const int64_t *rho_fix_dev, const double *wscale_dev,
+                      double particle_charge, const double *profile_dev, const double *table_dev,
+                      const int32_t *step_dev, int32_t table_len, double *rho_dev, void *stream);
+
+/* hist_w[*step] = sum w, hist_n[*step] = count (example01_basic.py:56-57). */
+int oec_history(const oec_particles_t *p, int32_t *step_dev, int32_t hist_len, double *hist_w_dev,
+                int32_t *hist_n_dev, double *scratch_dev, void *stream);
+
+/* ++*step_dev (keeps the step index on the device for graph replay). */
+int oec_step_advance(int32_t *step_dev, void *stream);
 
 /* --------------------------------------- particle management (A10, A25-A27) */
 
@@ -284,8 +302,8 @@ int oec_weight_stats(const oec_particles_t *p, double *acc_dev, void *stream);
 int oec_split_rows(const oec_grid_t *grid, oec_particles_t *p, int32_t n, int32_t k, double *rows_dev, void *stream);
 
 /* Cell-binned merge (localRandom :165-236): the first n_cand particles are
- * ordered by (cell, velocity projection); neighbouring pairs in one cell
- * whose squared phase-space distance dx^2 + dy^2 + lambda^2 |dv|^2 is below
+ * ordered by (Morton index of the cell, velocity projection); neighbouring
+ * pairs whose squared phase-space distance dx^2 + dy^2 + lambda^2 |dv|^2 is below
  * `limit` merge with probability min(1, n_merge / qualifying pairs); the
  * survivor is drawn with probability proportional to weight and takes the
  * summed weight; the other gets its removal bit.  scheme 1 rescales the

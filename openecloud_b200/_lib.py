@@ -81,6 +81,9 @@ SIGNATURES = {
     "oec_weight_stats": [_PP, _P, _P],
     "oec_split_rows": [_PG, _PP, _I32, _I32, _P, _P],
     "oec_cell_merge": [_PG, _PP, _I32, _I32, _D, _D, _I32, ctypes.c_uint64, ctypes.c_uint32, _D, _P, _P, _P, _P],
+    "oec_rhs_with_beam": [_PG, _P, _P, _D, _P, _P, _P, _I32, _P, _P],
+    "oec_history": [_PP, _P, _I32, _P, _P, _P, _P],
+    "oec_step_advance": [_P, _P],
 }
 _INT64_RETURNING = {"oec_sort_work_bytes": [_I64]}
 

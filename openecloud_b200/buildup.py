@@ -1,0 +1,212 @@
+"""Device-resident electron-cloud buildup loop.
+
+The reference's time loop (example01_basic.py:52-97) as one sequence of
+liboec launches per step with every count kept on the device, so a step needs
+no host synchronisation and can be captured once in a CUDA graph and
+replayed.  Per step:
+
+  1. Poisson right-hand side: fixed-point electron deposit (done by the
+     previous step) + beam imprint table[step] * profile   (oec_rhs_with_beam)
+  2. phi = A^-1 q, E = phiToE phi                          (oec_lu_solve, oec_spmv_csr)
+  3. E -> cell corner table                                 (oec_field_prepare)
+  4. gather + Boris push + move + wall test + deposit of the survivors
+                                                            (oec_push_gather)
+  5. absorbed indices, rows, wall point + normal            (oec_absorbed_index,
+                                                             oec_save_absorbed,
+                                                             oec_wall_interaction)
+  6. Furman emission                                        (oec_furman_emit)
+  7. holes <- secondaries, tail compaction, deposit of the
+     secondaries for the next step                          (oec_add_remove)
+  8. history (count, sum w) and ++step                      (oec_history, oec_step_advance)
+
+Particle management (globalRandom / localRandom) runs between graph replays
+at the reference's cadence; it re-deposits and refreshes the fixed-point
+scale.  Periodic cell sorting keeps the deposit's warp aggregation effective.
+"""
+import ctypes
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from . import device as D
+from .beam import LHCBeam, LHCBeamEndless
+from .grid import Grid
+from .particleBoundary import AbsorbElliptical, AbsorbRectangular, AbsorbArbitraryCutCell
+from .particleEmitter import FurmanEmitter, homoLoader, _declare as _emit_declare
+from .particleManagement import globalRandom, localRandom
+from .particles import Particles
+from .poissonSolver import PoissonSolver, _declare as _poisson_declare
+
+
+class Buildup:
+    """A buildup run: grid, particles, boundary, emitter, Poisson solver, beam.
+
+    Parameters mirror the configuration of example01_basic.py; `capacity`
+    bounds the device particle store (the run reports a capacity drop in the
+    status block instead of writing past it)."""
+
+    def __init__(self, nx=128, ny=128, lx=0.04, ly=0.04, boundType=1, n_init=10000, w_init=None, dt=1e-11,
+                 beam="endless", beam_particles=1.1e11, radius_sigma=0.002, bunch_length_sigma=0.25e-9 * 299792458.0,
+                 material="copper", sey_max=1.6, e_hat0=300.0, type_b_field=0, b_const=(0., 0., 0.),
+                 target=100000, management="global", management_every=50, capacity=None, seed=0,
+                 n_steps_table=2500, sort_every=50, boundFunc=None):
+        self.grid = Grid(nx, ny, lx, ly, boundType, boundFunc=boundFunc)
+        self.dt = float(dt)
+        self.target = int(target)
+        self.management = management
+        self.management_every = int(management_every)
+        self.sort_every = int(sort_every)
+        self.seed = int(seed)
+        self.type_b = int(type_b_field)
+        cap = capacity or max(4 * self.target, 4 * n_init, 65536)
+        self.P = Particles("electrons", "variableWeight", capacity=cap)
+        self.P.setBConst(b_const)
+        if boundType == 0:
+            self.bd = AbsorbRectangular(self.grid, self.P)
+        elif boundType == 1:
+            self.bd = AbsorbElliptical(self.grid, self.P)
+        else:
+            self.bd = AbsorbArbitraryCutCell(self.grid, self.P)
+        w_init = w_init if w_init is not None else 1e9 / n_init
+        homoLoader(self.grid, self.P, self.bd, n_init, w_init, seed=seed)
+        self.em = FurmanEmitter(self.bd, self.P, material=material, seyMax=sey_max, seed=seed + 17)
+        if e_hat0 is not None:
+            self.em.setEHat0(e_hat0)
+        self.ps = PoissonSolver(self.grid)
+        beam_cls = LHCBeamEndless if beam == "endless" else LHCBeam
+        self.beam = beam_cls(self.grid, self.dt, nParticles=beam_particles, radiusSigma=radius_sigma,
+                             bunchLengthSigma=bunch_length_sigma)
+        self._table_len = int(n_steps_table)
+        self.beam_profile = D.to_device(self.beam.getTransversalProfile(), torch.float64)
+        self.beam_table = D.to_device(self.beam.scalarTable(self._table_len), torch.float64)
+        G = self.grid.getNpExt()
+        self.step_dev = D.zeros(1, torch.int32)
+        self.rho = D.zeros(G, torch.float64)
+        self.etab = D.zeros(8 * G, torch.float32)
+        self.btab = None
+        self.hist_w = D.zeros(self._table_len, torch.float64)
+        self.hist_n = D.zeros(self._table_len, torch.int32)
+        self.scratch = D.zeros(4, torch.float64)
+        # absorbed rows per step: bounded by a fraction of the capacity
+        self.abs_cap = max(4096, cap // 8)
+        self.bd.ensure_buffers(self.abs_cap)
+        self.em.ensure_buffers(self.bd._rows.shape[0])
+        self.P._deposit_buffers(self.grid)
+        self.P._hole_buffers()
+        self._prepare_deposit()
+        _lib.call("oec_history", self.P.c_particles(), self.step_dev.data_ptr(), self._table_len,
+                  self.hist_w.data_ptr(), self.hist_n.data_ptr(), self.scratch.data_ptr(), D.stream())
+        self.graph = None
+        self.steps_done = 0
+
+    # ------------------------------------------------------------ pieces
+    def _prepare_deposit(self):
+        """Fixed-point scale from the current weights, then a full deposit."""
+        P, s = self.P, D.stream()
+        _lib.call("oec_deposit_scale", P.c_particles(), P._wscale.data_ptr(), s)
+        _lib.call("oec_deposit", self.grid.c_grid(), P.c_particles(), P._rho_fix.data_ptr(), P._wscale.data_ptr(),
+                  1, P._status.data_ptr(), s)
+
+    def _launch_step(self):
+        """All launches of one time step (no host synchronisation)."""
+        P, g, bd, em, ps = self.P, self.grid, self.bd, self.em, self.ps
+        s = D.stream()
+        cg, cp, cb = g.c_grid(), P.c_particles(), bd.c_boundary()
+        L = _lib.lib()
+        _lib.call("oec_rhs_with_beam", cg, P._rho_fix.data_ptr(), P._wscale.data_ptr(), P.particleCharge,
+                  self.beam_profile.data_ptr(), self.beam_table.data_ptr(), self.step_dev.data_ptr(),
+                  self._table_len, self.rho.data_ptr(), s)
+        ps.solveDevice(self.rho)
+        _lib.call("oec_field_prepare", cg, ps.eAtGridPoints.data_ptr(), 2, self.etab.data_ptr(), s)
+        _lib.call("oec_push_gather", cg, cp, self.etab.data_ptr(),
+                  self.btab.data_ptr() if self.btab is not None else None, _lib.d3(P.bConst), self.dt,
+                  P.particleCharge / P.particleMass, self.type_b, cb, P._mask.data_ptr(), P._rho_fix.data_ptr(),
+                  P._wscale.data_ptr(), P._status.data_ptr(), s)
+        _lib.call("oec_absorbed_index", cp, P._mask.data_ptr(), bd._index.data_ptr(), bd._index.shape[0],
+                  bd._n_abs.data_ptr(), bd._scratch.data_ptr(), P._status.data_ptr(), s)
+        cap = bd._rows.shape[0]
+        _lib.call("oec_save_absorbed", cg, cp, bd._index.data_ptr(), bd._n_abs.data_ptr(), cap, bd._rows.data_ptr(),
+                  s)
+        _lib.call("oec_wall_interaction", cg, cb, self.dt, bd._rows.data_ptr(), bd._n_abs.data_ptr(), cap,
+                  bd._normals.data_ptr(), P._status.data_ptr(), s)
+        rc = _emit_declare().oec_furman_emit(ctypes.byref(em.c_params()), bd._rows.data_ptr(),
+                                             bd._normals.data_ptr(), bd._n_abs.data_ptr(), cap, bd._index.data_ptr(),
+                                             em.seed, 0, self.step_dev.data_ptr(), None, em._work.data_ptr(),
+                                             em._out.data_ptr(),
+                                             em._out.shape[0], em._n_out.data_ptr(), P._status.data_ptr(), s)
+        if rc:
+            raise _lib.OecError("oec_furman_emit", rc)
+        _lib.call("oec_add_remove", cg, cp, P._mask.data_ptr(), bd._index.data_ptr(), bd._n_abs.data_ptr(),
+                  bd._index.shape[0], em._out.data_ptr(), em._n_out.data_ptr(), em._out.shape[0],
+                  P._rho_fix.data_ptr(), P._wscale.data_ptr(), P._scan_scratch.data_ptr(), P._status.data_ptr(), s)
+        _lib.call("oec_step_advance", self.step_dev.data_ptr(), s)
+        # state at the start of the next step, before its management
+        # (example01_basic.py:56-57 records it there)
+        _lib.call("oec_history", cp, self.step_dev.data_ptr(), self._table_len, self.hist_w.data_ptr(),
+                  self.hist_n.data_ptr(), self.scratch.data_ptr(), s)
+        del L
+
+    def _manage(self, step):
+        n = self.P.getMacroParticleCount()
+        if step > 0 and step % self.management_every == 0 and (n > 1.05 * self.target or n < 0.95 * self.target):
+            if self.management == "global":
+                globalRandom(self.grid, self.P, self.target, seed=self.seed + step)
+            elif self.management == "local":
+                localRandom(self.grid, self.P, self.bd, self.target, seed=self.seed + step)
+            else:
+                return False
+            self._prepare_deposit()
+            return True
+        return False
+
+    # -------------------------------------------------------------- run
+    def run(self, n_steps, use_graph=True):
+        """Advance n_steps; returns wall seconds on the device clock."""
+        s = torch.cuda.current_stream()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(s)
+        # emission draws are keyed by (seed, particle slot, device step
+        # counter), so replays of one captured step draw fresh numbers
+        k = 0
+        while k < n_steps:
+            step = self.steps_done + k
+            if step >= self._table_len:
+                raise ValueError("beam table exhausted: increase n_steps_table")
+            if self.sort_every and step % self.sort_every == 0 and step > 0:
+                self.P.sortByColumn(6)
+            changed = step % self.management_every == 0 and self._manage(step)
+            # steps until the next management / sort point
+            nxt = n_steps - k
+            for every in (self.management_every, self.sort_every):
+                if every:
+                    nxt = min(nxt, every - (step % every))
+            if use_graph:
+                self._replay(nxt, rebuild=changed or self.graph is None)
+            else:
+                for _ in range(nxt):
+                    self._launch_step()
+            k += nxt
+        t1.record(s)
+        t1.synchronize()
+        self.steps_done += n_steps
+        return t0.elapsed_time(t1) * 1e-3
+
+    def _replay(self, n, rebuild):
+        # A captured step holds raw device pointers; any reallocation
+        # (management, sorting swaps the store) needs a new capture.
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self._launch_step()
+        for _ in range(n):
+            self.graph.replay()
+
+    def history(self):
+        """(macro count, sum of weights) at the start of every step so far."""
+        n = self.steps_done + 1
+        return D.to_numpy(self.hist_n[:n]), D.to_numpy(self.hist_w[:n])
+
+    def status(self):
+        return self.P.status()

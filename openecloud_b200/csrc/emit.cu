@@ -35,7 +35,8 @@ __device__ __forceinline__ double clip(double x, double lo, double hi) {
 
 __global__ void k_furman_pass1(oec_furman_t f, const double *__restrict__ rows, const double *__restrict__ normals,
                                const int32_t *n_abs, int cap, const int32_t *__restrict__ ids, uint2 key,
-                               uint32_t step, const double *__restrict__ replay, Rec *__restrict__ rec,
+                               uint32_t step, const int32_t *step_dev, const double *__restrict__ replay,
+                               Rec *__restrict__ rec,
                                int32_t *__restrict__ nsec, oec_status_t *status) {
     int na = min(*n_abs, cap);
     const double eFactor = 0.5 * f.particle_mass / 1.602176565e-19;
@@ -70,7 +71,8 @@ __global__ void k_furman_pass1(oec_furman_t f, const double *__restrict__ rows, 
         }
         double pr = dTSp / f.m;
         double keep = 1 - dE - dR;
-        sf::Draws dr{key, ids ? (uint32_t)ids[i] : (uint32_t)i, step, replay ? replay + (int64_t)i * kDraws : nullptr};
+        sf::Draws dr{key, ids ? (uint32_t)ids[i] : (uint32_t)i, step + (step_dev ? (uint32_t)*step_dev : 0u),
+                     replay ? replay + (int64_t)i * kDraws : nullptr};
         double u = dr.next();
         // P_n = binom(n; m, pr) (1 - dE - dR), P_1 += dE + dR (:217-221);
         // inverse-CDF draw over n < m, default m (:222-229)
@@ -93,7 +95,8 @@ __global__ void k_furman_pass1(oec_furman_t f, const double *__restrict__ rows, 
 
 __global__ void k_furman_pass2(oec_furman_t f, const double *__restrict__ rows, const double *__restrict__ normals,
                                const int32_t *n_abs, int cap, const int32_t *__restrict__ ids, uint2 key,
-                               uint32_t step, const double *__restrict__ replay, const Rec *__restrict__ rec,
+                               uint32_t step, const int32_t *step_dev, const double *__restrict__ replay,
+                               const Rec *__restrict__ rec,
                                const int32_t *__restrict__ offset, double *__restrict__ out, int out_cap,
                                oec_status_t *status) {
     int na = min(*n_abs, cap);
@@ -107,7 +110,8 @@ __global__ void k_furman_pass2(oec_furman_t f, const double *__restrict__ rows, 
         if (n == 0) continue;
         const double *r = rows + 6 * (int64_t)i;
         const double n0 = normals[2 * i], n1 = normals[2 * i + 1];
-        sf::Draws dr{key, ids ? (uint32_t)ids[i] : (uint32_t)i, step, replay ? replay + (int64_t)i * kDraws : nullptr};
+        sf::Draws dr{key, ids ? (uint32_t)ids[i] : (uint32_t)i, step + (step_dev ? (uint32_t)*step_dev : 0u),
+                     replay ? replay + (int64_t)i * kDraws : nullptr};
         dr.d = 1;  // draw 0 was the secondary count
         double eSec[10];
         const double e0 = R.e0;
@@ -277,7 +281,8 @@ using namespace oec;
 
 extern "C" int oec_furman_emit(const oec_furman_t *params, const double *rows_dev, const double *normals_dev,
                                const int32_t *n_abs_dev, int32_t cap, const int32_t *ids_dev, uint64_t seed,
-                               uint32_t step, const double *replay_uniforms_dev, void *work_dev,
+                               uint32_t step, const int32_t *step_dev, const double *replay_uniforms_dev,
+                               void *work_dev,
                                double *out_rows_dev, int32_t out_cap, int32_t *n_out_dev, oec_status_t *status_dev,
                                void *stream) {
     if (!params || !rows_dev || !normals_dev || !n_abs_dev || !work_dev || !out_rows_dev || !n_out_dev ||
@@ -294,7 +299,7 @@ extern "C" int oec_furman_emit(const oec_furman_t *params, const double *rows_de
     int *partial = off + cap;
     uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
     int g = persistent_grid((cap + 127) / 128, 8);
-    k_furman_pass1<<<g, 128, 0, s>>>(*params, rows_dev, normals_dev, n_abs_dev, cap, ids_dev, key, step,
+    k_furman_pass1<<<g, 128, 0, s>>>(*params, rows_dev, normals_dev, n_abs_dev, cap, ids_dev, key, step, step_dev,
                                      replay_uniforms_dev, rec, nsec, status_dev);
     if (cap > 0) {
         k_scan_blocks<<<nblocks, kScanT, 0, s>>>(nsec, n_abs_dev, cap, off, partial);
@@ -303,7 +308,7 @@ extern "C" int oec_furman_emit(const oec_furman_t *params, const double *rows_de
     } else {
         OEC_CUDA_TRY(cudaMemsetAsync(n_out_dev, 0, sizeof(int32_t), s));
     }
-    k_furman_pass2<<<g, 128, 0, s>>>(*params, rows_dev, normals_dev, n_abs_dev, cap, ids_dev, key, step,
+    k_furman_pass2<<<g, 128, 0, s>>>(*params, rows_dev, normals_dev, n_abs_dev, cap, ids_dev, key, step, step_dev,
                                      replay_uniforms_dev, rec, off, out_rows_dev, out_cap, status_dev);
     OEC_LAUNCH_CHECK();
     return OEC_OK;

@@ -267,15 +267,18 @@ struct MergeArgs {
     int *counters;             // [0] qualifying pairs, [1] merges done
 };
 
-// Pair (2k, 2k+1) of the ordered candidates: qualifies when both are in the
-// same cell and the weighted phase-space distance passes the test.
+// Pair (2k, 2k+1) of the ordered candidates: qualifies when the weighted
+// phase-space distance passes the reference's test.
 __global__ void k_pair_count(MergeArgs a) {
     int npairs = a.n_cand / 2;
     int q = 0;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < npairs; k += gridDim.x * blockDim.x) {
         int i = a.order[2 * k], j = a.order[2 * k + 1];
-        if (a.p.cell[i] != a.p.cell[j]) continue;
-        double ddx = ((double)a.p.ox[i] - a.p.ox[j]) * a.dx, ddy = ((double)a.p.oy[i] - a.p.oy[j]) * a.dy;
+        int ix, iy, jx, jy;
+        split_cell(a.p.cell[i], a.nx, a.inv_nx, ix, iy);
+        split_cell(a.p.cell[j], a.nx, a.inv_nx, jx, jy);
+        double ddx = ((double)(ix - jx) + ((double)a.p.ox[i] - a.p.ox[j])) * a.dx;
+        double ddy = ((double)(iy - jy) + ((double)a.p.oy[i] - a.p.oy[j])) * a.dy;
         double dvx = (double)a.p.vx[i] - a.p.vx[j], dvy = (double)a.p.vy[i] - a.p.vy[j],
                dvz = (double)a.p.vz[i] - a.p.vz[j];
         double d2 = ddx * ddx + ddy * ddy + a.lam2 * (dvx * dvx + dvy * dvy + dvz * dvz);
@@ -292,8 +295,11 @@ __global__ void k_pair_merge(MergeArgs a) {
     int done = 0;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < npairs; k += gridDim.x * blockDim.x) {
         int i = a.order[2 * k], j = a.order[2 * k + 1];
-        if (a.p.cell[i] != a.p.cell[j]) continue;
-        double ddx = ((double)a.p.ox[i] - a.p.ox[j]) * a.dx, ddy = ((double)a.p.oy[i] - a.p.oy[j]) * a.dy;
+        int ix, iy, jx, jy;
+        split_cell(a.p.cell[i], a.nx, a.inv_nx, ix, iy);
+        split_cell(a.p.cell[j], a.nx, a.inv_nx, jx, jy);
+        double ddx = ((double)(ix - jx) + ((double)a.p.ox[i] - a.p.ox[j])) * a.dx;
+        double ddy = ((double)(iy - jy) + ((double)a.p.oy[i] - a.p.oy[j])) * a.dy;
         double dvx = (double)a.p.vx[i] - a.p.vx[j], dvy = (double)a.p.vy[i] - a.p.vy[j],
                dvz = (double)a.p.vz[i] - a.p.vz[j];
         double d2 = ddx * ddx + ddy * ddy + a.lam2 * (dvx * dvx + dvy * dvy + dvz * dvz);
@@ -324,12 +330,28 @@ __global__ void k_pair_merge(MergeArgs a) {
     if ((threadIdx.x & 31) == 0 && done) atomicAdd(&a.counters[1], done);
 }
 
-// Candidate keys: cell in the high bits, a coarse weighted-velocity key below.
-__global__ void k_cand_keys(oec_particles_t p, int n_cand, double vscale, uint32_t *keys, int32_t *vals) {
+__device__ __forceinline__ uint32_t spread_bits11(uint32_t v) {
+    // 11-bit value -> every other bit of a 22-bit word
+    v &= 0x7ffu;
+    v = (v | (v << 8)) & 0x00ff00ffu;
+    v = (v | (v << 4)) & 0x0f0f0f0fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+
+// Candidate keys: Morton order of the cell coordinates (22 bits) so that
+// neighbours in key order are neighbours in space, then a 10-bit velocity
+// projection inside a cell.
+__global__ void k_cand_keys(oec_particles_t p, int n_cand, int nx, float inv_nx, double vscale, uint32_t *keys,
+                            int32_t *vals) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_cand; i += gridDim.x * blockDim.x) {
+        int ix, iy;
+        split_cell(p.cell[i], nx, inv_nx, ix, iy);
+        uint32_t morton = spread_bits11((uint32_t)ix) | (spread_bits11((uint32_t)iy) << 1);
         double u = 0.5 + 0.25 * ((double)p.vx[i] + p.vy[i] + p.vz[i]) / vscale;  // projection in [0,1)
-        uint32_t vk = (uint32_t)fmin(fmax(u * 2048.0, 0.0), 2047.0);
-        keys[i] = ((uint32_t)p.cell[i] << 11) | vk;
+        uint32_t vk = (uint32_t)fmin(fmax(u * 1024.0, 0.0), 1023.0);
+        keys[i] = (morton << 10) | vk;
         vals[i] = i;
     }
 }
@@ -481,7 +503,7 @@ extern "C" int oec_cell_merge(const oec_grid_t *grid, oec_particles_t *p, int32_
         !work_dev)
         return OEC_ERR_INVALID;
     GridConst gc = make_grid_const(*grid);
-    if ((int64_t)gc.G >= (1 << 21)) return OEC_ERR_INVALID;  // 21 cell bits + 11 velocity bits
+    if (gc.nx > 2048 || gc.ny > 2048) return OEC_ERR_INVALID;  // 2 x 11 Morton bits + 10 velocity bits
     cudaStream_t s = as_stream(stream);
     int64_t cap = p->capacity;
     uint32_t *keys = static_cast<uint32_t *>(work_dev);
@@ -493,7 +515,7 @@ extern "C" int oec_cell_merge(const oec_grid_t *grid, oec_particles_t *p, int32_
     OEC_CUDA_TRY(cudaMemcpyAsync(ncand_dev, &n_cand, sizeof(int32_t), cudaMemcpyHostToDevice, s));
     OEC_CUDA_TRY(cudaMemsetAsync(counters_dev, 0, 2 * sizeof(int32_t), s));
     int g = persistent_grid((n_cand + 255) / 256 + 1, 8);
-    k_cand_keys<<<g, 256, 0, s>>>(*p, n_cand, vscale, keys, vals);
+    k_cand_keys<<<g, 256, 0, s>>>(*p, n_cand, gc.nx, 1.0f / (float)gc.nx, vscale, keys, vals);
     uint32_t *kout;
     int32_t *vout;
     int rc = radix_sort(keys, vals, k2, v2, hist, ncand_dev, cap, 32, s, &kout, &vout);

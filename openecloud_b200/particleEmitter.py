@@ -51,7 +51,7 @@ def _declare():
         P = ctypes.c_void_p
         L.oec_furman_emit.restype = ctypes.c_int
         L.oec_furman_emit.argtypes = [ctypes.POINTER(Furman_t), P, P, P, ctypes.c_int32, P, ctypes.c_uint64,
-                                      ctypes.c_uint32, P, P, P, ctypes.c_int32, P, P, P]
+                                      ctypes.c_uint32, P, P, P, P, ctypes.c_int32, P, P, P]
         L.oec_furman_work_bytes.restype = ctypes.c_int64
         L.oec_furman_work_bytes.argtypes = [ctypes.c_int32]
         L._emit_declared = True
@@ -130,7 +130,7 @@ class FurmanEmitter:
         step = self.step if step is None else int(step)
         ids = bd._index.data_ptr() if bd._index is not None else None
         rc = _declare().oec_furman_emit(ctypes.byref(self.c_params()), bd._rows.data_ptr(), bd._normals.data_ptr(),
-                                        bd._n_abs.data_ptr(), cap, ids, self.seed, step & 0xffffffff,
+                                        bd._n_abs.data_ptr(), cap, ids, self.seed, step & 0xffffffff, None,
                                         replay.data_ptr() if replay is not None else None, self._work.data_ptr(),
                                         self._out.data_ptr(), self._out.shape[0], self._n_out.data_ptr(),
                                         P._status.data_ptr(), D.stream())

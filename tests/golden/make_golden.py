@@ -182,7 +182,7 @@ def main():
         print("wrote", path, os.path.getsize(path))
 
 
-if __name__ == "__main__" and "--emission" not in sys.argv and "--management" not in sys.argv:
+if __name__ == "__main__" and not any(a.startswith("--") for a in sys.argv[1:]):
     main()
 
 
@@ -299,3 +299,86 @@ def management_golden():
 
 if __name__ == "__main__" and "--management" in sys.argv:
     management_golden()
+
+
+def reference_buildup(seed, n_steps, nx=128, lx=0.04, n_init=10000, dt=1e-11, target=100000):
+    """The reference's own loop (example01_basic.py:52-97, Python 3, no plots)
+    on the 128x128 circular chamber; returns (macro counts, sum of weights)."""
+    grid, particles, particleBoundary, poissonSolver, randomGen = _import_reference()
+    import particleEmitter
+    import particleManagement
+    from beam import LHCBeamEndless
+    randomGen.seed(seed)
+    g = grid.Grid(nx, nx, lx, lx, 1)
+    beam = LHCBeamEndless(g, dt, nParticles=1.1e11)
+    beam.bunchLengthSigma = 0.25e-9 * 299792458.0          # sigma_t = 0.25 ns
+    beam.tBunchLengthSigma = beam.bunchLengthSigma / beam.beamVelocity
+    P = particles.Particles("electrons", "variableWeight")
+    bd = particleBoundary.AbsorbElliptical(g, P)
+    em = particleEmitter.FurmanEmitter(bd, P, seyMax=1.6)
+    em.setEHat0(300.)
+    ps = poissonSolver.PoissonSolver(g)
+    particleEmitter.homoLoader(g, P, bd, n_init, 1e9 / n_init)
+    counts = np.zeros(n_steps + 1, np.int64)
+    weight = np.zeros(n_steps + 1)
+    for ii in range(n_steps):
+        weight[ii] = np.sum(np.asarray(P.getParticleData())[:, 5])
+        counts[ii] = P.getMacroParticleCount()
+        if ii > 0 and ii % 50 == 0 and (counts[ii] > 1.05 * target or counts[ii] < 0.95 * target):
+            particleManagement.globalRandom(g, P, target)
+        P.calcGridWeights(g)
+        P.chargeToGrid(g)
+        ps.solve(np.asarray(P.getChargeOnGrid()) + beam.getCharge(ii * dt))
+        P.eFieldToParticles(g, ps.getEAtGridPoints())
+        P.borisPush(dt, 0)
+        bd.indexInside()
+        bd.saveAbsorbed()
+        if bd.getAbsorbedMacroParticleCount() > 0:
+            bd.calculateInteractionPoint()
+            bd.calculateNormalVectors()
+            P.addAndRemoveParticles(em.generateSecondaries(), P.getIsInside())
+    weight[n_steps] = np.sum(np.asarray(P.getParticleData())[:, 5])
+    counts[n_steps] = P.getMacroParticleCount()
+    return counts, weight
+
+
+def buildup_golden(n_seeds=8, n_steps=2500):
+    out = {}
+    W, C = [], []
+    for s in range(n_seeds):
+        c, w = reference_buildup(100 + s, n_steps)
+        W.append(w)
+        C.append(c)
+        print("seed", s, "final count", c[-1], "line density", w[-1])
+    out["weight"] = np.array(W)[:, ::10]
+    out["count"] = np.array(C)[:, ::10]
+    out["every"] = np.array(10)
+    path = os.path.join(HERE, "buildup_c1.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path))
+
+
+if __name__ == "__main__" and "--buildup" in sys.argv:
+    buildup_golden()
+
+
+def beam_golden():
+    grid, particles, particleBoundary, poissonSolver, randomGen = _import_reference()
+    from beam import LHCBeam, LHCBeamEndless
+    g = grid.Grid(64, 48, 0.04, 0.03, 1)
+    e = LHCBeamEndless(g, 1e-11, nParticles=1.1e11)
+    t = LHCBeam(g, 1e-11, nParticles=1.15e11)
+    times = np.array([0.0, 1e-11, 3.3e-10, 1.0e-9, 1.7e-9, 2.5e-8 + 1.2e-9, 1.8e-6 + 4e-10, 2.05e-6 + 5e-10,
+                      7.9e-6 + 1e-9, 3.0e-5 + 8e-10])
+    as_arr = lambda v: np.zeros(g.getNpExt()) if np.isscalar(v) else np.asarray(v)  # noqa: E731
+    out = {"times": times, "endless_profile": np.asarray(e.getTransversalProfile()),
+           "train_profile": np.asarray(t.getTransversalProfile()),
+           "endless_charge": np.array([as_arr(e.getCharge(x)) for x in times]),
+           "train_charge": np.array([as_arr(t.getCharge(x)) for x in times])}
+    path = os.path.join(HERE, "beam.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path))
+
+
+if __name__ == "__main__" and "--beam" in sys.argv:
+    beam_golden()

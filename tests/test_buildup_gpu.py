@@ -1,0 +1,57 @@
+"""Statistical parity of the device buildup loop with the reference.
+
+Configuration: 128x128 circular chamber R = 20 mm, 1e4 initial electrons,
+endless bunch train (sigma_r 2 mm, sigma_t 0.25 ns, 1.1e11 protons, 25 ns),
+copper SEY with delta_max 1.6 and E_max 300 eV, roulette cap 1e5 every 50
+steps, dt = 1e-11 s, one bunch passage (2500 steps).  The golden file holds
+the reference's line density for 8 seeds; the ensemble mean of 8 device runs
+must stay within twice the reference's seed-to-seed spread (floor 0.2%).
+"""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def test_buildup_line_density_within_reference_spread(gpu):
+    from openecloud_b200.buildup import Buildup
+    z = golden("buildup_c1.npz")
+    every = int(z["every"])
+    ref = z["weight"]
+    runs = []
+    for s in range(8):
+        b = Buildup(seed=1000 + s, n_steps_table=2501)
+        b.run(2500)
+        n, w = b.history()
+        st = b.status()
+        assert st["n_capacity_drop"] == 0 and st["n_nonfinite"] == 0
+        runs.append(w[::every])
+    gpu_w = np.array(runs)
+    m_ref, s_ref = ref.mean(0), ref.std(0, ddof=1)
+    m_gpu = gpu_w.mean(0)
+    tol = 2 * np.maximum(s_ref, 0.002 * m_ref)
+    bad = np.abs(m_gpu - m_ref) > tol
+    assert not bad.any(), (np.nonzero(bad)[0][:10], m_gpu[bad][:5], m_ref[bad][:5])
+    # the cloud builds up over the passage as in the reference
+    assert m_gpu[-1] / m_gpu[0] > 1.2
+
+
+def test_beam_profile_and_charge_match_reference(gpu):
+    """Product beam (host setup) against the reference's beam.py values."""
+    z = golden("beam.npz")
+    from openecloud_b200.grid import Grid
+    from openecloud_b200.beam import LHCBeam, LHCBeamEndless
+    g = Grid(64, 48, 0.04, 0.03, 1)
+    e = LHCBeamEndless(g, 1e-11, nParticles=1.1e11)
+    t = LHCBeam(g, 1e-11, nParticles=1.15e11)
+    assert np.max(np.abs(e.getTransversalProfile() - z["endless_profile"])) <= 1e-15
+    assert np.max(np.abs(t.getTransversalProfile() - z["train_profile"])) <= 1e-15
+    for k, tt in enumerate(z["times"]):
+        ce = e.getCharge(tt)
+        ct = t.getCharge(tt)
+        ce = np.zeros(g.getNpExt()) if np.isscalar(ce) else ce
+        ct = np.zeros(g.getNpExt()) if np.isscalar(ct) else ct
+        assert np.allclose(ce, z["endless_charge"][k], rtol=1e-13, atol=0)
+        assert np.allclose(ct, z["train_charge"][k], rtol=1e-13, atol=0)
