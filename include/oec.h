@@ -301,9 +301,10 @@ int oec_weight_stats(const oec_particles_t *p, double *acc_dev, void *stream);
  * duplicates as rows (localRandom split, particleManagement.pyx:130-163). */
 int oec_split_rows(const oec_grid_t *grid, oec_particles_t *p, int32_t n, int32_t k, double *rows_dev, void *stream);
 
-/* Cell-binned merge (localRandom :165-236): the first n_cand particles are
- * ordered by (Morton index of the cell, velocity projection); neighbouring
- * pairs whose squared phase-space distance dx^2 + dy^2 + lambda^2 |dv|^2 is below
+/* Binned merge (localRandom :165-236): the first n_cand particles are
+ * ordered along a 5-D Morton curve of their weighted phase-space coordinates
+ * (x, y, lambda v; one scale for all axes); neighbouring pairs in that order
+ * whose squared phase-space distance dx^2 + dy^2 + lambda^2 |dv|^2 is below
  * `limit` merge with probability min(1, n_merge / qualifying pairs); the
  * survivor is drawn with probability proportional to weight and takes the
  * summed weight; the other gets its removal bit.  scheme 1 rescales the

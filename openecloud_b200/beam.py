@@ -13,9 +13,13 @@ The radius and bunch-length sigmas are constructor arguments with the
 reference's values as defaults (1 mm / 2 mm, 0.1 m).
 """
 import numpy as np
+import scipy.constants as spc
 from scipy.special import ndtr
 
-from .constants import c, elementary_charge
+# beam.py takes e and c from scipy.constants (beam.py:9, :25-26), not from the
+# reference's constants.pyx; the installed SciPy's values are used here too.
+elementary_charge = spc.elementary_charge
+c = spc.c
 
 
 class _BeamBase:

@@ -21,7 +21,15 @@ replayed.  Per step:
 
 Particle management (globalRandom / localRandom) runs between graph replays
 at the reference's cadence; it re-deposits and refreshes the fixed-point
-scale.  Periodic cell sorting keeps the deposit's warp aggregation effective.
+scale.
+
+Particle order is physics here: the reference's Furman emitter gives a lone
+secondary the elastic / rediffused / true-secondary split of the LAST
+absorbed particle of the step (particleEmitter.pyx:245-246), so which particle
+is last matters.  The driver keeps the reference's order (holes refilled by
+secondaries, extras appended, tail compaction) and does not sort by default.
+Periodic cell sorting (`sort_every`) helps the deposit's warp aggregation but
+is only order-neutral with the emitter's `compat` switch off.
 """
 import ctypes
 import time
@@ -51,7 +59,7 @@ class Buildup:
                  beam="endless", beam_particles=1.1e11, radius_sigma=0.002, bunch_length_sigma=0.25e-9 * 299792458.0,
                  material="copper", sey_max=1.6, e_hat0=300.0, type_b_field=0, b_const=(0., 0., 0.),
                  target=100000, management="global", management_every=50, capacity=None, seed=0,
-                 n_steps_table=2500, sort_every=50, boundFunc=None):
+                 n_steps_table=2500, sort_every=0, boundFunc=None):
         self.grid = Grid(nx, ny, lx, ly, boundType, boundFunc=boundFunc)
         self.dt = float(dt)
         self.target = int(target)

@@ -16,9 +16,9 @@
 //  * localRandom keeps the reference's bookkeeping (weight thresholds, split
 //    and merge counts, typical velocity, phase-space metric with
 //    lambda = ds / v_typical) but replaces the sequential kd-tree search by
-//    pairing inside grid cells: the merge candidates (the lightest particles)
-//    are ordered by (cell, weighted velocity) and neighbours in that order
-//    are merged when their phase-space distance passes the reference's test.
+//    binning: the merge candidates (the lightest particles) are ordered along
+//    a 5-D Morton curve of (x, y, lambda v) and neighbours in that order are
+//    merged when their phase-space distance passes the reference's test.
 #include <math.h>
 #include <stdint.h>
 
@@ -330,28 +330,74 @@ __global__ void k_pair_merge(MergeArgs a) {
     if ((threadIdx.x & 31) == 0 && done) atomicAdd(&a.counters[1], done);
 }
 
-__device__ __forceinline__ uint32_t spread_bits11(uint32_t v) {
-    // 11-bit value -> every other bit of a 22-bit word
-    v &= 0x7ffu;
-    v = (v | (v << 8)) & 0x00ff00ffu;
-    v = (v | (v << 4)) & 0x0f0f0f0fu;
-    v = (v | (v << 2)) & 0x33333333u;
-    v = (v | (v << 1)) & 0x55555555u;
-    return v;
+// Weighted phase-space coordinates of the merge metric (localRandom :166-171):
+// (x, y, lambda vx, lambda vy, lambda vz), positions relative to the grid corner.
+__device__ __forceinline__ void phase5(const oec_particles_t &p, int i, int nx, float inv_nx, double dx, double dy,
+                                       double lam, float c[5]) {
+    int ix, iy;
+    split_cell(p.cell[i], nx, inv_nx, ix, iy);
+    c[0] = (float)(((double)ix + p.ox[i]) * dx);
+    c[1] = (float)(((double)iy + p.oy[i]) * dy);
+    c[2] = (float)(lam * p.vx[i]);
+    c[3] = (float)(lam * p.vy[i]);
+    c[4] = (float)(lam * p.vz[i]);
 }
 
-// Candidate keys: Morton order of the cell coordinates (22 bits) so that
-// neighbours in key order are neighbours in space, then a 10-bit velocity
-// projection inside a cell.
-__global__ void k_cand_keys(oec_particles_t p, int n_cand, int nx, float inv_nx, double vscale, uint32_t *keys,
-                            int32_t *vals) {
+// Bounding box of the candidates' weighted coordinates (order-preserving
+// float keys, atomic min / max): bbox[0..4] minima, bbox[5..9] maxima.
+__global__ void k_cand_bbox(oec_particles_t p, int n_cand, int nx, float inv_nx, double dx, double dy, double lam,
+                            uint32_t *bbox) {
+    uint32_t mn[5], mx[5];
+    for (int d = 0; d < 5; ++d) {
+        mn[d] = 0xffffffffu;
+        mx[d] = 0u;
+    }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_cand; i += gridDim.x * blockDim.x) {
-        int ix, iy;
-        split_cell(p.cell[i], nx, inv_nx, ix, iy);
-        uint32_t morton = spread_bits11((uint32_t)ix) | (spread_bits11((uint32_t)iy) << 1);
-        double u = 0.5 + 0.25 * ((double)p.vx[i] + p.vy[i] + p.vz[i]) / vscale;  // projection in [0,1)
-        uint32_t vk = (uint32_t)fmin(fmax(u * 1024.0, 0.0), 1023.0);
-        keys[i] = (morton << 10) | vk;
+        float c[5];
+        phase5(p, i, nx, inv_nx, dx, dy, lam, c);
+        for (int d = 0; d < 5; ++d) {
+            uint32_t k = float_key(c[d]);
+            mn[d] = min(mn[d], k);
+            mx[d] = max(mx[d], k);
+        }
+    }
+    for (int d = 0; d < 5; ++d) {
+        for (int o = 16; o > 0; o >>= 1) {
+            mn[d] = min(mn[d], __shfl_xor_sync(kFullMask, mn[d], o));
+            mx[d] = max(mx[d], __shfl_xor_sync(kFullMask, mx[d], o));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(&bbox[d], mn[d]);
+            atomicMax(&bbox[5 + d], mx[d]);
+        }
+    }
+}
+
+__device__ __forceinline__ float key_float(uint32_t k) {
+    uint32_t u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+    return __uint_as_float(u);
+}
+
+// Candidate keys: 5-D Morton order (6 bits per axis, one common scale for all
+// axes so that the order follows the isotropic weighted metric): neighbours in
+// key order are close in (x, y, lambda v).
+__global__ void k_cand_keys(oec_particles_t p, int n_cand, int nx, float inv_nx, double dx, double dy, double lam,
+                            const uint32_t *bbox, uint32_t *keys, int32_t *vals) {
+    float lo[5], span = 0.f;
+    for (int d = 0; d < 5; ++d) {
+        lo[d] = key_float(bbox[d]);
+        span = fmaxf(span, key_float(bbox[5 + d]) - lo[d]);
+    }
+    float inv = span > 0.f ? 64.0f / span : 0.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_cand; i += gridDim.x * blockDim.x) {
+        float c[5];
+        phase5(p, i, nx, inv_nx, dx, dy, lam, c);
+        uint32_t q[5];
+        for (int d = 0; d < 5; ++d) q[d] = (uint32_t)fminf(fmaxf((c[d] - lo[d]) * inv, 0.f), 63.f);
+        uint32_t key = 0;
+        for (int b = 5; b >= 0; --b)
+            for (int d = 0; d < 5; ++d) key = (key << 1) | ((q[d] >> b) & 1u);
+        keys[i] = key;
         vals[i] = i;
     }
 }
@@ -503,7 +549,7 @@ extern "C" int oec_cell_merge(const oec_grid_t *grid, oec_particles_t *p, int32_
         !work_dev)
         return OEC_ERR_INVALID;
     GridConst gc = make_grid_const(*grid);
-    if (gc.nx > 2048 || gc.ny > 2048) return OEC_ERR_INVALID;  // 2 x 11 Morton bits + 10 velocity bits
+    (void)vscale;
     cudaStream_t s = as_stream(stream);
     int64_t cap = p->capacity;
     uint32_t *keys = static_cast<uint32_t *>(work_dev);
@@ -512,10 +558,14 @@ extern "C" int oec_cell_merge(const oec_grid_t *grid, oec_particles_t *p, int32_
     int32_t *v2 = reinterpret_cast<int32_t *>(k2 + cap);
     int *hist = reinterpret_cast<int *>(v2 + cap);
     int32_t *ncand_dev = reinterpret_cast<int32_t *>(hist + 256 * ((cap + kTile - 1) / kTile));
+    uint32_t *bbox = reinterpret_cast<uint32_t *>(ncand_dev + 1);  // 10 words (inside the 256-byte slack)
+    uint32_t init[10] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u, 0u, 0u};
     OEC_CUDA_TRY(cudaMemcpyAsync(ncand_dev, &n_cand, sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    OEC_CUDA_TRY(cudaMemcpyAsync(bbox, init, sizeof(init), cudaMemcpyHostToDevice, s));
     OEC_CUDA_TRY(cudaMemsetAsync(counters_dev, 0, 2 * sizeof(int32_t), s));
     int g = persistent_grid((n_cand + 255) / 256 + 1, 8);
-    k_cand_keys<<<g, 256, 0, s>>>(*p, n_cand, gc.nx, 1.0f / (float)gc.nx, vscale, keys, vals);
+    k_cand_bbox<<<g, 256, 0, s>>>(*p, n_cand, gc.nx, 1.0f / (float)gc.nx, gc.dx, gc.dy, lambda, bbox);
+    k_cand_keys<<<g, 256, 0, s>>>(*p, n_cand, gc.nx, 1.0f / (float)gc.nx, gc.dx, gc.dy, lambda, bbox, keys, vals);
     uint32_t *kout;
     int32_t *vout;
     int rc = radix_sort(keys, vals, k2, v2, hist, ncand_dev, cap, 32, s, &kout, &vout);
