@@ -166,6 +166,21 @@ int oec_deposit_finalize(const oec_grid_t *grid, const int64_t *rho_fix_dev,
                          const double *wscale_dev, double particle_charge, double *rho_dev,
                          void *stream);
 
+/* No counterpart in the reference.  The charge deposit above (scale + deposit
+ * + finalize, f64 charge per node into rho_dev) for callers that cannot
+ * allocate device memory: hosts that own the whole device memory budget
+ * through their own pool, or run with a memory plan fixed before the
+ * simulation starts.  The int64 scratch grid and the fixed-point scale live in
+ * file-scope device arrays (about 8.8 MB per GPU, held until the process
+ * exits); nothing is allocated.  Limit: nx*ny of the extended grid at most
+ * 1,100,000 nodes (a 1024 x 1024 grid), else OEC_ERR_CAPACITY.  All calls
+ * share the scratch, so calls that overlap on the GPU (other streams, other
+ * threads) race: serialise them.  Each call clears the scratch it uses; the
+ * first call on a device looks up the scratch address with that device
+ * current, so make it before any stream capture. */
+int oec_deposit_charge_noalloc(const oec_grid_t *grid, const oec_particles_t *p,
+                               double particle_charge, double *rho_dev, void *stream);
+
 /* ---------------------------------------------------- boundary (A17-A20) */
 
 /* indexInside (particleBoundary.pyx:84-97 / :227-242 / :336-370): absorbed

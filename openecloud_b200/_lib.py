@@ -67,6 +67,7 @@ SIGNATURES = {
     "oec_push_gather": [_PG, _PP, _P, _P, _P, _D, _D, _I32, _PB, _P, _P, _P, _P, _P],
     "oec_deposit": [_PG, _PP, _P, _P, _I32, _P, _P],
     "oec_deposit_finalize": [_PG, _P, _P, _D, _P, _P],
+    "oec_deposit_charge_noalloc": [_PG, _PP, _D, _P, _P],
     "oec_index_inside": [_PG, _PP, _PB, _P, _P, _P],
     "oec_absorbed_index": [_PP, _P, _P, _I32, _P, _P, _P, _P],
     "oec_save_absorbed": [_PG, _PP, _P, _P, _I32, _P, _P],
