@@ -77,32 +77,55 @@ __device__ __forceinline__ double abs_coord(int i, float o, double d, double hal
     return __dsub_rn(__dmul_rn(__dadd_rn((double)i, (double)o), d), half);
 }
 
-// Warp-segmented suffix sum of four int64 lanes grouped by equal, adjacent
-// keys.  On return the first lane of every segment ("head") holds the
-// segment's totals.  Keys need not be sorted: a key that reappears after a
-// different key starts a new segment.
-__device__ __forceinline__ bool warp_segment_sum4(int key, long long v[4]) {
-    const int lane = threadIdx.x & 31;
-    int prev = __shfl_up_sync(kFullMask, key, 1);
-    bool head = (lane == 0) || (prev != key);
-    unsigned heads = __ballot_sync(kFullMask, head);
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        long long o0 = __shfl_down_sync(kFullMask, v[0], off);
-        long long o1 = __shfl_down_sync(kFullMask, v[1], off);
-        long long o2 = __shfl_down_sync(kFullMask, v[2], off);
-        long long o3 = __shfl_down_sync(kFullMask, v[3], off);
-        if (lane + off < 32) {
-            unsigned between = ((1u << off) - 1u) << (lane + 1);
-            if ((heads & between) == 0u) {
-                v[0] += o0;
-                v[1] += o1;
-                v[2] += o2;
-                v[3] += o3;
-            }
-        }
+// ---- conversions without the conversion unit -----------------------------
+// Int <-> float conversion instructions issue at a quarter of the FP32 rate
+// or less; the hot kernel needs about twenty per particle written the plain
+// way, enough to saturate that unit.  The helpers below give bit-identical
+// results with FP32/FP64 adds and integer operations only.
+
+// cell -> (ix, iy) with m = ceil(2^64 / nx): floor(cell * m / 2^64) equals
+// cell / nx for every 0 <= cell < 2^32 and 2 <= nx < 2^31 (the error term
+// cell * (m - 2^64/nx) / 2^64 stays below 1/nx).
+inline unsigned long long split_magic(int nx) { return ~0ULL / (unsigned long long)nx + 1ULL; }
+
+__device__ __forceinline__ void split_cell_m(int cell, int nx, unsigned long long m, int &ix, int &iy) {
+    iy = (int)__umul64hi((unsigned long long)(unsigned)cell, m);
+    ix = cell - iy * nx;
+}
+
+// floorf(v) as (float, int) for |v| <= 2^22: adding 1.5*2^23 rounds v to an
+// integer held in the low mantissa bits; one compare turns round into floor.
+__device__ __forceinline__ int floor_small(float v, float &fl) {
+    const float C = 12582912.0f;  // 1.5 * 2^23, bits 0x4b400000
+    float t = __fadd_rn(v, C);
+    int r = __float_as_int(t) - 0x4b400000;
+    float rf = __fsub_rn(t, C);
+    if (rf > v) {
+        r -= 1;
+        rf = __fsub_rn(rf, 1.0f);
     }
-    return head;
+    fl = rf;
+    return r;
+}
+
+// (double)i for any int32: 1.5*2^52 + 2^31 + i carries i in the low word.
+__device__ __forceinline__ double int_to_double(int i) {
+    return __dsub_rn(__hiloint2double(0x43380000, (int)((unsigned)i ^ 0x80000000u)), 6755401588539392.0);
+}
+
+// llrint(x) (round to nearest, ties to even) for |x| < 2^51, also returned
+// as a double in xr.
+__device__ __forceinline__ long long rint_i64(double x, double &xr) {
+    const double C = 6755399441055744.0;  // 1.5 * 2^52, bits 0x4338000000000000
+    double t = __dadd_rn(x, C);
+    xr = __dsub_rn(t, C);
+    return __double_as_longlong(t) - 0x4338000000000000LL;
+}
+
+// The same with the offset already widened and the index added without a
+// conversion instruction (identical result).
+__device__ __forceinline__ double abs_coord_d(int i, double o, double d, double half) {
+    return __dsub_rn(__dmul_rn(__dadd_rn(int_to_double(i), o), d), half);
 }
 
 }  // namespace oec

@@ -11,6 +11,7 @@
 //  * the deposit is an int64 fixed-point sum, so the grid is independent of
 //    particle order and the total charge is conserved exactly.
 #include <math.h>
+#include <stdlib.h>
 
 #include "oec_common.cuh"
 
@@ -221,62 +222,143 @@ __device__ __forceinline__ bool inside_cutcell(const BoundaryConst &b, int cell,
 
 // Quantised corner charges of one particle; the four parts sum exactly to
 // llrint(w * wscale) so the deposited total is independent of splitting.
-__device__ __forceinline__ void corner_charges(float w, float fx, float fy, double wscale,
+// gx, gy are the in-cell offsets widened to f64.  Round-to-nearest f64
+// products and rint_i64 give the same parts as llrint of the plain products.
+__device__ __forceinline__ void corner_charges(float w, double gx, double gy, double wscale,
                                                long long v[4]) {
-    long long q = llrint((double)w * wscale);
-    double qd = (double)q;
-    double gx = (double)fx, gy = (double)fy;
-    double hx = 1.0 - gx, hy = 1.0 - gy;
-    v[0] = llrint(qd * (hx * hy));   // LowXLowY  -> node c
-    v[1] = llrint(qd * (gx * hy));   // UpXLowY   -> node c+1
-    v[2] = llrint(qd * (hx * gy));   // LowXUpY   -> node c+nx
-    v[3] = q - v[0] - v[1] - v[2];   // UpXUpY    -> node c+nx+1
+    double qd, r;
+    long long q = rint_i64(__dmul_rn((double)w, wscale), qd);
+    double hx = __dsub_rn(1.0, gx), hy = __dsub_rn(1.0, gy);
+    v[0] = rint_i64(__dmul_rn(qd, __dmul_rn(hx, hy)), r);   // LowXLowY  -> node c
+    v[1] = rint_i64(__dmul_rn(qd, __dmul_rn(gx, hy)), r);   // UpXLowY   -> node c+1
+    v[2] = rint_i64(__dmul_rn(qd, __dmul_rn(hx, gy)), r);   // LowXUpY   -> node c+nx
+    v[3] = q - v[0] - v[1] - v[2];                          // UpXUpY    -> node c+nx+1
 }
 
-// Warp-cooperative deposit of one particle per lane (key < 0: nothing).
-__device__ __forceinline__ void deposit_warp(int key, long long v[4], unsigned long long *rho, int nx) {
-    if (!__any_sync(kFullMask, key >= 0)) return;
-    bool head = warp_segment_sum4(key, v);
-    if (head && key >= 0) {
-        atomicAdd(rho + key, (unsigned long long)v[0]);
-        atomicAdd(rho + key + 1, (unsigned long long)v[1]);
-        atomicAdd(rho + key + nx, (unsigned long long)v[2]);
-        atomicAdd(rho + key + nx + 1, (unsigned long long)v[3]);
+__device__ __forceinline__ void add_node4(unsigned long long *rho, int key, int nx, const long long v[4]) {
+    atomicAdd(rho + key, (unsigned long long)v[0]);
+    atomicAdd(rho + key + 1, (unsigned long long)v[1]);
+    atomicAdd(rho + key + nx, (unsigned long long)v[2]);
+    atomicAdd(rho + key + nx + 1, (unsigned long long)v[3]);
+}
+
+// A CTA's deposit window: kWinRows x kWinCols node sums in shared memory,
+// anchored 3 cells left of and 2 cells below the cell of the chunk's first
+// particle.  Cell-ordered storage puts a chunk's 1024 particles in a short run
+// of one row; pushes move some of them to neighbouring cells and rows, which
+// cuts warps into many short key runs but keeps the chunk inside the window.
+// Nodes are summed here and sent to the grid once per chunk; a cell whose
+// four nodes fall outside the window is added to the grid directly, so any
+// particle order gives the same exact result.
+//
+// An int64 charge x is held as three 32-bit planes, x = lo + mid*2^21 +
+// hi*2^42 with lo, mid the 21-bit fields of x and hi = x >> 42 (signed), and
+// each plane is summed with fire-and-forget 32-bit shared atomics (a 64-bit
+// shared add would need a compare-and-swap loop or a carry read back).  A node
+// takes at most one add per particle of the chunk (1024), so the lo and mid
+// sums stay below 2^31 and the hi sum, with |x| < 2^52, below 2^20: no plane
+// overflows, and the recombined total is exact.
+//
+// Dense cells put most lanes of a warp on the same few nodes, and same-address
+// shared atomics serialise; each node therefore has kWinCopies copies of its
+// planes, lane l adding to copy l % kWinCopies, and the flush sums the copies.
+// Layout: word (entry * 3 + plane) * kWinCopies + copy.
+constexpr int kWinRows = 6, kWinCols = 64, kWinNodes = kWinRows * kWinCols;
+constexpr int kWinCopies = 8;
+constexpr int kWinWords = kWinNodes * 3 * kWinCopies;
+
+struct NodeWindow {
+    unsigned *v;  // shared, kWinWords
+    int ox, oy;   // node (column, row) of entry 0
+
+    __device__ __forceinline__ void add_entry(int e, long long x) const {
+        const unsigned lo = (unsigned)x & 0x1fffffu;
+        const unsigned mid = (unsigned)(x >> 21) & 0x1fffffu;
+        const unsigned hi = (unsigned)(x >> 42);
+        unsigned *w = v + e * (3 * kWinCopies) + (threadIdx.x & (kWinCopies - 1));
+        if (lo) atomicAdd(w, lo);
+        if (mid) atomicAdd(w + kWinCopies, mid);
+        if (hi) atomicAdd(w + 2 * kWinCopies, hi);
     }
-}
 
-// Deposit of a thread's four consecutive particles.  Cell-sorted storage
-// makes them share one or two cells: the first two distinct cells are summed
-// in registers and reduced across the warp (two rounds at most); any further
-// cell, rare for sorted data, is added directly.
-__device__ __forceinline__ void deposit_thread4(const int key[4], const float w[4], const float fx[4],
-                                                const float fy[4], double wscale, unsigned long long *rho,
-                                                int nx) {
-    long long a0[4] = {0, 0, 0, 0}, a1[4] = {0, 0, 0, 0};
-    int k0 = -1, k1 = -1;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        if (key[j] < 0) continue;
-        long long v[4];
-        corner_charges(w[j], fx[j], fy[j], wscale, v);
-        if (k0 < 0 || key[j] == k0) {
-            k0 = key[j];
-#pragma unroll
-            for (int t = 0; t < 4; ++t) a0[t] += v[t];
-        } else if (k1 < 0 || key[j] == k1) {
-            k1 = key[j];
-#pragma unroll
-            for (int t = 0; t < 4; ++t) a1[t] += v[t];
+    __device__ __forceinline__ void add(int key, const long long q[4], unsigned long long *rho, int nx,
+                                        unsigned long long nx_magic) const {
+        int ix, iy;
+        split_cell_m(key, nx, nx_magic, ix, iy);
+        const int rx = ix - ox, ry = iy - oy;
+        if ((unsigned)rx < (unsigned)(kWinCols - 1) && (unsigned)ry < (unsigned)(kWinRows - 1)) {
+            const int e = ry * kWinCols + rx;
+            add_entry(e, q[0]);
+            add_entry(e + 1, q[1]);
+            add_entry(e + kWinCols, q[2]);
+            add_entry(e + kWinCols + 1, q[3]);
         } else {
-            atomicAdd(rho + key[j], (unsigned long long)v[0]);
-            atomicAdd(rho + key[j] + 1, (unsigned long long)v[1]);
-            atomicAdd(rho + key[j] + nx, (unsigned long long)v[2]);
-            atomicAdd(rho + key[j] + nx + 1, (unsigned long long)v[3]);
+            add_node4(rho, key, nx, q);
         }
     }
-    deposit_warp(k0, a0, rho, nx);
-    deposit_warp(k1, a1, rho, nx);
+};
+
+// Window anchor from the chunk's first cell (clamped to a valid cell).
+__device__ __forceinline__ void window_anchor(NodeWindow &nw, int first, int ncell, int nx,
+                                              unsigned long long nx_magic) {
+    first = min(max(first, 0), ncell - 1);
+    int bx, by;
+    split_cell_m(first, nx, nx_magic, bx, by);
+    nw.ox = bx - 3;
+    nw.oy = by - 2;
 }
+
+__device__ __forceinline__ unsigned sum_copies(const uint4 &a, const uint4 &b) {
+    return a.x + a.y + a.z + a.w + b.x + b.y + b.z + b.w;  // < 2^31 in total (see above)
+}
+
+// Send the window's nonzero nodes to the grid and clear it (all threads of
+// the CTA, after a barrier that follows the last add).  Only entries that a
+// valid cell wrote are nonzero, so every node sent is on the grid.
+__device__ __forceinline__ void window_flush(const NodeWindow &nw, unsigned long long *rho, int nx) {
+    static_assert(kWinCopies == 8, "flush reads the copies of a plane as two uint4");
+    for (int e = threadIdx.x; e < kWinNodes; e += blockDim.x) {
+        uint4 *w = reinterpret_cast<uint4 *>(nw.v + e * (3 * kWinCopies));
+        const uint4 l0 = w[0], l1 = w[1], m0 = w[2], m1 = w[3], h0 = w[4], h1 = w[5];
+        const unsigned lo = sum_copies(l0, l1), mid = sum_copies(m0, m1), hi = sum_copies(h0, h1);
+        if (lo | mid | hi) {
+            const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+            w[0] = z; w[1] = z; w[2] = z; w[3] = z; w[4] = z; w[5] = z;
+            const long long x = (long long)lo + ((long long)mid << 21) + (long long)(int)hi * (1LL << 42);
+            if (x != 0) atomicAdd(rho + (nw.oy + e / kWinCols) * nx + nw.ox + e % kWinCols, (unsigned long long)x);
+        }
+    }
+}
+
+// A thread's deposit accumulator: charges of consecutive particles in the
+// same cell are summed in registers (cell-ordered storage puts a thread's
+// four consecutive particles in one or two cells) and a run goes to the node
+// window when the cell changes.
+struct DepAcc {
+    int k;
+    long long a[4];
+    __device__ __forceinline__ void reset() {
+        k = -1;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) a[t] = 0;
+    }
+    __device__ __forceinline__ void add(int key, const long long v[4], const NodeWindow &nw,
+                                        unsigned long long *rho, int nx, unsigned long long nx_magic) {
+        if (key != k) {
+            if (k >= 0) nw.add(k, a, rho, nx, nx_magic);
+            k = key;
+#pragma unroll
+            for (int t = 0; t < 4; ++t) a[t] = v[t];
+        } else {
+#pragma unroll
+            for (int t = 0; t < 4; ++t) a[t] += v[t];
+        }
+    }
+    __device__ __forceinline__ void deposit(const NodeWindow &nw, unsigned long long *rho, int nx,
+                                            unsigned long long nx_magic) const {
+        if (k >= 0) nw.add(k, a, rho, nx, nx_magic);
+    }
+};
 
 // ------------------------------------------------------- fused kernel
 
@@ -292,6 +374,7 @@ struct FusedArgs {
     int nx, ny;
     int ncell;               // cells with all four corners on the grid: G - nx - 1
     float inv_nx;
+    unsigned long long nx_magic;  // split_magic(nx)
     double dx, dy, lxh, lyh;
     uint32_t *mask;
     unsigned long long *rho;
@@ -300,17 +383,177 @@ struct FusedArgs {
     int64_t capacity;
 };
 
+struct Tally {
+    int absorbed = 0, nonfinite = 0, clipped = 0, outgrid = 0;
+};
+
+// One thread's group of kPer consecutive particles (float4 group q), its
+// SoA fields already in registers: gather, push, move, wall test, write-back,
+// absorbed bits and the deposit of the survivors.
 template <int TB, int KIND, bool DEP>
-__global__ void __launch_bounds__(kThreads) k_push_gather(FusedArgs a) {
-    const int n = *a.count;
+__device__ __forceinline__ void process_group(const FusedArgs &a, int q, int n, double wscale, int4 c4, float4 fx4,
+                                              float4 fy4, float4 vx4, float4 vy4, float4 vz4, float4 w4,
+                                              Tally &t, const NodeWindow &nw) {
     const int lane = threadIdx.x & 31;
+    const int base = q * kPer;
+    int cc[4] = {c4.x, c4.y, c4.z, c4.w};
+    float fx[4] = {fx4.x, fx4.y, fx4.z, fx4.w};
+    float fy[4] = {fy4.x, fy4.y, fy4.z, fy4.w};
+    float vx[4] = {vx4.x, vx4.y, vx4.z, vx4.w};
+    float vy[4] = {vy4.x, vy4.y, vy4.z, vy4.w};
+    float vz[4] = {vz4.x, vz4.y, vz4.z, vz4.w};
+    float ww[4] = {w4.x, w4.y, w4.z, w4.w};
+    unsigned nib = 0;
+    DepAcc acc;
+    if (DEP) acc.reset();
+
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+        if (base + j >= n) continue;
+        const int c = cc[j];
+        if ((unsigned)c >= (unsigned)a.ncell) {  // not a valid interpolation cell
+            nib |= 1u << j;
+            ++t.outgrid;
+            continue;
+        }
+        // --- gather at the current position (particles.pyx:354-372)
+        float gx = fx[j], gy = fy[j];
+        float w00 = (1.0f - gx) * (1.0f - gy), w10 = gx * (1.0f - gy);
+        float w01 = (1.0f - gx) * gy, w11 = gx * gy;
+        float4 qx = __ldg(&a.etab[2 * c]);
+        float4 qy = __ldg(&a.etab[2 * c + 1]);
+        float ex = corner_sum(qx, w00, w10, w01, w11);
+        float ey = corner_sum(qy, w00, w10, w01, w11);
+        float bx = 0.f, by = 0.f, bz = 0.f;
+        if (TB == 2) {
+            bx = corner_sum(__ldg(&a.btab[3 * c]), w00, w10, w01, w11);
+            by = corner_sum(__ldg(&a.btab[3 * c + 1]), w00, w10, w01, w11);
+            bz = corner_sum(__ldg(&a.btab[3 * c + 2]), w00, w10, w01, w11);
+        }
+        // --- push
+        boris<TB>(a.k, ex, ey, bx, by, bz, vx[j], vy[j], vz[j]);
+        // --- move in cell units and carry whole cells into the index
+        float nxo = gx + a.k.dtdxi * vx[j];
+        float nyo = gy + a.k.dtdyi * vy[j];
+        int ix, iy;
+        split_cell_m(c, a.nx, a.nx_magic, ix, iy);
+        bool finite = isfinite(nxo) && isfinite(nyo);
+        bool out = false;
+        if (!finite) {
+            ++t.nonfinite;
+            out = true;
+            fx[j] = nxo;
+            fy[j] = nyo;
+        } else {
+            float sx, sy;
+            const int isx = floor_small(fminf(fmaxf(nxo, -1048576.f), 1048576.f), sx);
+            const int isy = floor_small(fminf(fmaxf(nyo, -1048576.f), 1048576.f), sy);
+            nxo -= sx;
+            nyo -= sy;
+            ix += isx;
+            iy += isy;
+            if (nxo >= 1.0f) { nxo = 0.0f; ix += 1; }
+            if (nyo >= 1.0f) { nyo = 0.0f; iy += 1; }
+            if (KIND == OEC_BOUNDARY_CUTCELL) {
+                // _clipParticleDataToGrid (particleBoundary.pyx:485-508):
+                // keep the point 1e-6 cells inside the extended grid.
+                bool clip = false;
+                if (ix < 0 || (ix == 0 && nxo < a.b.clip_lo)) { ix = 0; nxo = a.b.clip_lo; clip = true; }
+                if (ix > a.nx - 2) { ix = a.nx - 2; nxo = 1.0f - a.b.clip_lo; clip = true; }
+                if (ix == a.nx - 2 && nxo > 1.0f - a.b.clip_lo) { nxo = 1.0f - a.b.clip_lo; clip = true; }
+                if (iy < 0 || (iy == 0 && nyo < a.b.clip_lo)) { iy = 0; nyo = a.b.clip_lo; clip = true; }
+                if (iy > a.ny - 2) { iy = a.ny - 2; nyo = 1.0f - a.b.clip_lo; clip = true; }
+                if (iy == a.ny - 2 && nyo > 1.0f - a.b.clip_lo) { nyo = 1.0f - a.b.clip_lo; clip = true; }
+                t.clipped += clip ? 1 : 0;
+            } else if (ix < 0 || iy < 0 || ix > a.nx - 2 || iy > a.ny - 2) {
+                // Left the extended grid: outside any rect/ellipse wall.
+                // Keep the old (valid) cell and the unfloored offset so
+                // the absolute position stays exact for the wall
+                // intersection and no packed index wraps around.
+                out = true;
+                ++t.outgrid;
+                nxo = gx + a.k.dtdxi * vx[j];
+                nyo = gy + a.k.dtdyi * vy[j];
+                ix = -1;
+            }
+            fx[j] = nxo;
+            fy[j] = nyo;
+            if (ix >= 0) cc[j] = ix + iy * a.nx;
+            if (!out) {
+                const double dox = (double)nxo, doy = (double)nyo;
+                double x = abs_coord_d(ix, dox, a.dx, a.lxh);
+                double y = abs_coord_d(iy, doy, a.dy, a.lyh);
+                bool in;
+                if (KIND == OEC_BOUNDARY_RECT)
+                    in = inside_rect(a.b, x, y);
+                else if (KIND == OEC_BOUNDARY_ELLIPSE)
+                    in = inside_ellipse(a.b, x, y);
+                else
+                    in = inside_cutcell(a.b, cc[j], x, y);
+                out = !in;
+                // --- charge of the survivor at its new position
+                if (DEP && !out) {
+                    long long v[4];
+                    corner_charges(ww[j], dox, doy, wscale, v);
+                    acc.add(cc[j], v, nw, a.rho, a.nx, a.nx_magic);
+                }
+            }
+        }
+        if (out) nib |= 1u << j;
+    }
+
+    // --- write back (invalid tail slots are rewritten unchanged)
+    reinterpret_cast<int4 *>(a.cell)[q] = make_int4(cc[0], cc[1], cc[2], cc[3]);
+    reinterpret_cast<float4 *>(a.ox)[q] = make_float4(fx[0], fx[1], fx[2], fx[3]);
+    reinterpret_cast<float4 *>(a.oy)[q] = make_float4(fy[0], fy[1], fy[2], fy[3]);
+    reinterpret_cast<float4 *>(a.vx)[q] = make_float4(vx[0], vx[1], vx[2], vx[3]);
+    reinterpret_cast<float4 *>(a.vy)[q] = make_float4(vy[0], vy[1], vy[2], vy[3]);
+    reinterpret_cast<float4 *>(a.vz)[q] = make_float4(vz[0], vz[1], vz[2], vz[3]);
+
+    // --- absorbed bits: 8 lanes x 4 particles = one 32-bit word
+    unsigned word = nib << (4 * (lane & 7));
+    word |= __shfl_xor_sync(kFullMask, word, 1);
+    word |= __shfl_xor_sync(kFullMask, word, 2);
+    word |= __shfl_xor_sync(kFullMask, word, 4);
+    if ((lane & 7) == 0) a.mask[q >> 3] = word;
+    t.absorbed += __popc(nib);
+
+    // --- deposit of the surviving particles at their new position
+    if (DEP) acc.deposit(nw, a.rho, a.nx, a.nx_magic);
+}
+
+template <int KIND>
+__device__ __forceinline__ void publish_tally(const FusedArgs &a, const Tally &t) {
+    const int lane = threadIdx.x & 31;
+    int s = __reduce_add_sync(kFullMask, t.absorbed);
+    if (lane == 0 && s) atomicAdd(&a.status->n_absorbed, s);
+    s = __reduce_add_sync(kFullMask, t.nonfinite);
+    if (lane == 0 && s) atomicAdd(&a.status->n_nonfinite, s);
+    s = __reduce_add_sync(kFullMask, t.outgrid);
+    if (lane == 0 && s) atomicAdd(&a.status->n_out_of_grid, s);
+    if (KIND == OEC_BOUNDARY_CUTCELL) {
+        s = __reduce_add_sync(kFullMask, t.clipped);
+        if (lane == 0 && s) atomicAdd(&a.status->n_clipped, s);
+    }
+}
+
+constexpr int fused_min_blocks(int tb, int kind) { return (tb == 2 || kind == OEC_BOUNDARY_CUTCELL) ? 3 : 4; }
+
+// Persistent loop over chunks of kChunk particles; with the deposit, two
+// barriers per chunk bracket the use of the CTA's node window.
+template <int TB, int KIND, bool DEP>
+__global__ void __launch_bounds__(kThreads, fused_min_blocks(TB, KIND)) k_push_gather(FusedArgs a) {
+    __shared__ __align__(16) unsigned win[DEP ? kWinWords : 4];
+    __shared__ int first_cell;
+    const int n = min(*a.count, (int)a.capacity);
     const int nchunks = (n + kChunk - 1) / kChunk;
     const double wscale = DEP ? *a.wscale : 0.0;
-    int absorbed_local = 0, nonfinite_local = 0, clipped_local = 0, outgrid_local = 0;
-
+    Tally t;
+    NodeWindow nw{win, 0, 0};
+    if (DEP)
+        for (int e = threadIdx.x; e < kWinWords; e += kThreads) win[e] = 0u;
     for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
         const int q = chunk * kThreads + threadIdx.x;  // float4 group index
-        const int base = q * kPer;
         int4 c4 = reinterpret_cast<const int4 *>(a.cell)[q];
         float4 fx4 = reinterpret_cast<const float4 *>(a.ox)[q];
         float4 fy4 = reinterpret_cast<const float4 *>(a.oy)[q];
@@ -318,139 +561,19 @@ __global__ void __launch_bounds__(kThreads) k_push_gather(FusedArgs a) {
         float4 vy4 = reinterpret_cast<const float4 *>(a.vy)[q];
         float4 vz4 = reinterpret_cast<const float4 *>(a.vz)[q];
         float4 w4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (DEP) w4 = reinterpret_cast<const float4 *>(a.w)[q];
-
-        int cc[4] = {c4.x, c4.y, c4.z, c4.w};
-        float fx[4] = {fx4.x, fx4.y, fx4.z, fx4.w};
-        float fy[4] = {fy4.x, fy4.y, fy4.z, fy4.w};
-        float vx[4] = {vx4.x, vx4.y, vx4.z, vx4.w};
-        float vy[4] = {vy4.x, vy4.y, vy4.z, vy4.w};
-        float vz[4] = {vz4.x, vz4.y, vz4.z, vz4.w};
-        float ww[4] = {w4.x, w4.y, w4.z, w4.w};
-        unsigned nib = 0;
-        int key[4];
-
-#pragma unroll
-        for (int j = 0; j < kPer; ++j) {
-            key[j] = -1;
-            if (base + j >= n) continue;
-            const int c = cc[j];
-            if ((unsigned)c >= (unsigned)a.ncell) {  // not a valid interpolation cell
-                nib |= 1u << j;
-                ++outgrid_local;
-                continue;
-            }
-            // --- gather at the current position (particles.pyx:354-372)
-            float gx = fx[j], gy = fy[j];
-            float w00 = (1.0f - gx) * (1.0f - gy), w10 = gx * (1.0f - gy);
-            float w01 = (1.0f - gx) * gy, w11 = gx * gy;
-            float4 qx = __ldg(&a.etab[2 * c]);
-            float4 qy = __ldg(&a.etab[2 * c + 1]);
-            float ex = corner_sum(qx, w00, w10, w01, w11);
-            float ey = corner_sum(qy, w00, w10, w01, w11);
-            float bx = 0.f, by = 0.f, bz = 0.f;
-            if (TB == 2) {
-                bx = corner_sum(__ldg(&a.btab[3 * c]), w00, w10, w01, w11);
-                by = corner_sum(__ldg(&a.btab[3 * c + 1]), w00, w10, w01, w11);
-                bz = corner_sum(__ldg(&a.btab[3 * c + 2]), w00, w10, w01, w11);
-            }
-            // --- push
-            boris<TB>(a.k, ex, ey, bx, by, bz, vx[j], vy[j], vz[j]);
-            // --- move in cell units and carry whole cells into the index
-            float nxo = gx + a.k.dtdxi * vx[j];
-            float nyo = gy + a.k.dtdyi * vy[j];
-            int ix, iy;
-            split_cell(c, a.nx, a.inv_nx, ix, iy);
-            bool finite = isfinite(nxo) && isfinite(nyo);
-            bool out = false;
-            if (!finite) {
-                ++nonfinite_local;
-                out = true;
-                fx[j] = nxo;
-                fy[j] = nyo;
-            } else {
-                float sx = floorf(fminf(fmaxf(nxo, -1048576.f), 1048576.f));
-                float sy = floorf(fminf(fmaxf(nyo, -1048576.f), 1048576.f));
-                nxo -= sx;
-                nyo -= sy;
-                ix += (int)sx;
-                iy += (int)sy;
-                if (nxo >= 1.0f) { nxo = 0.0f; ix += 1; }
-                if (nyo >= 1.0f) { nyo = 0.0f; iy += 1; }
-                if (KIND == OEC_BOUNDARY_CUTCELL) {
-                    // _clipParticleDataToGrid (particleBoundary.pyx:485-508):
-                    // keep the point 1e-6 cells inside the extended grid.
-                    bool clip = false;
-                    if (ix < 0 || (ix == 0 && nxo < a.b.clip_lo)) { ix = 0; nxo = a.b.clip_lo; clip = true; }
-                    if (ix > a.nx - 2) { ix = a.nx - 2; nxo = 1.0f - a.b.clip_lo; clip = true; }
-                    if (ix == a.nx - 2 && nxo > 1.0f - a.b.clip_lo) { nxo = 1.0f - a.b.clip_lo; clip = true; }
-                    if (iy < 0 || (iy == 0 && nyo < a.b.clip_lo)) { iy = 0; nyo = a.b.clip_lo; clip = true; }
-                    if (iy > a.ny - 2) { iy = a.ny - 2; nyo = 1.0f - a.b.clip_lo; clip = true; }
-                    if (iy == a.ny - 2 && nyo > 1.0f - a.b.clip_lo) { nyo = 1.0f - a.b.clip_lo; clip = true; }
-                    clipped_local += clip ? 1 : 0;
-                } else if (ix < 0 || iy < 0 || ix > a.nx - 2 || iy > a.ny - 2) {
-                    // Left the extended grid: outside any rect/ellipse wall.
-                    // Keep the old (valid) cell and the unfloored offset so
-                    // the absolute position stays exact for the wall
-                    // intersection and no packed index wraps around.
-                    out = true;
-                    ++outgrid_local;
-                    nxo = gx + a.k.dtdxi * vx[j];
-                    nyo = gy + a.k.dtdyi * vy[j];
-                    ix = -1;
-                }
-                fx[j] = nxo;
-                fy[j] = nyo;
-                if (ix >= 0) cc[j] = ix + iy * a.nx;
-                if (!out) {
-                    double x = abs_coord(ix, nxo, a.dx, a.lxh);
-                    double y = abs_coord(iy, nyo, a.dy, a.lyh);
-                    bool in;
-                    if (KIND == OEC_BOUNDARY_RECT)
-                        in = inside_rect(a.b, x, y);
-                    else if (KIND == OEC_BOUNDARY_ELLIPSE)
-                        in = inside_ellipse(a.b, x, y);
-                    else
-                        in = inside_cutcell(a.b, cc[j], x, y);
-                    out = !in;
-                }
-            }
-            if (out) {
-                nib |= 1u << j;
-            } else if (DEP) {
-                key[j] = cc[j];
-            }
+        if (DEP) {
+            w4 = reinterpret_cast<const float4 *>(a.w)[q];
+            if (threadIdx.x == 0) first_cell = c4.x;
+            __syncthreads();  // anchor published; the previous chunk's flush is done
+            window_anchor(nw, first_cell, a.ncell, a.nx, a.nx_magic);
         }
-
-        // --- write back (invalid tail slots are rewritten unchanged)
-        reinterpret_cast<int4 *>(a.cell)[q] = make_int4(cc[0], cc[1], cc[2], cc[3]);
-        reinterpret_cast<float4 *>(a.ox)[q] = make_float4(fx[0], fx[1], fx[2], fx[3]);
-        reinterpret_cast<float4 *>(a.oy)[q] = make_float4(fy[0], fy[1], fy[2], fy[3]);
-        reinterpret_cast<float4 *>(a.vx)[q] = make_float4(vx[0], vx[1], vx[2], vx[3]);
-        reinterpret_cast<float4 *>(a.vy)[q] = make_float4(vy[0], vy[1], vy[2], vy[3]);
-        reinterpret_cast<float4 *>(a.vz)[q] = make_float4(vz[0], vz[1], vz[2], vz[3]);
-
-        // --- absorbed bits: 8 lanes x 4 particles = one 32-bit word
-        unsigned word = nib << (4 * (lane & 7));
-        word |= __shfl_xor_sync(kFullMask, word, 1);
-        word |= __shfl_xor_sync(kFullMask, word, 2);
-        word |= __shfl_xor_sync(kFullMask, word, 4);
-        if ((lane & 7) == 0) a.mask[q >> 3] = word;
-        absorbed_local += __popc(nib);
-
-        // --- deposit of the surviving particles at their new position
-        if (DEP) deposit_thread4(key, ww, fx, fy, wscale, a.rho, a.nx);
+        process_group<TB, KIND, DEP>(a, q, n, wscale, c4, fx4, fy4, vx4, vy4, vz4, w4, t, nw);
+        if (DEP) {
+            __syncthreads();  // every add of this chunk is in the window
+            window_flush(nw, a.rho, a.nx);
+        }
     }
-    int s = __reduce_add_sync(kFullMask, absorbed_local);
-    if (lane == 0 && s) atomicAdd(&a.status->n_absorbed, s);
-    s = __reduce_add_sync(kFullMask, nonfinite_local);
-    if (lane == 0 && s) atomicAdd(&a.status->n_nonfinite, s);
-    s = __reduce_add_sync(kFullMask, outgrid_local);
-    if (lane == 0 && s) atomicAdd(&a.status->n_out_of_grid, s);
-    if (KIND == OEC_BOUNDARY_CUTCELL) {
-        s = __reduce_add_sync(kFullMask, clipped_local);
-        if (lane == 0 && s) atomicAdd(&a.status->n_clipped, s);
-    }
+    publish_tally<KIND>(a, t);
 }
 
 // ------------------------------------------------------ standalone deposit
@@ -458,14 +581,22 @@ __global__ void __launch_bounds__(kThreads) k_push_gather(FusedArgs a) {
 __global__ void __launch_bounds__(kThreads)
     k_deposit(const int32_t *__restrict__ cell, const float *__restrict__ ox,
               const float *__restrict__ oy, const float *__restrict__ w, const int32_t *count, int nx,
-              int ncell, unsigned long long *rho, const double *wscale_p) {
-    const int n = *count;
+              int ncell, unsigned long long nx_magic, int capacity, unsigned long long *rho,
+              const double *wscale_p) {
+    __shared__ __align__(16) unsigned win[kWinWords];
+    __shared__ int first_cell;
+    const int n = min(*count, capacity);
     const double wscale = *wscale_p;
     const int nchunks = (n + kChunk - 1) / kChunk;
+    NodeWindow nw{win, 0, 0};
+    for (int e = threadIdx.x; e < kWinWords; e += kThreads) win[e] = 0u;
     for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
         const int q = chunk * kThreads + threadIdx.x;
         const int base = q * kPer;
         int4 c4 = reinterpret_cast<const int4 *>(cell)[q];
+        if (threadIdx.x == 0) first_cell = c4.x;
+        __syncthreads();
+        window_anchor(nw, first_cell, ncell, nx, nx_magic);
         float4 fx4 = reinterpret_cast<const float4 *>(ox)[q];
         float4 fy4 = reinterpret_cast<const float4 *>(oy)[q];
         float4 w4 = reinterpret_cast<const float4 *>(w)[q];
@@ -473,10 +604,19 @@ __global__ void __launch_bounds__(kThreads)
         float fx[4] = {fx4.x, fx4.y, fx4.z, fx4.w};
         float fy[4] = {fy4.x, fy4.y, fy4.z, fy4.w};
         float ww[4] = {w4.x, w4.y, w4.z, w4.w};
-        int key[4];
+        DepAcc acc;
+        acc.reset();
 #pragma unroll
-        for (int j = 0; j < kPer; ++j) key[j] = (base + j < n && (unsigned)cc[j] < (unsigned)ncell) ? cc[j] : -1;
-        deposit_thread4(key, ww, fx, fy, wscale, rho, nx);
+        for (int j = 0; j < kPer; ++j) {
+            if (base + j < n && (unsigned)cc[j] < (unsigned)ncell) {
+                long long v[4];
+                corner_charges(ww[j], (double)fx[j], (double)fy[j], wscale, v);
+                acc.add(cc[j], v, nw, rho, nx, nx_magic);
+            }
+        }
+        acc.deposit(nw, rho, nx, nx_magic);
+        __syncthreads();
+        window_flush(nw, rho, nx);
     }
 }
 
@@ -583,9 +723,15 @@ using namespace oec;
 
 // =================================================================== C ABI
 
+static bool aligned16(const void *ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 15u) == 0; }
+
+// The kernels read and write whole float4 groups and whole chunks: every
+// field array 16-byte aligned, capacity a multiple of kChunk.
 static bool valid_particles(const oec_particles_t *p) {
     return p && p->cell && p->ox && p->oy && p->vx && p->vy && p->vz && p->w && p->count &&
-           p->capacity > 0 && (p->capacity % kChunk) == 0;
+           p->capacity > 0 && p->capacity <= INT32_MAX && (p->capacity % kChunk) == 0 && aligned16(p->cell) &&
+           aligned16(p->ox) && aligned16(p->oy) && aligned16(p->vx) && aligned16(p->vy) && aligned16(p->vz) &&
+           aligned16(p->w);
 }
 
 static bool valid_grid(const oec_grid_t *g) {
@@ -826,6 +972,7 @@ static FusedArgs make_fused_args(const GridConst &gc, oec_particles_t *p) {
     a.ny = gc.ny;
     a.ncell = gc.G - gc.nx - 1;
     a.inv_nx = 1.0f / (float)gc.nx;
+    a.nx_magic = split_magic(gc.nx);
     a.dx = gc.dx;
     a.dy = gc.dy;
     a.lxh = gc.lxh;
@@ -882,8 +1029,8 @@ extern "C" int oec_deposit(const oec_grid_t *grid, const oec_particles_t *p, int
     int G = grid->nx * grid->ny;
     if (zero_first) OEC_CUDA_TRY(cudaMemsetAsync(rho_fix_dev, 0, sizeof(int64_t) * (size_t)G, s));
     k_deposit<<<persistent_grid(cap_chunks(p), 8), kThreads, 0, s>>>(
-        p->cell, p->ox, p->oy, p->w, p->count, grid->nx, G - grid->nx - 1,
-        reinterpret_cast<unsigned long long *>(rho_fix_dev),
+        p->cell, p->ox, p->oy, p->w, p->count, grid->nx, G - grid->nx - 1, split_magic(grid->nx),
+        (int)p->capacity, reinterpret_cast<unsigned long long *>(rho_fix_dev),
         wscale_dev);
     OEC_LAUNCH_CHECK();
     return OEC_OK;
