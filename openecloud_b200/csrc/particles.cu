@@ -222,28 +222,33 @@ __device__ __forceinline__ bool inside_cutcell(const BoundaryConst &b, int cell,
 
 // Quantised corner charges of one particle; the four parts sum exactly to
 // llrint(w * wscale) so the deposited total is independent of splitting.
-// gx, gy are the in-cell offsets widened to f64.  Round-to-nearest f64
-// products and rint_i64 give the same parts as llrint of the plain products.
-__device__ __forceinline__ void corner_charges(float w, double gx, double gy, double wscale,
-                                               long long v[4]) {
-    double qd, r;
-    long long q = rint_i64(__dmul_rn((double)w, wscale), qd);
-    double hx = __dsub_rn(1.0, gx), hy = __dsub_rn(1.0, gy);
-    v[0] = rint_i64(__dmul_rn(qd, __dmul_rn(hx, hy)), r);   // LowXLowY  -> node c
-    v[1] = rint_i64(__dmul_rn(qd, __dmul_rn(gx, hy)), r);   // UpXLowY   -> node c+1
-    v[2] = rint_i64(__dmul_rn(qd, __dmul_rn(hx, gy)), r);   // LowXUpY   -> node c+nx
-    v[3] = q - v[0] - v[1] - v[2];                          // UpXUpY    -> node c+nx+1
+// gx, gy are the in-cell offsets widened to f64.  The parts are integers
+// below 2^51 held in doubles: round-to-nearest products and rint_d give the
+// same values as llrint of the plain products, and sums of a few parts stay
+// exact in f64.
+__device__ __forceinline__ double rint_d(double x) {
+    const double C = 6755399441055744.0;  // 1.5 * 2^52: x + C rounds x to an integer (|x| < 2^51)
+    return __dsub_rn(__dadd_rn(x, C), C);
 }
 
-__device__ __forceinline__ void add_node4(unsigned long long *rho, int key, int nx, const long long v[4]) {
-    atomicAdd(rho + key, (unsigned long long)v[0]);
-    atomicAdd(rho + key + 1, (unsigned long long)v[1]);
-    atomicAdd(rho + key + nx, (unsigned long long)v[2]);
-    atomicAdd(rho + key + nx + 1, (unsigned long long)v[3]);
+__device__ __forceinline__ void corner_charges(float w, double gx, double gy, double wscale, double v[4]) {
+    const double qd = rint_d(__dmul_rn((double)w, wscale));
+    const double hx = __dsub_rn(1.0, gx), hy = __dsub_rn(1.0, gy);
+    v[0] = rint_d(__dmul_rn(qd, __dmul_rn(hx, hy)));  // LowXLowY  -> node c
+    v[1] = rint_d(__dmul_rn(qd, __dmul_rn(gx, hy)));  // UpXLowY   -> node c+1
+    v[2] = rint_d(__dmul_rn(qd, __dmul_rn(hx, gy)));  // LowXUpY   -> node c+nx
+    v[3] = __dsub_rn(__dsub_rn(__dsub_rn(qd, v[0]), v[1]), v[2]);  // UpXUpY -> node c+nx+1
+}
+
+__device__ __forceinline__ void add_node4(unsigned long long *rho, int key, int nx, const double v[4]) {
+    atomicAdd(rho + key, (unsigned long long)__double2ll_rn(v[0]));
+    atomicAdd(rho + key + 1, (unsigned long long)__double2ll_rn(v[1]));
+    atomicAdd(rho + key + nx, (unsigned long long)__double2ll_rn(v[2]));
+    atomicAdd(rho + key + nx + 1, (unsigned long long)__double2ll_rn(v[3]));
 }
 
 // A CTA's deposit window: kWinRows x kWinCols node sums in shared memory,
-// anchored 3 cells left of and 2 cells below the cell of the chunk's first
+// anchored 4 cells left of and 4 cells below the cell of the chunk's first
 // particle.  Cell-ordered storage puts a chunk's 1024 particles in a short run
 // of one row; pushes move some of them to neighbouring cells and rows, which
 // cuts warps into many short key runs but keeps the chunk inside the window.
@@ -257,41 +262,47 @@ __device__ __forceinline__ void add_node4(unsigned long long *rho, int key, int 
 // shared add would need a compare-and-swap loop or a carry read back).  A node
 // takes at most one add per particle of the chunk (1024), so the lo and mid
 // sums stay below 2^31 and the hi sum, with |x| < 2^52, below 2^20: no plane
-// overflows, and the recombined total is exact.
+// overflows, and the recombined total is exact.  The hi plane is only touched
+// for charges of 2^42 units or more (small particle stores); the flush skips
+// it when no thread of the CTA wrote it.
 //
 // Dense cells put most lanes of a warp on the same few nodes, and same-address
 // shared atomics serialise; each node therefore has kWinCopies copies of its
 // planes, lane l adding to copy l % kWinCopies, and the flush sums the copies.
 // Layout: word (entry * 3 + plane) * kWinCopies + copy.
-constexpr int kWinRows = 6, kWinCols = 64, kWinNodes = kWinRows * kWinCols;
-constexpr int kWinCopies = 8;
+constexpr int kWinRows = 10, kWinCols = 40, kWinNodes = kWinRows * kWinCols;
+constexpr int kWinCopies = 4;
 constexpr int kWinWords = kWinNodes * 3 * kWinCopies;
 
 struct NodeWindow {
-    unsigned *v;  // shared, kWinWords
-    int ox, oy;   // node (column, row) of entry 0
+    unsigned *v;   // shared, kWinWords
+    int ox, oy;    // node (column, row) of entry 0
+    bool hi_used;  // this thread wrote the hi plane since the last flush
 
-    __device__ __forceinline__ void add_entry(int e, long long x) const {
+    __device__ __forceinline__ void add_entry(int e, long long x) {
         const unsigned lo = (unsigned)x & 0x1fffffu;
         const unsigned mid = (unsigned)(x >> 21) & 0x1fffffu;
         const unsigned hi = (unsigned)(x >> 42);
         unsigned *w = v + e * (3 * kWinCopies) + (threadIdx.x & (kWinCopies - 1));
         if (lo) atomicAdd(w, lo);
         if (mid) atomicAdd(w + kWinCopies, mid);
-        if (hi) atomicAdd(w + 2 * kWinCopies, hi);
+        if (hi) {
+            atomicAdd(w + 2 * kWinCopies, hi);
+            hi_used = true;
+        }
     }
 
-    __device__ __forceinline__ void add(int key, const long long q[4], unsigned long long *rho, int nx,
-                                        unsigned long long nx_magic) const {
+    __device__ __forceinline__ void add(int key, const double q[4], unsigned long long *rho, int nx,
+                                        unsigned long long nx_magic) {
         int ix, iy;
         split_cell_m(key, nx, nx_magic, ix, iy);
         const int rx = ix - ox, ry = iy - oy;
         if ((unsigned)rx < (unsigned)(kWinCols - 1) && (unsigned)ry < (unsigned)(kWinRows - 1)) {
             const int e = ry * kWinCols + rx;
-            add_entry(e, q[0]);
-            add_entry(e + 1, q[1]);
-            add_entry(e + kWinCols, q[2]);
-            add_entry(e + kWinCols + 1, q[3]);
+            add_entry(e, __double2ll_rn(q[0]));
+            add_entry(e + 1, __double2ll_rn(q[1]));
+            add_entry(e + kWinCols, __double2ll_rn(q[2]));
+            add_entry(e + kWinCols + 1, __double2ll_rn(q[3]));
         } else {
             add_node4(rho, key, nx, q);
         }
@@ -304,26 +315,30 @@ __device__ __forceinline__ void window_anchor(NodeWindow &nw, int first, int nce
     first = min(max(first, 0), ncell - 1);
     int bx, by;
     split_cell_m(first, nx, nx_magic, bx, by);
-    nw.ox = bx - 3;
-    nw.oy = by - 2;
+    nw.ox = bx - 4;
+    nw.oy = by - 4;
 }
 
-__device__ __forceinline__ unsigned sum_copies(const uint4 &a, const uint4 &b) {
-    return a.x + a.y + a.z + a.w + b.x + b.y + b.z + b.w;  // < 2^31 in total (see above)
-}
+__device__ __forceinline__ unsigned sum4(const uint4 &a) { return a.x + a.y + a.z + a.w; }
 
 // Send the window's nonzero nodes to the grid and clear it (all threads of
-// the CTA, after a barrier that follows the last add).  Only entries that a
-// valid cell wrote are nonzero, so every node sent is on the grid.
-__device__ __forceinline__ void window_flush(const NodeWindow &nw, unsigned long long *rho, int nx) {
-    static_assert(kWinCopies == 8, "flush reads the copies of a plane as two uint4");
+// the CTA, after a barrier that follows the last add; any_hi = some thread
+// wrote the hi plane).  Only entries that a valid cell wrote are nonzero, so
+// every node sent is on the grid.
+__device__ __forceinline__ void window_flush(const NodeWindow &nw, bool any_hi, unsigned long long *rho, int nx) {
+    static_assert(kWinCopies == 4, "flush reads the copies of a plane as one uint4");
+    const uint4 z = make_uint4(0u, 0u, 0u, 0u);
     for (int e = threadIdx.x; e < kWinNodes; e += blockDim.x) {
         uint4 *w = reinterpret_cast<uint4 *>(nw.v + e * (3 * kWinCopies));
-        const uint4 l0 = w[0], l1 = w[1], m0 = w[2], m1 = w[3], h0 = w[4], h1 = w[5];
-        const unsigned lo = sum_copies(l0, l1), mid = sum_copies(m0, m1), hi = sum_copies(h0, h1);
+        const unsigned lo = sum4(w[0]), mid = sum4(w[1]);
+        unsigned hi = 0u;
+        if (any_hi) {
+            hi = sum4(w[2]);
+            w[2] = z;
+        }
         if (lo | mid | hi) {
-            const uint4 z = make_uint4(0u, 0u, 0u, 0u);
-            w[0] = z; w[1] = z; w[2] = z; w[3] = z; w[4] = z; w[5] = z;
+            w[0] = z;
+            w[1] = z;
             const long long x = (long long)lo + ((long long)mid << 21) + (long long)(int)hi * (1LL << 42);
             if (x != 0) atomicAdd(rho + (nw.oy + e / kWinCols) * nx + nw.ox + e % kWinCols, (unsigned long long)x);
         }
@@ -332,18 +347,19 @@ __device__ __forceinline__ void window_flush(const NodeWindow &nw, unsigned long
 
 // A thread's deposit accumulator: charges of consecutive particles in the
 // same cell are summed in registers (cell-ordered storage puts a thread's
-// four consecutive particles in one or two cells) and a run goes to the node
-// window when the cell changes.
+// four consecutive particles in one or two cells; the f64 sums of integer
+// parts below 2^50 are exact) and a run goes to the node window when the
+// cell changes.
 struct DepAcc {
     int k;
-    long long a[4];
+    double a[4];
     __device__ __forceinline__ void reset() {
         k = -1;
 #pragma unroll
-        for (int t = 0; t < 4; ++t) a[t] = 0;
+        for (int t = 0; t < 4; ++t) a[t] = 0.0;
     }
-    __device__ __forceinline__ void add(int key, const long long v[4], const NodeWindow &nw,
-                                        unsigned long long *rho, int nx, unsigned long long nx_magic) {
+    __device__ __forceinline__ void add(int key, const double v[4], NodeWindow &nw, unsigned long long *rho, int nx,
+                                        unsigned long long nx_magic) {
         if (key != k) {
             if (k >= 0) nw.add(k, a, rho, nx, nx_magic);
             k = key;
@@ -351,10 +367,10 @@ struct DepAcc {
             for (int t = 0; t < 4; ++t) a[t] = v[t];
         } else {
 #pragma unroll
-            for (int t = 0; t < 4; ++t) a[t] += v[t];
+            for (int t = 0; t < 4; ++t) a[t] = __dadd_rn(a[t], v[t]);
         }
     }
-    __device__ __forceinline__ void deposit(const NodeWindow &nw, unsigned long long *rho, int nx,
+    __device__ __forceinline__ void deposit(NodeWindow &nw, unsigned long long *rho, int nx,
                                             unsigned long long nx_magic) const {
         if (k >= 0) nw.add(k, a, rho, nx, nx_magic);
     }
@@ -393,7 +409,7 @@ struct Tally {
 template <int TB, int KIND, bool DEP>
 __device__ __forceinline__ void process_group(const FusedArgs &a, int q, int n, double wscale, int4 c4, float4 fx4,
                                               float4 fy4, float4 vx4, float4 vy4, float4 vz4, float4 w4,
-                                              Tally &t, const NodeWindow &nw) {
+                                              Tally &t, NodeWindow &nw) {
     const int lane = threadIdx.x & 31;
     const int base = q * kPer;
     int cc[4] = {c4.x, c4.y, c4.z, c4.w};
@@ -437,7 +453,14 @@ __device__ __forceinline__ void process_group(const FusedArgs &a, int q, int n, 
         float nyo = gy + a.k.dtdyi * vy[j];
         int ix, iy;
         split_cell_m(c, a.nx, a.nx_magic, ix, iy);
-        bool finite = isfinite(nxo) && isfinite(nyo);
+        // huge or non-finite moves take the checked path
+        bool finite = true;
+        float cxo = nxo, cyo = nyo;
+        if (!(fabsf(nxo) < 1048576.f && fabsf(nyo) < 1048576.f)) {
+            finite = isfinite(nxo) && isfinite(nyo);
+            cxo = fminf(fmaxf(nxo, -1048576.f), 1048576.f);
+            cyo = fminf(fmaxf(nyo, -1048576.f), 1048576.f);
+        }
         bool out = false;
         if (!finite) {
             ++t.nonfinite;
@@ -446,8 +469,8 @@ __device__ __forceinline__ void process_group(const FusedArgs &a, int q, int n, 
             fy[j] = nyo;
         } else {
             float sx, sy;
-            const int isx = floor_small(fminf(fmaxf(nxo, -1048576.f), 1048576.f), sx);
-            const int isy = floor_small(fminf(fmaxf(nyo, -1048576.f), 1048576.f), sy);
+            const int isx = floor_small(cxo, sx);
+            const int isy = floor_small(cyo, sy);
             nxo -= sx;
             nyo -= sy;
             ix += isx;
@@ -493,7 +516,7 @@ __device__ __forceinline__ void process_group(const FusedArgs &a, int q, int n, 
                 out = !in;
                 // --- charge of the survivor at its new position
                 if (DEP && !out) {
-                    long long v[4];
+                    double v[4];
                     corner_charges(ww[j], dox, doy, wscale, v);
                     acc.add(cc[j], v, nw, a.rho, a.nx, a.nx_magic);
                 }
@@ -549,7 +572,7 @@ __global__ void __launch_bounds__(kThreads, fused_min_blocks(TB, KIND)) k_push_g
     const int nchunks = (n + kChunk - 1) / kChunk;
     const double wscale = DEP ? *a.wscale : 0.0;
     Tally t;
-    NodeWindow nw{win, 0, 0};
+    NodeWindow nw{win, 0, 0, false};
     if (DEP)
         for (int e = threadIdx.x; e < kWinWords; e += kThreads) win[e] = 0u;
     for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
@@ -569,8 +592,10 @@ __global__ void __launch_bounds__(kThreads, fused_min_blocks(TB, KIND)) k_push_g
         }
         process_group<TB, KIND, DEP>(a, q, n, wscale, c4, fx4, fy4, vx4, vy4, vz4, w4, t, nw);
         if (DEP) {
-            __syncthreads();  // every add of this chunk is in the window
-            window_flush(nw, a.rho, a.nx);
+            // every add of this chunk is in the window
+            const bool any_hi = __syncthreads_or(nw.hi_used);
+            nw.hi_used = false;
+            window_flush(nw, any_hi, a.rho, a.nx);
         }
     }
     publish_tally<KIND>(a, t);
@@ -588,7 +613,7 @@ __global__ void __launch_bounds__(kThreads)
     const int n = min(*count, capacity);
     const double wscale = *wscale_p;
     const int nchunks = (n + kChunk - 1) / kChunk;
-    NodeWindow nw{win, 0, 0};
+    NodeWindow nw{win, 0, 0, false};
     for (int e = threadIdx.x; e < kWinWords; e += kThreads) win[e] = 0u;
     for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
         const int q = chunk * kThreads + threadIdx.x;
@@ -609,14 +634,15 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
         for (int j = 0; j < kPer; ++j) {
             if (base + j < n && (unsigned)cc[j] < (unsigned)ncell) {
-                long long v[4];
+                double v[4];
                 corner_charges(ww[j], (double)fx[j], (double)fy[j], wscale, v);
                 acc.add(cc[j], v, nw, rho, nx, nx_magic);
             }
         }
         acc.deposit(nw, rho, nx, nx_magic);
-        __syncthreads();
-        window_flush(nw, rho, nx);
+        const bool any_hi = __syncthreads_or(nw.hi_used);
+        nw.hi_used = false;
+        window_flush(nw, any_hi, rho, nx);
     }
 }
 
