@@ -335,13 +335,14 @@ def run_ours(args, rank, world, local_rank):
             peak_src = "measured"
         except Exception:
             pass
+    # DRAM bytes per launch of the fused kernel from the committed ncu summary
+    # (scaled to 2^24 particles there); only meaningful for that size.
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic_push_gather.json")
-    if os.path.exists(tpath):
-        try:
-            traffic = json.load(open(tpath)).get("bytes_per_launch")
-        except Exception:
-            traffic = None
+    tpath = os.path.join(ROOT, "profiles", "push_gather_c2.md")
+    if os.path.exists(tpath) and n == 1 << 24:
+        import re
+        m = re.search(r"^traffic_per_launch_bytes:\s*([0-9]+)", open(tpath).read(), re.M)
+        traffic = int(m.group(1)) if m else None
 
     if e2e is not None:
         _log(f"e2e: {e2e['ms_per_step']:.3f} ms/step")
