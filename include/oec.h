@@ -369,6 +369,59 @@ int oec_spmv_csr(int32_t nrows, const int32_t *ptr_dev, const int32_t *idx_dev, 
 int oec_trsv_levels(int32_t nrows, const int32_t *ptr, const int32_t *idx, int32_t lower, int32_t ncols_dep,
                     int32_t *level_out, int32_t *nlevels_out);
 
+/* ---------------------------------------- iterative Poisson solve (A16) */
+
+/* The reference's system matrix A = S diag(meps) S^T restricted to the inside
+ * nodes (poissonSolver.pyx:41-58) is a 5-point operator; it is stored by edge
+ * on the full extended grid: ex[i] is the weight meps of the x edge between
+ * nodes i and i+1, ey[i] that of the y edge between i and i+nx.  For an
+ * inside node i, (A x)_i = sum over its four edges of meps * (x_i - x_j) with
+ * x_j = 0 for outside nodes j (their value is fixed at 0).  Vectors live on
+ * the full extended grid [G = nx*ny] and are zero outside.  The f32 copies
+ * hold scale32 * the f64 weights (scale32 brings them to order one);
+ * dinv32 = 1 / diag of that scaled operator (0 outside). */
+typedef struct oec_stencil {
+    int32_t nx, ny;
+    const double *ex64, *ey64;
+    const float *ex32, *ey32, *dinv32;
+    const uint8_t *inside;
+    double scale32;
+} oec_stencil_t;
+
+/* y = A x in f64 on the inside nodes, 0 outside (used by the solver's
+ * residual and by the tests; poissonSolver.pyx:57 assembles the same A). */
+int oec_stencil_apply(const oec_stencil_t *st, const double *x_dev, double *y_dev, void *stream);
+
+#define OEC_PRECOND_NONE 0
+#define OEC_PRECOND_JACOBI 1
+#define OEC_PRECOND_CNN 2
+
+typedef struct oec_pcg_stats {
+    int32_t iterations;   /* f32 inner iterations, all refinements */
+    int32_t refinements;  /* f64 residual evaluations */
+    int32_t converged;    /* 1 if the f64 relative residual reached tol */
+    int32_t breakdown;    /* 1 if an inner solve stopped on a non-positive or non-finite curvature */
+    double rel_residual;  /* final ||q - A phi||_2 / ||q||_2 over the inside nodes, in f64 */
+    double rel_residual0; /* the same for the warm start */
+} oec_pcg_stats_t;
+
+int64_t oec_pcg_work_bytes(int32_t nx, int32_t ny);
+
+/* No counterpart in the reference (it only has the direct solve of
+ * poissonSolver.pyx:85).  phi = A^-1 q on the inside nodes by f64 iterative
+ * refinement around an f32 flexible preconditioned conjugate-gradient solve:
+ * each refinement forms r = q - A phi in f64, solves A d = r in f32 to a
+ * relative 2e-5 (or stagnation), and adds d in f64; it stops when
+ * ||r||/||q|| <= tol or after max_iter inner iterations in total.
+ * phi_dev holds the warm start on entry (zeros for none) and the solution on
+ * return (0 outside).  precond: OEC_PRECOND_NONE / _JACOBI / _CNN (precond_ctx
+ * = an oec_cnn_t, see below).  stats (host) reports convergence; the caller
+ * falls back to oec_lu_solve when stats->converged is 0.  work_dev:
+ * oec_pcg_work_bytes.  Synchronises the stream every few iterations. */
+int oec_pcg_solve(const oec_stencil_t *st, const double *q_dev, double *phi_dev, double tol, int32_t max_iter,
+                  int32_t precond, const void *precond_ctx, void *work_dev, oec_pcg_stats_t *stats,
+                  void *stream);
+
 /* ------------------------------------------- grid geometry (A11-A14, host) */
 
 /* Boundary function of the grid (grid.pyx:88-105). */

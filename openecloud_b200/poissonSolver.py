@@ -10,7 +10,11 @@ diag_pivot_thresh 0.1).  The y-derivative operator uses the signed offset
 
 Solve (every step, device): the FP64 LU back-substitution of
 ``oec_lu_solve`` (level-scheduled head rows + dense-inverse tail rows) and
-the CSR product E = phiToE . phi (``oec_spmv_csr``).
+the CSR product E = phiToE . phi (``oec_spmv_csr``).  With ``method='pcg'``
+the solve is iterative instead (``oec_pcg_solve``: f64 residual refinement
+around an f32 flexible PCG on the matrix-free 5-point operator, warm-started
+from the previous phi, Jacobi or learned preconditioner); the LU solve stays
+the fallback whenever the f64 relative residual misses ``pcgTol``.
 """
 import ctypes
 
@@ -34,7 +38,22 @@ class LU_t(ctypes.Structure):
                 ("u_ptr", _P), ("u_idx", _P), ("u_val", _P), ("u_diag", _P), ("tu_inv", _P)]
 
 
-_lib.OTHER_DECLARED.update({"oec_lu_solve", "oec_spmv_csr", "oec_trsv_levels"})
+class Stencil_t(ctypes.Structure):
+    _P = ctypes.c_void_p
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("ex64", _P), ("ey64", _P), ("ex32", _P),
+                ("ey32", _P), ("dinv32", _P), ("inside", _P), ("scale32", ctypes.c_double)]
+
+
+class PcgStats_t(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int32), ("refinements", ctypes.c_int32), ("converged", ctypes.c_int32),
+                ("breakdown", ctypes.c_int32), ("rel_residual", ctypes.c_double),
+                ("rel_residual0", ctypes.c_double)]
+
+
+PRECOND = {"none": 0, "jacobi": 1, "cnn": 2}
+
+_lib.OTHER_DECLARED.update({"oec_lu_solve", "oec_spmv_csr", "oec_trsv_levels", "oec_stencil_apply",
+                            "oec_pcg_work_bytes", "oec_pcg_solve"})
 
 
 def _declare():
@@ -48,6 +67,13 @@ def _declare():
         L.oec_trsv_levels.restype = ctypes.c_int
         L.oec_trsv_levels.argtypes = [ctypes.c_int32, P, P, ctypes.c_int32, ctypes.c_int32, P,
                                       ctypes.POINTER(ctypes.c_int32)]
+        L.oec_stencil_apply.restype = ctypes.c_int
+        L.oec_stencil_apply.argtypes = [ctypes.POINTER(Stencil_t), P, P, P]
+        L.oec_pcg_work_bytes.restype = ctypes.c_int64
+        L.oec_pcg_work_bytes.argtypes = [ctypes.c_int32, ctypes.c_int32]
+        L.oec_pcg_solve.restype = ctypes.c_int
+        L.oec_pcg_solve.argtypes = [ctypes.POINTER(Stencil_t), P, P, ctypes.c_double, ctypes.c_int32,
+                                    ctypes.c_int32, P, P, ctypes.POINTER(PcgStats_t), P]
         L._poisson_declared = True
     return L
 
@@ -94,27 +120,93 @@ def choose_tail(Lcsr, Ucsr, n, launch_us=1.5, gbs=3000.0, max_tail=12288):
     return best[1]
 
 
+def assemble(gridObj):
+    """poissonSolver.pyx:41-58: A = S diag(meps) S^T over the inside nodes.
+
+    Returns (A as CSC, meps [2*npExt] edge weights (x edges then y edges),
+    S = [Px | Py] and the inside node indices)."""
+    nx = gridObj.getNxExt()
+    npn = gridObj.getNpExt()
+    inside = np.nonzero(gridObj.getInsidePoints())[0]
+    pxmt = spsp.identity(npn) - spsp.eye(npn, npn, -1)
+    pymt = spsp.identity(npn) - spsp.eye(npn, npn, -int(nx))
+    st = spsp.hstack([pxmt, pymt])
+    meps = epsilon_0 * np.asarray(gridObj.getDsi()) * np.roll(gridObj.getDst(), npn)
+    a = st.dot(spsp.diags(meps, 0).dot(st.transpose()))[:, inside].tocsc()[inside, :]
+    return a, meps, st, inside
+
+
+def stencil_apply_host(meps, inside_mask, nx, x):
+    """Host restatement of oec_stencil_apply: (A x)_i = sum over the four edges
+    of node i of meps * (x_i - x_j), x_j = 0 outside; 0 on outside nodes."""
+    npn = inside_mask.shape[0]
+    ex, ey = meps[:npn], meps[npn:]
+    x = np.where(inside_mask, x, 0.0)
+    y = np.zeros(npn)
+    i = np.nonzero(inside_mask)[0]
+    y[i] = (ex[i] * (x[i] - x[i + 1]) + ex[i - 1] * (x[i] - x[i - 1]) + ey[i] * (x[i] - x[i + nx]) +
+            ey[i - nx] * (x[i] - x[i - nx]))
+    return y
+
+
 class PoissonSolver:
     """Reference: poissonSolver.pyx:33-67 (setup) and :83-98 (solve, getters)."""
 
-    def __init__(self, gridObj, tail=None):
+    def __init__(self, gridObj, tail=None, method="lu", precond="jacobi", pcgTol=1e-8, pcgMaxIter=4000):
         nx = gridObj.getNxExt()
         npn = gridObj.getNpExt()
         self.gridObj = gridObj
-        self.insidePointsInd = np.nonzero(gridObj.getInsidePoints())[0]
-        pxmt = spsp.identity(npn) - spsp.eye(npn, npn, -1)
-        pymt = spsp.identity(npn) - spsp.eye(npn, npn, -int(nx))
-        st = spsp.hstack([pxmt, pymt])
-        meps = epsilon_0 * np.asarray(gridObj.getDsi()) * np.roll(gridObj.getDst(), npn)
-        a = st.dot(spsp.diags(meps, 0).dot(st.transpose()))[:, self.insidePointsInd].tocsc()[self.insidePointsInd, :]
+        a, meps, st, self.insidePointsInd = assemble(gridObj)
         self.systemMatrix = a
         self.ludecom = spspl.splu(a, permc_spec='MMD_AT_PLUS_A', diag_pivot_thresh=0.1)
         self.phiToEAtGridPoints = gridObj.getEdgeToNode().dot(
             spsp.diags(gridObj.getDsi(), 0, (2 * npn, 2 * npn)).dot(st.transpose()))
         self.n_nodes = npn
         self._device_setup(tail)
+        self._stencil_setup(meps, nx, npn)
         self.phi = D.zeros(npn, torch.float64)
         self.eAtGridPoints = D.zeros(2 * npn, torch.float64)
+        self.method = method
+        self.precond = precond
+        self.pcgTol = float(pcgTol)
+        self.pcgMaxIter = int(pcgMaxIter)
+        self.cnn = None          # a trained network (openecloud_b200.cnn) for precond='cnn'
+        self.lastStats = None    # PcgStats_t of the last iterative solve
+        self.nSolves = 0
+        self.nFallbacks = 0
+
+    def _stencil_setup(self, meps, nx, npn):
+        """Edge weights of A on the full extended grid (oec_stencil_t)."""
+        ex = np.ascontiguousarray(meps[:npn], np.float64)
+        ey = np.ascontiguousarray(meps[npn:], np.float64)
+        inside = np.asarray(self.gridObj.getInsidePoints()).astype(np.uint8)
+        diag = np.zeros(npn)
+        i = np.nonzero(inside)[0]
+        diag[i] = ex[i] + ex[i - 1] + ey[i] + ey[i - nx]
+        scale = 1.0 / float(np.max(np.abs(meps))) if np.max(np.abs(meps)) > 0 else 1.0
+        dinv = np.zeros(npn, np.float32)
+        dinv[i] = (1.0 / (scale * diag[i])).astype(np.float32)
+        k = self._keep
+        k["ex64"], k["ey64"] = D.to_device(ex, torch.float64), D.to_device(ey, torch.float64)
+        k["ex32"] = D.to_device((ex * scale).astype(np.float32), torch.float32)
+        k["ey32"] = D.to_device((ey * scale).astype(np.float32), torch.float32)
+        k["dinv32"] = D.to_device(dinv, torch.float32)
+        k["inside"] = D.to_device(inside, torch.uint8)
+        st = Stencil_t()
+        st.nx, st.ny = nx, npn // nx
+        for name in ("ex64", "ey64", "ex32", "ey32", "dinv32", "inside"):
+            setattr(st, name, D.ptr(k[name]))
+        st.scale32 = scale
+        self._stencil = st
+        self._pcg_work = D.empty(int(_declare().oec_pcg_work_bytes(st.nx, st.ny)), torch.uint8)
+
+    def applyOperator(self, x):
+        """A x on the inside nodes (device f64 [npExt] in and out)."""
+        y = torch.empty_like(x)
+        rc = _declare().oec_stencil_apply(ctypes.byref(self._stencil), x.data_ptr(), y.data_ptr(), D.stream())
+        if rc:
+            raise _lib.OecError("oec_stencil_apply", rc)
+        return y
 
     # -------------------------------------------------------------- setup
     def _device_setup(self, tail):
@@ -181,13 +273,46 @@ class PoissonSolver:
         self.levels = (nl, nu)
 
     # -------------------------------------------------------------- solve
-    def solveDevice(self, q):
-        """q: device float64 [npExt] charge per node -> device E [2*npExt]."""
-        L = _declare()
-        s = D.stream()
-        rc = L.oec_lu_solve(ctypes.byref(self._lu_t), q.data_ptr(), self.phi.data_ptr(), self._work.data_ptr(), s)
+    def _lu_solve(self, q):
+        rc = _declare().oec_lu_solve(ctypes.byref(self._lu_t), q.data_ptr(), self.phi.data_ptr(),
+                                     self._work.data_ptr(), D.stream())
         if rc:
             raise _lib.OecError("oec_lu_solve", rc)
+
+    def _pcg_solve(self, q):
+        """Iterative solve warm-started from the current phi; False if it missed pcgTol."""
+        pc = PRECOND[self.precond]
+        ctx = None
+        if pc == PRECOND["cnn"]:
+            if self.cnn is None:
+                raise ValueError("precond='cnn' needs a trained network in PoissonSolver.cnn")
+            ctx = self.cnn.c_handle()
+        st = PcgStats_t()
+        rc = _declare().oec_pcg_solve(ctypes.byref(self._stencil), q.data_ptr(), self.phi.data_ptr(), self.pcgTol,
+                                      self.pcgMaxIter, pc, ctx, self._pcg_work.data_ptr(), ctypes.byref(st),
+                                      D.stream())
+        if rc:
+            raise _lib.OecError("oec_pcg_solve", rc)
+        self.lastStats = st
+        return bool(st.converged)
+
+    def solveDevice(self, q, method=None):
+        """q: device float64 [npExt] charge per node -> device E [2*npExt].
+
+        method 'lu' (default of the instance: self.method) or 'pcg' (falls
+        back to LU when the f64 relative residual misses pcgTol)."""
+        L = _declare()
+        s = D.stream()
+        method = method or self.method
+        self.nSolves += 1
+        if method == "pcg":
+            if not self._pcg_solve(q):
+                self.nFallbacks += 1
+                self._lu_solve(q)
+        elif method == "lu":
+            self._lu_solve(q)
+        else:
+            raise ValueError("method must be 'lu' or 'pcg'")
         k = self._keep
         rc = L.oec_spmv_csr(2 * self.n_nodes, k["e_ptr"].data_ptr(), k["e_idx"].data_ptr(), k["e_val"].data_ptr(),
                             self.phi.data_ptr(), self.eAtGridPoints.data_ptr(), s)
