@@ -411,7 +411,8 @@ int64_t oec_pcg_work_bytes(int32_t nx, int32_t ny);
  * poissonSolver.pyx:85).  phi = A^-1 q on the inside nodes by f64 iterative
  * refinement around an f32 flexible preconditioned conjugate-gradient solve:
  * each refinement forms r = q - A phi in f64, solves A d = r in f32 to a
- * relative 2e-5 (or stagnation), and adds d in f64; it stops when
+ * relative max(1e-6, tol / (2 ||r||/||q||)) (or stagnation), and adds d in
+ * f64; it stops when
  * ||r||/||q|| <= tol or after max_iter inner iterations in total.
  * phi_dev holds the warm start on entry (zeros for none) and the solution on
  * return (0 outside).  precond: OEC_PRECOND_NONE / _JACOBI / _CNN (precond_ctx
@@ -421,6 +422,49 @@ int64_t oec_pcg_work_bytes(int32_t nx, int32_t ny);
 int oec_pcg_solve(const oec_stencil_t *st, const double *q_dev, double *phi_dev, double tol, int32_t max_iter,
                   int32_t precond, const void *precond_ctx, void *work_dev, oec_pcg_stats_t *stats,
                   void *stream);
+
+/* ------------------------------------- learned preconditioner (no counterpart
+ * in the reference): a linear 4-level U-Net (16-32-64-64 channels, 3x3
+ * convolutions, bf16 weights and activations, f32 accumulation) on the
+ * extended grid, z = inside * N(inside * x). */
+typedef struct oec_cnn {
+    int32_t nx, ny;         /* extended grid */
+    const uint8_t *inside;  /* [nx*ny] */
+    void *w16;              /* bf16 parameters, oec_cnn_num_params() of them */
+    void *act;              /* workspace of oec_cnn_act_bytes(nx, ny, training) bytes */
+} oec_cnn_t;
+
+int32_t oec_cnn_num_params(void);
+/* offsets[9]: start of each layer's weights in the flat parameter vector
+ * (7 conv layers e0 e1 e2 e3 d2 d1 d0, the 1x1 output, the total);
+ * shapes[24]: (out channels, taps, in channels) per layer.  Layer weights are
+ * [out][tap][in] with tap = 3*ty + tx. */
+int oec_cnn_param_layout(int32_t *offsets, int32_t *shapes);
+int64_t oec_cnn_act_bytes(int32_t nx, int32_t ny, int32_t training);
+/* z = N(x) (f32 [nx*ny] in and out, device). */
+int oec_cnn_forward(const oec_cnn_t *c, const float *x_dev, float *z_dev, void *stream);
+/* Warm start of the iterative solve: phi0 = |b| N(b / |b|) with
+ * b = scale32 * q on the inside nodes (the network approximates the inverse
+ * of the scaled operator); phi0 = 0 outside.  work_dev:
+ * oec_cnn_warm_start_work_bytes. */
+int64_t oec_cnn_warm_start_work_bytes(int32_t nx, int32_t ny);
+int oec_cnn_warm_start(const oec_cnn_t *c, double scale32, const double *q_dev, double *phi_dev, void *work_dev,
+                       void *stream);
+/* bf16 parameters from f32 ones. */
+int oec_cnn_set_weights(const oec_cnn_t *c, const float *w32_dev, void *stream);
+/* One training step on one input x: z = N(x); the loss is either the
+ * supervised sum(z-t)^2 / sum t^2 (op NULL, target t) or, with the scaled
+ * FIT operator op (its ex32/ey32 weights), the scale-free residual loss
+ * min_s sum(s A z - x)^2 / sum x^2 (target unused); numerator and
+ * denominator go to loss_dev[2], sums over the inside nodes.  The gradient w.r.t. the parameters goes to grad_dev
+ * (f32), and with update != 0 an Adam step (lr, beta 0.9 / 0.999,
+ * step = 1, 2, ...) updates the f32 master weights w32_dev with moments m, v
+ * and refreshes c->w16.  wt16_dev: bf16 scratch of oec_cnn_num_params()
+ * entries (flipped weights of the data gradients).  c->act must hold
+ * oec_cnn_act_bytes(nx, ny, 1) bytes. */
+int oec_cnn_train_step(const oec_cnn_t *c, const oec_stencil_t *op, const float *x_dev, const float *target_dev,
+                       float *z_dev, float *w32_dev, float *grad_dev, float *adam_m_dev, float *adam_v_dev,
+                       void *wt16_dev, float lr, int32_t step, int32_t update, double *loss_dev, void *stream);
 
 /* ------------------------------------------- grid geometry (A11-A14, host) */
 

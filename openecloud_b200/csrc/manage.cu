@@ -116,7 +116,6 @@ __global__ void k_scatter(const uint32_t *__restrict__ keys, const int32_t *__re
     // local start of each digit
     for (int t = threadIdx.x; t < 256; t += blockDim.x) dcount[t] = 0;
     __syncthreads();
-    int j = blockIdx.x * kTile + threadIdx.x;
     int local_valid = min(kTile, n - blockIdx.x * kTile);
     if ((int)threadIdx.x < local_valid) atomicAdd(&dcount[d], 1);
     __syncthreads();
@@ -133,7 +132,6 @@ __global__ void k_scatter(const uint32_t *__restrict__ keys, const int32_t *__re
         okeys[dst] = k;
         ovals[dst] = v;
     }
-    (void)j;
 }
 
 // float -> order-preserving uint32

@@ -1,5 +1,6 @@
 // pcg.cu -- iterative Poisson solve: f64 iterative refinement around an f32
-// flexible preconditioned conjugate-gradient solve on the 5-point FIT
+// flexible preconditioned conjugate-gradient solve (FCG with one stored
+// direction) on the 5-point FIT
 // operator, with the LU back-substitution (poisson.cu) as judge and fallback.
 //
 // Reference operator: PoissonSolver.__init__ (poissonSolver.pyx:41-58) builds
@@ -27,11 +28,11 @@ namespace {
 
 constexpr int kT = 256;
 constexpr int kCheck = 8;            // inner iterations between host checks
-constexpr double kInnerTol = 2e-5;   // inner relative residual (f32)
+constexpr double kInnerFloor = 1e-6;  // tightest inner relative residual asked of f32
 constexpr int kMaxRefine = 12;
 
 struct Acc {
-    double pq, rz, rr, rzn, rzo, pad0, pad1, pad2;
+    double pq, rz, rr, rzn, zq, pad0, pad1, pad2;
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -147,9 +148,10 @@ __global__ void __launch_bounds__(kT) k_apply32(int nx, int G, const float *__re
     cta_add(pq, &acc->pq);
 }
 
-// alpha = rz / pq; d += alpha p; r -= alpha q; acc.rr += |r|^2.  Without a
-// network preconditioner also z_new = M r, acc.rzn += r.z_new,
-// acc.rzo += r.z_old, z = z_new.  A non-positive or non-finite curvature
+// alpha = rz / pq (the exact line search along p: r.p = r.z because r is
+// orthogonal to the previous direction); d += alpha p; r -= alpha q;
+// acc.rr += |r|^2.  Without a network preconditioner also z = M r,
+// acc.rzn += r.z, acc.zq += z.q.  A non-positive or non-finite curvature
 // leaves every vector unchanged and marks rr as NaN for the host.
 __global__ void __launch_bounds__(kT) k_update32(int G, const float *__restrict__ dinv, int precond,
                                                  const float *__restrict__ p, const float *__restrict__ q,
@@ -161,48 +163,50 @@ __global__ void __launch_bounds__(kT) k_update32(int G, const float *__restrict_
         return;
     }
     const float alpha = (float)(rzv / pq);
-    double rr = 0.0, rzn = 0.0, rzo = 0.0;
+    double rr = 0.0, rzn = 0.0, zq = 0.0;
     for (int i = blockIdx.x * kT + threadIdx.x; i < G; i += gridDim.x * kT) {
+        const float qi = q[i];
         d[i] = fmaf(alpha, p[i], d[i]);
-        const float ri = fmaf(-alpha, q[i], r[i]);
+        const float ri = fmaf(-alpha, qi, r[i]);
         r[i] = ri;
         rr += (double)ri * (double)ri;
         if (precond != OEC_PRECOND_CNN) {
-            const float zo = z[i];
             const float zn = precond == OEC_PRECOND_JACOBI ? ri * dinv[i] : ri;
             z[i] = zn;
             rzn += (double)ri * (double)zn;
-            rzo += (double)ri * (double)zo;
+            zq += (double)zn * (double)qi;
         }
     }
     cta_add(rr, &acc->rr);
     if (precond != OEC_PRECOND_CNN) {
         cta_add(rzn, &acc->rzn);
-        cta_add(rzo, &acc->rzo);
+        cta_add(zq, &acc->zq);
     }
 }
 
-// Network preconditioner: acc.rzn += r.z_new, acc.rzo += r.z_old, z = z_new.
+// Network preconditioner: acc.rzn += r.z, acc.zq += z.q with z = M r from
+// the network (z_new), copied into z.
 __global__ void __launch_bounds__(kT) k_zdots32(int G, const float *__restrict__ r, const float *__restrict__ zn,
-                                                float *__restrict__ z, Acc *acc) {
-    double rzn = 0.0, rzo = 0.0;
+                                                const float *__restrict__ q, float *__restrict__ z, Acc *acc) {
+    double rzn = 0.0, zq = 0.0;
     for (int i = blockIdx.x * kT + threadIdx.x; i < G; i += gridDim.x * kT) {
-        const float ri = r[i], a = zn[i], b = z[i];
-        rzn += (double)ri * (double)a;
-        rzo += (double)ri * (double)b;
+        const float a = zn[i];
+        rzn += (double)r[i] * (double)a;
+        zq += (double)a * (double)q[i];
         z[i] = a;
     }
     cta_add(rzn, &acc->rzn);
-    cta_add(rzo, &acc->rzo);
+    cta_add(zq, &acc->zq);
 }
 
-// beta = (rzn - rzo) / rz (flexible, Polak-Ribiere form); p = z + beta p.
-// One thread prepares the next slot: rz = rzn, other sums zero.
+// beta = -(z.q) / (p.q): the new direction p = z + beta p is A-conjugate to
+// the previous one whatever the preconditioner (flexible CG, one stored
+// direction).  One thread prepares the next slot: rz = r.z, other sums zero.
 __global__ void __launch_bounds__(kT) k_direction32(int G, const float *__restrict__ z, float *__restrict__ p,
                                                     Acc *acc, Acc *next) {
     const double rz = acc->rz;
-    double b = (acc->rzn - acc->rzo) / rz;
-    if (!isfinite(b) || b < 0.0) b = 0.0;  // restart on loss of conjugacy
+    double b = -acc->zq / acc->pq;
+    if (!isfinite(b)) b = 0.0;
     const float beta = (float)b;
     if (isfinite(acc->rr) && isfinite(rz) && acc->pq > 0.0) {
         for (int i = blockIdx.x * kT + threadIdx.x; i < G; i += gridDim.x * kT) p[i] = fmaf(beta, p[i], z[i]);
@@ -210,7 +214,7 @@ __global__ void __launch_bounds__(kT) k_direction32(int G, const float *__restri
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         // a breakdown (rr NaN) propagates: the next update sees rz NaN
         next->rz = isfinite(acc->rr) ? acc->rzn : acc->rr;
-        next->pq = next->rr = next->rzn = next->rzo = 0.0;
+        next->pq = next->rr = next->rzn = next->zq = 0.0;
     }
 }
 
@@ -304,6 +308,9 @@ extern "C" int oec_pcg_solve(const oec_stencil_t *st, const double *q_dev, doubl
         if (refine > 0 && rel > 0.5 * prev_rel) break;  // refinement no longer pays: stagnation
         prev_rel = rel;
         const double rnorm = sqrt(h[0]);
+        // aim the f32 solve at the target when it can get there, so a good warm
+        // start needs a single refinement
+        const double inner_tol = fmax(kInnerFloor, 0.5 * tol / rel);
         // ---- inner f32 solve of (scale32 A) d = r / ||r||
         OEC_CUDA_TRY(cudaMemsetAsync(w.acc, 0, 2 * sizeof(Acc), s));
         if (precond == OEC_PRECOND_CNN) {
@@ -325,7 +332,7 @@ extern "C" int oec_pcg_solve(const oec_stencil_t *st, const double *q_dev, doubl
             if (precond == OEC_PRECOND_CNN) {
                 int rc = cnn_precond_apply(precond_ctx, w.r, w.zn, s);
                 if (rc != OEC_OK) return rc;
-                k_zdots32<<<grid, kT, 0, s>>>(G, w.r, w.zn, w.z, a);
+                k_zdots32<<<grid, kT, 0, s>>>(G, w.r, w.zn, w.q, w.z, a);
             }
             k_direction32<<<grid, kT, 0, s>>>(G, w.z, w.p, a, nxt);
             OEC_LAUNCH_CHECK();
@@ -341,7 +348,7 @@ extern "C" int oec_pcg_solve(const oec_stencil_t *st, const double *q_dev, doubl
                     break;
                 }
                 const double rel_in = sqrt(rr);
-                if (rel_in <= kInnerTol) break;
+                if (rel_in <= inner_tol) break;
                 // f32 stagnation: the best residual did not drop by 10 % in
                 // 1024 iterations (CG residual norms are not monotone)
                 if (rel_in < 0.9 * best) {

@@ -152,7 +152,8 @@ def stencil_apply_host(meps, inside_mask, nx, x):
 class PoissonSolver:
     """Reference: poissonSolver.pyx:33-67 (setup) and :83-98 (solve, getters)."""
 
-    def __init__(self, gridObj, tail=None, method="lu", precond="jacobi", pcgTol=1e-8, pcgMaxIter=4000):
+    def __init__(self, gridObj, tail=None, method="lu", precond="jacobi", pcgTol=1e-8, pcgMaxIter=4000,
+                 warmStart="previous"):
         nx = gridObj.getNxExt()
         npn = gridObj.getNpExt()
         self.gridObj = gridObj
@@ -170,7 +171,8 @@ class PoissonSolver:
         self.precond = precond
         self.pcgTol = float(pcgTol)
         self.pcgMaxIter = int(pcgMaxIter)
-        self.cnn = None          # a trained network (openecloud_b200.cnn) for precond='cnn'
+        self.cnn = None          # a trained network (openecloud_b200.cnn) for precond='cnn' / warmStart='cnn'
+        self.warmStart = warmStart  # 'previous' (last phi), 'zero' or 'cnn'
         self.lastStats = None    # PcgStats_t of the last iterative solve
         self.nSolves = 0
         self.nFallbacks = 0
@@ -287,6 +289,14 @@ class PoissonSolver:
             if self.cnn is None:
                 raise ValueError("precond='cnn' needs a trained network in PoissonSolver.cnn")
             ctx = self.cnn.c_handle()
+        if self.warmStart == "zero":
+            self.phi.zero_()
+        elif self.warmStart == "cnn":
+            if self.cnn is None:
+                raise ValueError("warmStart='cnn' needs a trained network in PoissonSolver.cnn")
+            self.cnn.warm_start(self._stencil.scale32, q, self.phi)
+        elif self.warmStart != "previous":
+            raise ValueError("warmStart must be 'previous', 'zero' or 'cnn'")
         st = PcgStats_t()
         rc = _declare().oec_pcg_solve(ctypes.byref(self._stencil), q.data_ptr(), self.phi.data_ptr(), self.pcgTol,
                                       self.pcgMaxIter, pc, ctx, self._pcg_work.data_ptr(), ctypes.byref(st),
