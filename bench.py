@@ -10,6 +10,11 @@ the survivors: the work of calcGridWeights + eFieldToParticles + borisPush
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+At one GPU the line also carries "bunch_passage": seconds per bunch passage
+of the c1 buildup (128x128 circular chamber, 2500 steps) on the device, LU
+and Jacobi-PCG Poisson solves, next to the compiled reference's passage on
+one host core (the other half of the headline metric).
+
 N > 1 runs under torchrun, one rank per GPU; every rank advances its own
 2^24 particles (independent shards, no collective on the data path:
 weak scaling).  Rank 0 prints one JSON line.
@@ -193,6 +198,47 @@ def cpu_reference_steps(n_sample, min_seconds, max_steps, min_steps=1):
                       f"single thread ({dt:.1f} s)"}
 
 
+PASSAGE = ("c1 buildup: 128x128 circular chamber R=20 mm, 1e4 initial electrons at rest, endless train "
+           "1.1e11 p/bunch, sigma_r 2 mm, sigma_t 0.25 ns, 25 ns spacing, copper SEY deltaMax 1.6 (Emax 300 eV), "
+           "roulette cap 1e5 every 50 steps, dt=1e-11 s; one bunch passage = 2500 steps")
+
+
+def cpu_reference_passage():
+    """Wall seconds of one bunch passage of the compiled reference's own loop
+    (oracle/ref_buildup.py) on one host core; None without oracle/_ref."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    try:
+        import ref_buildup
+    except Exception:
+        return None
+    if not ref_buildup.available():
+        return None
+    t = {}
+    ref_buildup.reference_buildup(100, 2500, timing=t)
+    return {"s_per_passage": t["seconds"], "cores": 1, "kind": "reference",
+            "sample": "one full passage (2500 steps) of the compiled reference's loop, seed 100"}
+
+
+def gpu_passage():
+    """Device seconds of one bunch passage of the buildup driver: LU solve with
+    graph replay (the production path), and the iterative Jacobi-PCG solve
+    (warm-started from the previous step, f64 residual 1e-8) timed over its
+    first 250 steps and scaled to 2500."""
+    from openecloud_b200.buildup import Buildup
+    Buildup(seed=999, n_steps_table=60).run(50)  # warm-up: module load, kernel attributes
+    b = Buildup(seed=1000, n_steps_table=2501)
+    s_lu = b.run(2500)
+    nfin = int(b.history()[0][-1])
+    p = Buildup(seed=1000, n_steps_table=2501)
+    p.ps.method = "pcg"
+    p.ps.precond = "jacobi"
+    s_pcg = p.run(250, use_graph=False) * 10.0
+    return {"workload": PASSAGE, "s_per_passage": s_lu, "solver": "LU (f64, level-scheduled + dense tail)",
+            "final_macro_particles": nfin, "s_per_passage_pcg_jacobi": s_pcg,
+            "pcg_jacobi_sample": "first 250 steps x 10", "pcg_fallbacks": p.ps.nFallbacks,
+            "timing": "device time (CUDA events) of the whole passage, state resident on the GPU"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -208,8 +254,11 @@ def run_reference(args, rank, world):
                                    "40x40 mm, B_y=0.5 T, weights+deposit+gather+Boris+wall test",
                        "inputs_vs_L2": "sample 200 MB > L2"},
             "impl": "reference", "cpu_baseline": {k: res[k] for k in ("kind", "cores", "sample", "value")},
-            "e2e": {"value": res["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "wall_s": time.perf_counter() - t0}
+            "e2e": {"value": res["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    cp = cpu_reference_passage()
+    if cp is not None:
+        line["bunch_passage"] = dict(workload=PASSAGE, **cp)
+    line["wall_s"] = time.perf_counter() - t0
     print(json.dumps(line), flush=True)
 
 
@@ -349,6 +398,15 @@ def run_ours(args, rank, world, local_rank):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_steps(1 << 21, min_seconds=10.0, max_steps=200, min_steps=3)
+    passage = None
+    if rank == 0 and world == 1 and not args.no_passage:
+        passage = gpu_passage()
+        _log(f"bunch passage: {passage['s_per_passage']:.3f} s (LU), "
+             f"{passage['s_per_passage_pcg_jacobi']:.2f} s (Jacobi-PCG, est.)")
+        if not args.no_cpu_baseline:
+            cp = cpu_reference_passage()
+            if cp is not None:
+                passage["cpu_reference"] = cp
 
     if rank == 0:
         line = {"metric": METRIC, "value": n * world / (ms_step * 1e-3), "unit": METRIC, "n_gpus": world,
@@ -368,6 +426,8 @@ def run_ours(args, rank, world, local_rank):
                 "status": {k: v for k, v in status.items() if v}}
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        if passage is not None:
+            line["bunch_passage"] = passage
         print(json.dumps(line), flush=True)
 
 
@@ -384,6 +444,7 @@ def main():
     ap.add_argument("--particles", type=int, default=1 << 24)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-passage", action="store_true", help="skip the buildup bunch-passage timing")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world = int(os.environ.get("WORLD_SIZE", "1"))

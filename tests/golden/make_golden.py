@@ -301,45 +301,11 @@ if __name__ == "__main__" and "--management" in sys.argv:
     management_golden()
 
 
-def reference_buildup(seed, n_steps, nx=128, lx=0.04, n_init=10000, dt=1e-11, target=100000):
-    """The reference's own loop (example01_basic.py:52-97, Python 3, no plots)
-    on the 128x128 circular chamber; returns (macro counts, sum of weights)."""
-    grid, particles, particleBoundary, poissonSolver, randomGen = _import_reference()
-    import particleEmitter
-    import particleManagement
-    from beam import LHCBeamEndless
-    randomGen.seed(seed)
-    g = grid.Grid(nx, nx, lx, lx, 1)
-    beam = LHCBeamEndless(g, dt, nParticles=1.1e11)
-    beam.bunchLengthSigma = 0.25e-9 * 299792458.0          # sigma_t = 0.25 ns
-    beam.tBunchLengthSigma = beam.bunchLengthSigma / beam.beamVelocity
-    P = particles.Particles("electrons", "variableWeight")
-    bd = particleBoundary.AbsorbElliptical(g, P)
-    em = particleEmitter.FurmanEmitter(bd, P, seyMax=1.6)
-    em.setEHat0(300.)
-    ps = poissonSolver.PoissonSolver(g)
-    particleEmitter.homoLoader(g, P, bd, n_init, 1e9 / n_init)
-    counts = np.zeros(n_steps + 1, np.int64)
-    weight = np.zeros(n_steps + 1)
-    for ii in range(n_steps):
-        weight[ii] = np.sum(np.asarray(P.getParticleData())[:, 5])
-        counts[ii] = P.getMacroParticleCount()
-        if ii > 0 and ii % 50 == 0 and (counts[ii] > 1.05 * target or counts[ii] < 0.95 * target):
-            particleManagement.globalRandom(g, P, target)
-        P.calcGridWeights(g)
-        P.chargeToGrid(g)
-        ps.solve(np.asarray(P.getChargeOnGrid()) + beam.getCharge(ii * dt))
-        P.eFieldToParticles(g, ps.getEAtGridPoints())
-        P.borisPush(dt, 0)
-        bd.indexInside()
-        bd.saveAbsorbed()
-        if bd.getAbsorbedMacroParticleCount() > 0:
-            bd.calculateInteractionPoint()
-            bd.calculateNormalVectors()
-            P.addAndRemoveParticles(em.generateSecondaries(), P.getIsInside())
-    weight[n_steps] = np.sum(np.asarray(P.getParticleData())[:, 5])
-    counts[n_steps] = P.getMacroParticleCount()
-    return counts, weight
+def reference_buildup(seed, n_steps, **kw):
+    """oracle/ref_buildup.py: the reference's own loop on the c1 chamber."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import ref_buildup
+    return ref_buildup.reference_buildup(seed, n_steps, **kw)
 
 
 def buildup_golden(n_seeds=8, n_steps=2500):
