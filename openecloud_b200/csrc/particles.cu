@@ -190,6 +190,11 @@ struct BoundaryConst {
     const double *bpts;
     const int32_t *cpi;
     float clip_lo;           // cut-cell clip, cell units (1e-6)
+    // rect: the cells [sx0, sx1] x [sy0, sy1] lie wholly inside the box with
+    // a margin far above the rounding of the f64 coordinate, so every particle
+    // in them passes the f64 test; particles in other cells (and all of the
+    // other kinds: empty range) take the f64 test.
+    int sx0, sx1, sy0, sy1;
 };
 
 // Inside predicates of particleBoundary.pyx evaluated in FP64 with explicit
@@ -504,15 +509,20 @@ __device__ __forceinline__ void process_group(const FusedArgs &a, int q, int n, 
             if (ix >= 0) cc[j] = ix + iy * a.nx;
             if (!out) {
                 const double dox = (double)nxo, doy = (double)nyo;
-                double x = abs_coord_d(ix, dox, a.dx, a.lxh);
-                double y = abs_coord_d(iy, doy, a.dy, a.lyh);
                 bool in;
-                if (KIND == OEC_BOUNDARY_RECT)
-                    in = inside_rect(a.b, x, y);
-                else if (KIND == OEC_BOUNDARY_ELLIPSE)
-                    in = inside_ellipse(a.b, x, y);
-                else
-                    in = inside_cutcell(a.b, cc[j], x, y);
+                if (KIND == OEC_BOUNDARY_RECT && (unsigned)(ix - a.b.sx0) <= (unsigned)(a.b.sx1 - a.b.sx0) &&
+                    (unsigned)(iy - a.b.sy0) <= (unsigned)(a.b.sy1 - a.b.sy0)) {
+                    in = true;  // interior cell
+                } else {
+                    const double x = abs_coord_d(ix, dox, a.dx, a.lxh);
+                    const double y = abs_coord_d(iy, doy, a.dy, a.lyh);
+                    if (KIND == OEC_BOUNDARY_RECT)
+                        in = inside_rect(a.b, x, y);
+                    else if (KIND == OEC_BOUNDARY_ELLIPSE)
+                        in = inside_ellipse(a.b, x, y);
+                    else
+                        in = inside_cutcell(a.b, cc[j], x, y);
+                }
                 out = !in;
                 // --- charge of the survivor at its new position
                 if (DEP && !out) {
@@ -796,6 +806,25 @@ static int make_boundary_const(const oec_boundary_t *bd, const GridConst &gc, Bo
     b.ex = 4.0 / (gc.lx * gc.lx);
     b.ey = 4.0 / (gc.ly * gc.ly);
     b.clip_lo = 1e-6f;
+    b.sx0 = b.sy0 = 1;
+    b.sx1 = b.sy1 = 0;
+    if (b.kind == OEC_BOUNDARY_RECT) {
+        // x = ((ix + o) dx) - lxExt/2 with o in [0, 1) is rounded twice in f64
+        // (below 1e-17 m here); the margin is 1e-12 of the box size
+        const double mx = 1e-12 * (gc.lx > gc.ly ? gc.lx : gc.ly);
+        int x0 = (int)ceil((-b.rx + mx + gc.lxh) / gc.dx), x1 = (int)floor((b.rx - mx + gc.lxh) / gc.dx) - 1;
+        int y0 = (int)ceil((-b.ry + mx + gc.lyh) / gc.dy), y1 = (int)floor((b.ry - mx + gc.lyh) / gc.dy) - 1;
+        while (x0 * gc.dx - gc.lxh < -b.rx + mx) ++x0;
+        while ((x1 + 1) * gc.dx - gc.lxh > b.rx - mx) --x1;
+        while (y0 * gc.dy - gc.lyh < -b.ry + mx) ++y0;
+        while ((y1 + 1) * gc.dy - gc.lyh > b.ry - mx) --y1;
+        if (x0 <= x1 && y0 <= y1) {
+            b.sx0 = x0;
+            b.sx1 = x1;
+            b.sy0 = y0;
+            b.sy1 = y1;
+        }
+    }
     if (b.kind == OEC_BOUNDARY_CUTCELL) {
         if (!bd->inside_faces_dev || !bd->boundary_points_dev || !bd->cut_cell_points_ind_dev)
             return OEC_ERR_INVALID;
