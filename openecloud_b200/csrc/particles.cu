@@ -572,19 +572,26 @@ __device__ __forceinline__ void publish_tally(const FusedArgs &a, const Tally &t
 
 constexpr int fused_min_blocks(int tb, int kind) { return (tb == 2 || kind == OEC_BOUNDARY_CUTCELL) ? 3 : 4; }
 
-// Persistent loop over chunks of kChunk particles; with the deposit, two
-// barriers per chunk bracket the use of the CTA's node window.
+// Persistent loop over chunks of kChunk particles.  With the deposit the CTA
+// has two node windows used by alternate chunks, and one barrier per chunk:
+// the barrier at the start of chunk k publishes its anchor and ends every add
+// of chunk k-1, whose window is then flushed while chunk k adds into the
+// other one (that window's last flush, of chunk k-2, ended at the same
+// barrier).  A last barrier after the loop ends the final chunk's adds.
 template <int TB, int KIND, bool DEP>
 __global__ void __launch_bounds__(kThreads, fused_min_blocks(TB, KIND)) k_push_gather(FusedArgs a) {
-    __shared__ __align__(16) unsigned win[DEP ? kWinWords : 4];
-    __shared__ int first_cell;
+    __shared__ __align__(16) unsigned win[DEP ? 2 * kWinWords : 4];
+    __shared__ int first_cell[2];
     const int n = min(*a.count, (int)a.capacity);
     const int nchunks = (n + kChunk - 1) / kChunk;
     const double wscale = DEP ? *a.wscale : 0.0;
     Tally t;
     NodeWindow nw{win, 0, 0, false};
+    NodeWindow prev{win, 0, 0, false};  // the previous chunk's window and anchor
+    bool have_prev = false;
+    int parity = 0;
     if (DEP)
-        for (int e = threadIdx.x; e < kWinWords; e += kThreads) win[e] = 0u;
+        for (int e = threadIdx.x; e < 2 * kWinWords; e += kThreads) win[e] = 0u;
     for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
         const int q = chunk * kThreads + threadIdx.x;  // float4 group index
         int4 c4 = reinterpret_cast<const int4 *>(a.cell)[q];
@@ -596,17 +603,25 @@ __global__ void __launch_bounds__(kThreads, fused_min_blocks(TB, KIND)) k_push_g
         float4 w4 = make_float4(0.f, 0.f, 0.f, 0.f);
         if (DEP) {
             w4 = reinterpret_cast<const float4 *>(a.w)[q];
-            if (threadIdx.x == 0) first_cell = c4.x;
-            __syncthreads();  // anchor published; the previous chunk's flush is done
-            window_anchor(nw, first_cell, a.ncell, a.nx, a.nx_magic);
+            if (threadIdx.x == 0) first_cell[parity] = c4.x;
+            const bool any_hi = __syncthreads_or(nw.hi_used);
+            nw.hi_used = false;
+            if (have_prev) window_flush(prev, any_hi, a.rho, a.nx);
+            nw.v = win + parity * kWinWords;
+            window_anchor(nw, first_cell[parity], a.ncell, a.nx, a.nx_magic);
         }
         process_group<TB, KIND, DEP>(a, q, n, wscale, c4, fx4, fy4, vx4, vy4, vz4, w4, t, nw);
         if (DEP) {
-            // every add of this chunk is in the window
-            const bool any_hi = __syncthreads_or(nw.hi_used);
-            nw.hi_used = false;
-            window_flush(nw, any_hi, a.rho, a.nx);
+            prev.v = nw.v;
+            prev.ox = nw.ox;
+            prev.oy = nw.oy;
+            have_prev = true;
+            parity ^= 1;
         }
+    }
+    if (DEP) {
+        const bool any_hi = __syncthreads_or(nw.hi_used);
+        if (have_prev) window_flush(prev, any_hi, a.rho, a.nx);
     }
     publish_tally<KIND>(a, t);
 }
