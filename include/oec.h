@@ -278,7 +278,8 @@ int oec_rhs_with_beam(const oec_grid_t *grid, const int64_t *rho_fix_dev, const 
                       double particle_charge, const double *profile_dev, const double *table_dev,
                       const int32_t *step_dev, int32_t table_len, double *rho_dev, void *stream);
 
-/* hist_w[*step] = sum w, hist_n[*step] = count (example01_basic.py:56-57). */
+/* hist_w[*step] = sum w, hist_n[*step] = count (example01_basic.py:56-57).
+ * scratch_dev: 256 doubles. */
 int oec_history(const oec_particles_t *p, int32_t *step_dev, int32_t hist_len, double *hist_w_dev,
                 int32_t *hist_n_dev, double *scratch_dev, void *stream);
 

@@ -96,7 +96,7 @@ class Buildup:
         self.btab = None
         self.hist_w = D.zeros(self._table_len, torch.float64)
         self.hist_n = D.zeros(self._table_len, torch.int32)
-        self.scratch = D.zeros(4, torch.float64)
+        self.scratch = D.zeros(256, torch.float64)  # oec_history's partial sums
         # absorbed rows per step: bounded by a fraction of the capacity
         self.abs_cap = max(4096, cap // 8)
         self.bd.ensure_buffers(self.abs_cap)

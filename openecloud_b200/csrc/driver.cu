@@ -23,26 +23,35 @@ __global__ void k_rhs(const long long *__restrict__ fix, int G, const double *ws
 }
 
 // history[step] = (count, sum w); then ++step
-__global__ void k_history(const int32_t *count, const float *__restrict__ w, int32_t *step, int hist_len,
-                          double *__restrict__ hist_w, int32_t *__restrict__ hist_n, double *scratch) {
-    // single CTA reduction (the per-step history is a diagnostic)
+// Per-CTA partial sums of w (first level of the history reduction).
+constexpr int kHistCtas = 256;
+
+__global__ void k_history_partial(const int32_t *count, const float *__restrict__ w, double *__restrict__ partial) {
     __shared__ double red[32];
-    int n = *count;
+    const int n = *count;
     double s = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) s += (double)w[i];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += (double)w[i];
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFullMask, s, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
     __syncthreads();
     if (threadIdx.x < 32) {
         s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFullMask, s, o);
-        if (threadIdx.x == 0) {
-            int k = *step;
-            if (k >= 0 && k < hist_len) {
-                hist_w[k] = s;
-                hist_n[k] = n;
-            }
-            *scratch = s;
+        if (threadIdx.x == 0) partial[blockIdx.x] = s;
+    }
+}
+
+// Second level: one warp sums the partials in a fixed order (deterministic).
+__global__ void k_history(const int32_t *count, const double *__restrict__ partial, int nparts, int32_t *step,
+                          int hist_len, double *__restrict__ hist_w, int32_t *__restrict__ hist_n) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < nparts; i += 32) s += partial[i];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFullMask, s, o);
+    if (threadIdx.x == 0) {
+        const int k = *step;
+        if (k >= 0 && k < hist_len) {
+            hist_w[k] = s;
+            hist_n[k] = *count;
         }
     }
 }
@@ -69,8 +78,10 @@ extern "C" int oec_rhs_with_beam(const oec_grid_t *grid, const int64_t *rho_fix_
 extern "C" int oec_history(const oec_particles_t *p, int32_t *step_dev, int32_t hist_len, double *hist_w_dev,
                            int32_t *hist_n_dev, double *scratch_dev, void *stream) {
     if (!p || !step_dev || !hist_w_dev || !hist_n_dev || !scratch_dev) return OEC_ERR_INVALID;
-    k_history<<<1, 1024, 0, as_stream(stream)>>>(p->count, p->w, step_dev, hist_len, hist_w_dev, hist_n_dev,
-                                                  scratch_dev);
+    const int g = persistent_grid((p->capacity + 255) / 256, 2) < kHistCtas ? persistent_grid((p->capacity + 255) / 256, 2)
+                                                                            : kHistCtas;
+    k_history_partial<<<g, 256, 0, as_stream(stream)>>>(p->count, p->w, scratch_dev);
+    k_history<<<1, 32, 0, as_stream(stream)>>>(p->count, scratch_dev, g, step_dev, hist_len, hist_w_dev, hist_n_dev);
     OEC_LAUNCH_CHECK();
     return OEC_OK;
 }

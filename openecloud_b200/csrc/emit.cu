@@ -41,6 +41,9 @@ __global__ void k_furman_pass1(oec_furman_t f, const double *__restrict__ rows, 
     int na = min(*n_abs, cap);
     const double eFactor = 0.5 * f.particle_mass / 1.602176565e-19;
     int wd = 0, wt = 0;
+    double lfac[11];  // lgamma(j + 1), j <= m <= 10, by the threads that have work
+    if ((int)(blockIdx.x * blockDim.x + threadIdx.x) < na)
+        for (int j = 0; j <= f.m; ++j) lfac[j] = sf::lgam((double)j + 1.0);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += gridDim.x * blockDim.x) {
         const double *r = rows + 6 * (int64_t)i;
         const double n0 = normals[2 * i], n1 = normals[2 * i + 1];
@@ -76,11 +79,21 @@ __global__ void k_furman_pass1(oec_furman_t f, const double *__restrict__ rows, 
         double u = dr.next();
         // P_n = binom(n; m, pr) (1 - dE - dR), P_1 += dE + dR (:217-221);
         // inverse-CDF draw over n < m, default m (:222-229)
-        const double pN1 = sf::binom_pdf(1u, pr, (unsigned)f.m) * keep + (dE + dR);
+        // binom_pdf(k; m, pr) with lgamma(j+1) and the logs of pr evaluated once
+        // (the same values as sf::binom_pdf)
+        const double lp = log(pr), l1p = log1p(-pr);
+        auto pdf = [&](unsigned k) -> double {
+            const unsigned m = (unsigned)f.m;
+            if (pr == 0.0) return k == 0 ? 1.0 : 0.0;
+            if (pr == 1.0) return k == m ? 1.0 : 0.0;
+            const double lc = lfac[m] - lfac[k] - lfac[m - k];
+            return exp(lc + k * lp + (double)(m - k) * l1p);
+        };
+        const double pN1 = pdf(1u) * keep + (dE + dR);
         int n = f.m;
         double cum = 0.0;
         for (int k = 0; k < f.m; ++k) {
-            cum += (k == 1) ? pN1 : sf::binom_pdf((unsigned)k, pr, (unsigned)f.m) * keep;
+            cum += (k == 1) ? pN1 : pdf((unsigned)k) * keep;
             if (u <= cum) {
                 n = k;
                 break;
@@ -93,10 +106,44 @@ __global__ void k_furman_pass1(oec_furman_t f, const double *__restrict__ rows, 
     if (wt) atomicAdd(&status->warn_tsprime, wt);
 }
 
+// Pass 2a: the costly inverses of the joint energy split of a multi-secondary
+// emission (particleEmitter.pyx:255-266), one thread per (absorbed particle,
+// slot).  For n secondaries slot k < n-1 holds theta_k =
+// asin(sqrt(I^-1_u(P(n-k-1), P))) from draw 1+k and slot n-1 holds
+// y = sqrt(P^-1(nP, u p0)) from draw n: the same draws and the same
+// arithmetic as one thread doing them in sequence, but the n calls run side
+// by side instead of one after the other.
+constexpr int kSlots = 10;
+
+__global__ void k_furman_pass2a(oec_furman_t f, const int32_t *n_abs, int cap, const int32_t *__restrict__ ids,
+                                uint2 key, uint32_t step, const int32_t *step_dev, const double *__restrict__ replay,
+                                const Rec *__restrict__ rec, double *__restrict__ split) {
+    const int na = min(*n_abs, cap);
+    const int total = na * kSlots;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const int i = t / kSlots, k = t % kSlots;
+        const Rec R = rec[i];
+        const int n = R.nsec;
+        if (n < 2 || k >= n) continue;
+        const double P = f.pSmallN[n - 1], eps = f.epsN[n - 1];
+        sf::Draws dr{key, ids ? (uint32_t)ids[i] : (uint32_t)i, step + (step_dev ? (uint32_t)*step_dev : 0u),
+                     replay ? replay + (int64_t)i * kDraws : nullptr};
+        dr.d = 1 + k;
+        double v;
+        if (k < n - 1) {
+            v = asin(sqrt(sf::betaincinv(P * (n - k - 1), P, dr.next())));
+        } else {
+            const double p0 = sf::gammainc(n * P, R.e0 / eps);
+            v = sqrt(sf::gammaincinv(n * P, dr.next() * p0));
+        }
+        split[(int64_t)i * kSlots + k] = v;
+    }
+}
+
 __global__ void k_furman_pass2(oec_furman_t f, const double *__restrict__ rows, const double *__restrict__ normals,
                                const int32_t *n_abs, int cap, const int32_t *__restrict__ ids, uint2 key,
                                uint32_t step, const int32_t *step_dev, const double *__restrict__ replay,
-                               const Rec *__restrict__ rec,
+                               const Rec *__restrict__ rec, const double *__restrict__ split,
                                const int32_t *__restrict__ offset, double *__restrict__ out, int out_cap,
                                oec_status_t *status) {
     int na = min(*n_abs, cap);
@@ -131,11 +178,13 @@ __global__ void k_furman_pass2(oec_furman_t f, const double *__restrict__ rows, 
                 eSec[0] = f.epsN[0] * sf::gammaincinv(f.pSmallN[0], dr.next() * sf::gammainc(f.pSmallN[0], e0 / f.epsN[0]));
             }
         } else {
-            const double P = f.pSmallN[n - 1], eps = f.epsN[n - 1];
-            double p0 = sf::gammainc(n * P, e0 / eps);
+            // theta_k and y from pass 2a (draws 1 .. n)
+            const double *sp = split + (int64_t)i * kSlots;
+            const double eps = f.epsN[n - 1];
             double th[10];
-            for (int k = 0; k < n - 1; ++k) th[k] = asin(sqrt(sf::betaincinv(P * (n - k - 1), P, dr.next())));
-            double y = sqrt(sf::gammaincinv(n * P, dr.next() * p0));
+            for (int k = 0; k < n - 1; ++k) th[k] = sp[k];
+            const double y = sp[n - 1];
+            dr.d = n + 1;
             double yk[10];
             yk[0] = y * cos(th[0]);
             yk[n - 1] = y;
@@ -291,10 +340,11 @@ extern "C" int oec_furman_emit(const oec_furman_t *params, const double *rows_de
     int nblocks = (cap + kScanT - 1) / kScanT;
     if (nblocks > kScanT) return OEC_ERR_INVALID;
     cudaStream_t s = as_stream(stream);
-    // work layout: Rec[cap] | nsec[cap] | offset[cap] | partial[1024]
+    // work layout: Rec[cap] | split[cap * kSlots] (f64) | nsec[cap] | offset[cap] | partial[1024]
     char *w = static_cast<char *>(work_dev);
     Rec *rec = reinterpret_cast<Rec *>(w);
-    int32_t *nsec = reinterpret_cast<int32_t *>(w + sizeof(Rec) * (size_t)cap);
+    double *split = reinterpret_cast<double *>(w + sizeof(Rec) * (size_t)cap);
+    int32_t *nsec = reinterpret_cast<int32_t *>(split + (size_t)cap * kSlots);
     int32_t *off = nsec + cap;
     int *partial = off + cap;
     uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
@@ -308,14 +358,17 @@ extern "C" int oec_furman_emit(const oec_furman_t *params, const double *rows_de
     } else {
         OEC_CUDA_TRY(cudaMemsetAsync(n_out_dev, 0, sizeof(int32_t), s));
     }
+    k_furman_pass2a<<<persistent_grid(((int64_t)cap * kSlots + 127) / 128, 8), 128, 0, s>>>(
+        *params, n_abs_dev, cap, ids_dev, key, step, step_dev, replay_uniforms_dev, rec, split);
     k_furman_pass2<<<g, 128, 0, s>>>(*params, rows_dev, normals_dev, n_abs_dev, cap, ids_dev, key, step, step_dev,
-                                     replay_uniforms_dev, rec, off, out_rows_dev, out_cap, status_dev);
+                                     replay_uniforms_dev, rec, split, off, out_rows_dev, out_cap, status_dev);
     OEC_LAUNCH_CHECK();
     return OEC_OK;
 }
 
 extern "C" int64_t oec_furman_work_bytes(int32_t cap) {
-    return (int64_t)sizeof(Rec) * cap + 2 * sizeof(int32_t) * (int64_t)cap + sizeof(int) * 1024 + 256;
+    return (int64_t)sizeof(Rec) * cap + (int64_t)sizeof(double) * kSlots * cap + 2 * sizeof(int32_t) * (int64_t)cap +
+           sizeof(int) * 1024 + 256;
 }
 
 extern "C" int oec_homo_load(const oec_grid_t *grid, const oec_boundary_t *boundary, oec_particles_t *p, int64_t n,

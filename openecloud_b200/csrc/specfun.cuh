@@ -27,11 +27,12 @@ constexpr double kCfEps = 1e-16;
 
 __device__ inline double lgam(double a) { return lgamma(a); }
 
-// Regularised lower incomplete gamma P(a, x), a > 0.
-__device__ inline double gammainc(double a, double x) {
+// Regularised lower incomplete gamma P(a, x), a > 0, with lga = lgamma(a)
+// given (an inverse evaluates it many times for one a).
+__device__ inline double gammainc_lg(double a, double x, double lga) {
     if (!(x > 0.0)) return 0.0;
     if (isinf(x)) return 1.0;
-    double lpref = -x + a * log(x) - lgam(a);
+    double lpref = -x + a * log(x) - lga;
     if (x < a + 1.0) {
         double term = 1.0 / a, sum = term, an = a;
         for (int n = 0; n < 100000; ++n) {
@@ -43,59 +44,90 @@ __device__ inline double gammainc(double a, double x) {
         double p = sum * exp(lpref);
         return p > 1.0 ? 1.0 : p;
     }
-    double b = x + 1.0 - a, c = 1.0 / kTiny, d = 1.0 / b, f = d;
+    // continued fraction f = 1/(b0 + a1/(b1 + a2/(b2 + ...))), b_i = x+1-a+2i,
+    // a_i = -i(i-a), by the forward recurrence of its convergents (one fused
+    // multiply-add per term on the dependency chain; a division only at the
+    // convergence checks, every 4 terms, which also renormalise A and B)
+    const double b0 = x + 1.0 - a;
+    double A2 = 0.0, B2 = 1.0, A1 = 1.0, B1 = b0;  // convergents n-2, n-1
+    double f = A1 / B1;
     for (int i = 1; i < 100000; ++i) {
-        double an = -i * (i - a);
-        b += 2.0;
-        d = an * d + b;
-        if (fabs(d) < kTiny) d = kTiny;
-        c = b + an / c;
-        if (fabs(c) < kTiny) c = kTiny;
-        d = 1.0 / d;
-        double del = d * c;
-        f *= del;
-        if (fabs(del - 1.0) <= kCfEps) break;
+        const double an = -i * (i - a), bn = b0 + 2.0 * i;
+        const double A = bn * A1 + an * A2, B = bn * B1 + an * B2;
+        A2 = A1;
+        B2 = B1;
+        A1 = A;
+        B1 = B;
+        if ((i & 3) == 0) {
+            const double r = 1.0 / B1, fn = A1 * r;
+            A1 *= r;
+            A2 *= r;
+            B2 *= r;
+            B1 = 1.0;
+            const bool done = fabs(fn - f) <= 4.0 * kCfEps * fabs(fn);
+            f = fn;
+            if (done) break;
+        }
     }
     double p = 1.0 - exp(lpref) * f;
     return p < 0.0 ? 0.0 : p;
 }
 
+// Regularised lower incomplete gamma P(a, x), a > 0.
+__device__ inline double gammainc(double a, double x) { return gammainc_lg(a, x, lgam(a)); }
+
+// Continued fraction of I_x(a, b): 1/(1 + d1/(1 + d2/(1 + ...))) with
+// d1 = -(a+b)x/(a+1), d_{2m} = m(b-m)x/((a+2m-1)(a+2m)),
+// d_{2m+1} = -(a+m)(a+b+m)x/((a+2m)(a+2m+1)), by the forward recurrence of
+// its convergents (one fused multiply-add per term on the dependency chain;
+// a division only at the convergence checks, which also renormalise).
 __device__ inline double beta_cf(double a, double b, double x) {
-    double qab = a + b, qap = a + 1.0, qam = a - 1.0;
-    double c = 1.0, d = 1.0 - qab * x / qap;
-    if (fabs(d) < kTiny) d = kTiny;
-    d = 1.0 / d;
-    double h = d;
+    const double qab = a + b, qap = a + 1.0, qam = a - 1.0;
+    double A2 = 1.0, B2 = 1.0, A1 = 1.0, B1 = 1.0 - qab * x / qap;  // convergents 1 and 2
+    double h = A1 / B1;
     for (int m = 1; m < 100000; ++m) {
-        int m2 = 2 * m;
-        double aa = m * (b - m) * x / ((qam + m2) * (a + m2));
-        d = 1.0 + aa * d;
-        if (fabs(d) < kTiny) d = kTiny;
-        c = 1.0 + aa / c;
-        if (fabs(c) < kTiny) c = kTiny;
-        d = 1.0 / d;
-        h *= d * c;
-        aa = -(a + m) * (qab + m) * x / ((a + m2) * (qap + m2));
-        d = 1.0 + aa * d;
-        if (fabs(d) < kTiny) d = kTiny;
-        c = 1.0 + aa / c;
-        if (fabs(c) < kTiny) c = kTiny;
-        d = 1.0 / d;
-        double del = d * c;
-        h *= del;
-        if (fabs(del - 1.0) <= kCfEps) break;
+        const int m2 = 2 * m;
+        const double de = m * (b - m) * x / ((qam + m2) * (a + m2));
+        const double dodd = -(a + m) * (qab + m) * x / ((a + m2) * (qap + m2));
+        double A = A1 + de * A2, B = B1 + de * B2;
+        A2 = A1;
+        B2 = B1;
+        A1 = A;
+        B1 = B;
+        A = A1 + dodd * A2;
+        B = B1 + dodd * B2;
+        A2 = A1;
+        B2 = B1;
+        A1 = A;
+        B1 = B;
+        if ((m & 1) == 0) {
+            const double r = 1.0 / B1, hn = A1 * r;
+            A1 *= r;
+            A2 *= r;
+            B2 *= r;
+            B1 = 1.0;
+            const bool done = fabs(hn - h) <= 4.0 * kCfEps * fabs(hn);
+            h = hn;
+            if (done) break;
+        }
     }
     return h;
 }
 
-// Regularised incomplete beta I_x(a, b).
-__device__ inline double betainc(double a, double b, double x) {
+// Regularised incomplete beta I_x(a, b) with lb = lgamma(a+b) - lgamma(a) -
+// lgamma(b) given (the same value, computed once per inverse).
+__device__ inline double betainc_lb(double a, double b, double x, double lb) {
     if (x <= 0.0) return 0.0;
     if (x >= 1.0) return 1.0;
-    double bt = exp(lgam(a + b) - lgam(a) - lgam(b) + a * log(x) + b * log1p(-x));
+    double bt = exp(lb + a * log(x) + b * log1p(-x));
     if (x < (a + 1.0) / (a + b + 2.0)) return bt * beta_cf(a, b, x) / a;
     return 1.0 - bt * beta_cf(b, a, 1.0 - x) / b;
 }
+
+__device__ inline double lbeta_inv(double a, double b) { return lgam(a + b) - lgam(a) - lgam(b); }
+
+// Regularised incomplete beta I_x(a, b).
+__device__ inline double betainc(double a, double b, double x) { return betainc_lb(a, b, x, lbeta_inv(a, b)); }
 
 __device__ inline double beta(double a, double b) { return exp(lgam(a) + lgam(b) - lgam(a + b)); }
 
@@ -160,7 +192,7 @@ __device__ inline double gammaincinv(double a, double p, double acc = 1.e-9) {
     int j;
     for (j = 0; j < 20; ++j) {
         if (x <= 0.0) return 0.0;
-        double err = gammainc(a, x) - p;
+        double err = gammainc_lg(a, x, gln) - p;
         if (a > 1.0)
             t = afac * exp(-(x - a1) + a1 * (log(x) - lna1));
         else
@@ -177,16 +209,16 @@ __device__ inline double gammaincinv(double a, double p, double acc = 1.e-9) {
     if (j == 20) j = 19;  // the reference's loop variable ends at 19 when no break
     if (j == 19 && x < a) {
         eps = eps * eps;
-        double err = gammainc(a, x) - p;
+        double err = gammainc_lg(a, x, gln) - p;
         double xr = x;
         for (int guard = 0; err <= 0 && guard < 2000; ++guard) {
             xr *= 2.0;
-            err = gammainc(a, xr) - p;
+            err = gammainc_lg(a, xr, gln) - p;
         }
         double xl = 0.0;
         x = 0.5 * (xr + xl);
         for (int k = 0; k < 100; ++k) {
-            err = gammainc(a, x) - p;
+            err = gammainc_lg(a, x, gln) - p;
             if (err <= 0.0)
                 xl = x;
             else
@@ -381,11 +413,12 @@ __device__ inline double betaincinv(double a, double b, double p, double acc = 1
     // Halley refinement on I_x(a,b) - p.
     const double bfi = 1. / beta(a, b);
     const double a1 = a - 1., a2 = a1 - 1., b1 = b - 1., b2 = b1 - 1.;
+    const double lb = lbeta_inv(a, b);
     for (unsigned j = 0; j < n_halley; ++j) {
         // as in the reference, these early exits ignore the a<->b swap
         if (x <= 0.0) return 0.0;
         if (x >= 1.) return 1.0;
-        double err = betainc(a, b, x) - p;
+        double err = betainc_lb(a, b, x, lb) - p;
         double y = 1. - x;
         double xa1 = pow(x, a1), xa2 = pow(x, a2), yb1 = pow(y, b1), yb2 = pow(y, b2);
         double der1 = xa1 * yb1 * bfi;
