@@ -11,9 +11,13 @@ the survivors: the work of calcGridWeights + eFieldToParticles + borisPush
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 At one GPU the line also carries "bunch_passage": seconds per bunch passage
-of the c1 buildup (128x128 circular chamber, 2500 steps) on the device, LU
-and Jacobi-PCG Poisson solves, next to the compiled reference's passage on
-one host core (the other half of the headline metric).
+of the c1 buildup (128x128 circular chamber, 2500 steps) on the device with
+the LU, multigrid-PCG and Jacobi-PCG Poisson solves, next to the compiled
+reference's passage on one host core (the other half of the headline
+metric); and "production_passage": the 1024x1024 elliptical production
+buildup sampled over 100 steps with the LU and multigrid-PCG solves, with
+the single-solve comparison on that grid (LU against the iterative solve at
+relative residual 1e-8).
 
 N > 1 runs under torchrun, one rank per GPU; every rank advances its own
 2^24 particles (independent shards, no collective on the data path:
@@ -220,23 +224,134 @@ def cpu_reference_passage():
 
 
 def gpu_passage():
-    """Device seconds of one bunch passage of the buildup driver: LU solve with
-    graph replay (the production path), and the iterative Jacobi-PCG solve
-    (warm-started from the previous step, f64 residual 1e-8) timed over its
-    first 250 steps and scaled to 2500."""
+    """Device seconds of one bunch passage of the buildup driver with each
+    Poisson solve, every time step replayed from one captured graph: LU
+    (f64, level-scheduled + dense tail), the multigrid-preconditioned
+    iterative solve (f64 residual 1e-8, its loops inside the step graph, LU
+    fallback on the device) over the whole passage, and the Jacobi-
+    preconditioned one over its first 250 steps, scaled to 2500."""
     from openecloud_b200.buildup import Buildup
     Buildup(seed=999, n_steps_table=60).run(50)  # warm-up: module load, kernel attributes
     b = Buildup(seed=1000, n_steps_table=2501)
     s_lu = b.run(2500)
     nfin = int(b.history()[0][-1])
-    p = Buildup(seed=1000, n_steps_table=2501)
-    p.ps.method = "pcg"
-    p.ps.precond = "jacobi"
-    s_pcg = p.run(250, use_graph=False) * 10.0
-    return {"workload": PASSAGE, "s_per_passage": s_lu, "solver": "LU (f64, level-scheduled + dense tail)",
-            "final_macro_particles": nfin, "s_per_passage_pcg_jacobi": s_pcg,
-            "pcg_jacobi_sample": "first 250 steps x 10", "pcg_fallbacks": p.ps.nFallbacks,
-            "timing": "device time (CUDA events) of the whole passage, state resident on the GPU"}
+    out = {"workload": PASSAGE, "s_per_passage": s_lu, "solver": "LU (f64, level-scheduled + dense tail)",
+           "final_macro_particles": nfin}
+    m = Buildup(seed=1000, n_steps_table=2501)
+    m.ps.method, m.ps.precond = "pcg", "mg"
+    out["s_per_passage_pcg_mg"] = m.run(2500)
+    out["pcg_mg_fallbacks"] = m.ps.nFallbacks
+    out["pcg_mg_final_macro_particles"] = int(m.history()[0][-1])
+    j = Buildup(seed=1000, n_steps_table=2501)
+    j.ps.method, j.ps.precond = "pcg", "jacobi"
+    out["s_per_passage_pcg_jacobi"] = j.run(250) * 10.0
+    out["pcg_jacobi_sample"] = "first 250 steps x 10"
+    out["pcg_jacobi_fallbacks"] = j.ps.nFallbacks
+    out["timing"] = "device time (CUDA events) of the whole passage, state resident on the GPU, step graphs replayed"
+    return out
+
+
+PRODUCTION = ("production buildup (sampled): 1024x1024 grid over an elliptical chamber with half-axes 45x18 mm, "
+              "dipole B_y=8.33 T, 25 ns train of 1.15e11 p/bunch (sigma_r 1 mm, sigma_t 0.25 ns), SEY deltaMax 1.8, "
+              "2e6 initial macro-electrons, kd-tree merge (localRandom) toward 2e6 every 10 steps, dt=5e-12 s; "
+              "one bunch passage = 5000 steps")
+
+
+def _smooth_charge(grid, seed=11, n=16):
+    """Charge per node from a sum of Gaussians (sigma 1-4 mm) inside the chamber."""
+    rng = np.random.default_rng(seed)
+    nx, ny = grid.getNxExt(), grid.getNyExt()
+    x = (np.arange(nx) - (nx - 1) / 2) * grid.getDx()
+    y = (np.arange(ny) - (ny - 1) / 2) * grid.getDy()
+    X, Y = np.meshgrid(x, y)
+    rho = np.zeros_like(X)
+    for _ in range(n):
+        cx, cy = rng.uniform(-0.5, 0.5, 2) * np.array([x[-1], y[-1]])
+        s = rng.uniform(1e-3, 4e-3)
+        rho += rng.uniform(0.5, 1.5) * np.exp(-((X - cx) ** 2 + (Y - cy) ** 2) / (2 * s * s))
+    ins = np.asarray(grid.getInsidePoints()).reshape(ny, nx) != 0
+    return (np.where(ins, rho, 0.0) * 1e-12).ravel()
+
+
+def poisson_comparison(ps, reps=10):
+    """Solve times on one grid: LU against the iterative solve (f64 residual
+    1e-8) with the multigrid preconditioner (cold: zero start; warm: from
+    the solution of a 0.1 % different charge, as between time steps) and
+    with the Jacobi one (cold)."""
+    import torch
+    from openecloud_b200 import device as D
+    q = _smooth_charge(ps.gridObj)
+    qd = D.to_device(q, torch.float64)
+    q2 = D.to_device(q * (1.0 + 1e-3 * np.sin(np.linspace(0, 2 * np.pi, q.size))), torch.float64)
+    s = torch.cuda.current_stream()
+
+    def timed(fn, n):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(n):
+            fn()
+        e1.record(s)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    out = {}
+    ps.method = "lu"
+    out["lu_ms"] = timed(lambda: ps.solveDevice(qd), reps)
+    phi_lu = D.to_numpy(ps.phi)
+    fb0 = ps.nFallbacks
+    ps.method, ps.precond, ps.warmStart = "pcg", "mg", "zero"
+    out["mg_cold_ms"] = timed(lambda: ps.solveDevice(qd), reps)
+    st = ps.lastStats
+    out["mg_cold_iterations"], out["mg_cold_refinements"] = st.iterations, st.refinements
+    out["mg_vs_lu_max_rel"] = float(np.abs(D.to_numpy(ps.phi) - phi_lu).max() / np.abs(phi_lu).max())
+    ps.warmStart = "previous"
+
+    def warm():
+        ps.solveDevice(qd)
+        ps.solveDevice(q2)
+    out["mg_warm_ms"] = timed(warm, reps) / 2.0
+    st = ps.lastStats
+    out["mg_warm_iterations"], out["mg_warm_rel_residual0"] = st.iterations, st.rel_residual0
+    ps.precond, ps.warmStart = "jacobi", "zero"
+    out["jacobi_cold_ms"] = timed(lambda: ps.solveDevice(qd), 2)
+    out["jacobi_cold_iterations"] = ps.lastStats.iterations
+    out["fallbacks"] = ps.nFallbacks - fb0
+    ps.method, ps.precond, ps.warmStart = "lu", "jacobi", "previous"
+    out["tol"] = 1e-8
+    out["timing"] = "device time (CUDA events) per solve, charge resident on the GPU"
+    return out
+
+
+def production_passage(steps=100):
+    """Config-3 buildup sampled over its first `steps` steps with the LU and
+    the multigrid-preconditioned iterative Poisson solve (one factorisation
+    shared), scaled to a 5000-step passage; plus the config-5 solve
+    comparison on the same 1024x1024 elliptical grid."""
+    from openecloud_b200.buildup import Buildup
+    kw = dict(nx=1024, ny=1024, lx=0.09, ly=0.036, boundType=1, n_init=2_000_000, w_init=1e3, dt=5e-12,
+              beam_particles=1.15e11, radius_sigma=1e-3, sey_max=1.8, type_b_field=1, b_const=(0., 8.33, 0.),
+              target=2_000_000, management="local", management_every=10, n_steps_table=steps + 1, seed=2000)
+    t0 = time.perf_counter()
+    lu = Buildup(**kw)
+    setup = time.perf_counter() - t0
+    out = {"workload": PRODUCTION, "steps_timed": steps, "setup_s": setup}
+    out["poisson_solve"] = dict(workload="1024x1024 elliptical cut-cell grid 45x18 mm (the production grid), charge "
+                                         "from 16 Gaussians (sigma 1-4 mm)", **poisson_comparison(lu.ps))
+    t_lu = lu.run(steps)
+    out["s_per_passage_lu"] = t_lu / steps * 5000
+    out["final_macro_particles_lu"] = int(lu.history()[0][-1])
+    m = Buildup(poisson=lu.ps, **kw)
+    m.ps.method, m.ps.precond = "pcg", "mg"
+    fb0 = m.ps.nFallbacks
+    t_mg = m.run(steps)
+    out["s_per_passage_pcg_mg"] = t_mg / steps * 5000
+    out["pcg_mg_fallbacks"] = m.ps.nFallbacks - fb0
+    out["final_macro_particles_pcg_mg"] = int(m.history()[0][-1])
+    out["timing"] = (f"device time (CUDA events) of the first {steps} steps (management and graph captures "
+                     "included) x 5000/steps")
+    return out
 
 
 def run_reference(args, rank, world):
@@ -401,12 +516,19 @@ def run_ours(args, rank, world, local_rank):
     passage = None
     if rank == 0 and world == 1 and not args.no_passage:
         passage = gpu_passage()
-        _log(f"bunch passage: {passage['s_per_passage']:.3f} s (LU), "
-             f"{passage['s_per_passage_pcg_jacobi']:.2f} s (Jacobi-PCG, est.)")
+        _log(f"bunch passage: {passage['s_per_passage']:.3f} s (LU), {passage['s_per_passage_pcg_mg']:.3f} s "
+             f"(MG-PCG), {passage['s_per_passage_pcg_jacobi']:.2f} s (Jacobi-PCG, est.)")
         if not args.no_cpu_baseline:
             cp = cpu_reference_passage()
             if cp is not None:
                 passage["cpu_reference"] = cp
+    production = None
+    if rank == 0 and world == 1 and not args.no_production:
+        production = production_passage()
+        _log(f"production passage: {production['s_per_passage_lu']:.1f} s (LU), "
+             f"{production['s_per_passage_pcg_mg']:.1f} s (MG-PCG); solve 1024^2: "
+             f"{production['poisson_solve']['lu_ms']:.2f} ms LU, {production['poisson_solve']['mg_cold_ms']:.2f} ms "
+             f"MG-PCG cold, {production['poisson_solve']['mg_warm_ms']:.2f} ms warm")
 
     if rank == 0:
         line = {"metric": METRIC, "value": n * world / (ms_step * 1e-3), "unit": METRIC, "n_gpus": world,
@@ -428,6 +550,8 @@ def run_ours(args, rank, world, local_rank):
             line["cpu_baseline"] = cpu
         if passage is not None:
             line["bunch_passage"] = passage
+        if production is not None:
+            line["production_passage"] = production
         print(json.dumps(line), flush=True)
 
 
@@ -445,6 +569,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-passage", action="store_true", help="skip the buildup bunch-passage timing")
+    ap.add_argument("--no-production", action="store_true",
+                    help="skip the 1024x1024 production passage sample and solve comparison")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -245,7 +245,8 @@ typedef struct oec_furman {
     int32_t reserved;
 } oec_furman_t;
 
-/* Bytes of `work_dev` oec_furman_emit needs for `cap` absorbed rows. */
+/* Bytes of `work_dev` oec_furman_emit needs for `cap` absorbed rows
+ * (cap <= 2^26; -1 beyond). */
 int64_t oec_furman_work_bytes(int32_t cap);
 
 /* generateSecondaries (particleEmitter.pyx:154-308) on the absorbed rows at
@@ -396,6 +397,45 @@ int oec_stencil_apply(const oec_stencil_t *st, const double *x_dev, double *y_de
 #define OEC_PRECOND_NONE 0
 #define OEC_PRECOND_JACOBI 1
 #define OEC_PRECOND_CNN 2
+#define OEC_PRECOND_MG 3
+
+/* Multigrid preconditioner for oec_pcg_solve (precond = OEC_PRECOND_MG,
+ * precond_ctx = an oec_mg_t): one V-cycle of aggregation multigrid on the
+ * scaled operator.  No counterpart in the reference, whose only solve is the
+ * direct one (poissonSolver.pyx:83-88).  Level 0 is the solver's f32 operator
+ * (leak 0); level l+1 aggregates 2x2 nodes of level l (node (r, c) ->
+ * (r/2, c/2), nx_{l+1} = (nx_l + 1) / 2), and its operator is the Galerkin
+ * product P^T A P with the piecewise-constant P: again a 5-point stencil plus
+ * a diagonal "leak" (the weight of edges from inside nodes to the fixed
+ * outside).  On a level, (A x)_i = leak_i x_i + sum over the 4 grid edges of
+ * w (x_i - x_j), with x = 0 outside; a node is inside exactly when its
+ * dinv (1/diagonal) is nonzero.  Two damped-Jacobi sweeps (weight omega)
+ * before and after the coarse correction, which is scaled by `scale`.
+ * Levels block_level .. nlevels-1 are solved by one CTA in shared memory
+ * (7 floats per node of those levels, at most 226 KB), the last of them by
+ * its dense inverse over its inside nodes. */
+typedef struct oec_mg_level {
+    int32_t nx, ny;
+    const float *ex, *ey, *leak, *dinv;  /* [nx*ny] edge weights (ex: (r,c)-(r,c+1), ey: (r,c)-(r+1,c)), leak,
+                                            1/diagonal (0 outside) */
+    const uint8_t *inside;               /* [nx*ny] (informational; dinv decides) */
+    float *b, *x, *y;                    /* [nx*ny] work: right-hand side, pre-smoothed iterate, result */
+} oec_mg_level_t;
+
+typedef struct oec_mg {
+    int32_t nlevels;                 /* 1..16 */
+    const oec_mg_level_t *levels;    /* HOST array, level 0 the fine grid */
+    int32_t block_level;             /* first level solved inside one CTA; at most 8 levels from there */
+    int32_t ncoarse;                 /* inside nodes of the coarsest level (1..1024) */
+    const int32_t *coarse_idx;       /* [ncoarse] their node indices */
+    const float *coarse_inv;         /* [ncoarse*ncoarse] row-major inverse of its operator */
+    float omega;                     /* damped-Jacobi weight */
+    float scale;                     /* coarse-correction scale */
+} oec_mg_t;
+
+/* z = M r, one V-cycle (r, z f32 [nx*ny] of level 0; z is 0 outside).
+ * Overlapping calls with one oec_mg_t race on its work vectors. */
+int oec_mg_apply(const oec_mg_t *mg, const float *r_dev, float *z_dev, void *stream);
 
 typedef struct oec_pcg_stats {
     int32_t iterations;   /* f32 inner iterations, all refinements */
@@ -412,17 +452,35 @@ int64_t oec_pcg_work_bytes(int32_t nx, int32_t ny);
  * poissonSolver.pyx:85).  phi = A^-1 q on the inside nodes by f64 iterative
  * refinement around an f32 flexible preconditioned conjugate-gradient solve:
  * each refinement forms r = q - A phi in f64, solves A d = r in f32 to a
- * relative max(1e-6, tol / (2 ||r||/||q||)) (or stagnation), and adds d in
- * f64; it stops when
- * ||r||/||q|| <= tol or after max_iter inner iterations in total.
+ * relative max(1e-6, tol / (2 ||r||/||q||)) (or stagnation: the best inner
+ * residual did not drop by 10 % in 1024 iterations), and adds d in f64; it
+ * stops when ||r||/||q|| <= tol, after max_iter inner iterations in total,
+ * after 12 refinements, or when a refinement gained less than a factor 2.
  * phi_dev holds the warm start on entry (zeros for none) and the solution on
- * return (0 outside).  precond: OEC_PRECOND_NONE / _JACOBI / _CNN (precond_ctx
- * = an oec_cnn_t, see below).  stats (host) reports convergence; the caller
+ * return (0 outside).  precond: OEC_PRECOND_NONE / _JACOBI / _CNN
+ * (precond_ctx = an oec_cnn_t, see below) / _MG (precond_ctx = an oec_mg_t).
+ * max_iter <= 2^24.  The solve runs as one CUDA graph whose loops the device
+ * controls (conditional nodes); it is instantiated on the first call with
+ * given arguments and cached by the argument values and the contents of the
+ * structures they point to.  stats (host) reports convergence; the caller
  * falls back to oec_lu_solve when stats->converged is 0.  work_dev:
- * oec_pcg_work_bytes.  Synchronises the stream every few iterations. */
+ * oec_pcg_work_bytes.  Synchronises the stream once, at the end; not
+ * callable on a capturing stream (use oec_pcg_solve_async). */
 int oec_pcg_solve(const oec_stencil_t *st, const double *q_dev, double *phi_dev, double tol, int32_t max_iter,
                   int32_t precond, const void *precond_ctx, void *work_dev, oec_pcg_stats_t *stats,
                   void *stream);
+
+/* The same solve without any host synchronisation: stats_dev (device
+ * oec_pcg_stats_t) receives the statistics.  With fallback (an oec_lu_t, its
+ * work in lu_work_dev) the device runs oec_lu_solve when the solve missed tol
+ * and adds 1 to *fallback_count_dev (optional).  On a capturing stream the
+ * solve is recorded into the capture (a buildup step graph replays it with
+ * its loops intact); otherwise the cached graph is launched on the stream.
+ * Overlapping solves with one work_dev race. */
+int oec_pcg_solve_async(const oec_stencil_t *st, const double *q_dev, double *phi_dev, double tol,
+                        int32_t max_iter, int32_t precond, const void *precond_ctx, void *work_dev,
+                        oec_pcg_stats_t *stats_dev, const oec_lu_t *fallback, double *lu_work_dev,
+                        int32_t *fallback_count_dev, void *stream);
 
 /* ------------------------------------- learned preconditioner (no counterpart
  * in the reference): a linear 4-level U-Net (16-32-64-64 channels, 3x3

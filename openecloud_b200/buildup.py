@@ -53,13 +53,15 @@ class Buildup:
 
     Parameters mirror the configuration of example01_basic.py; `capacity`
     bounds the device particle store (the run reports a capacity drop in the
-    status block instead of writing past it)."""
+    status block instead of writing past it).  `poisson` reuses a
+    PoissonSolver built for the same grid (its factorisation is the costly
+    part of the setup on large grids)."""
 
     def __init__(self, nx=128, ny=128, lx=0.04, ly=0.04, boundType=1, n_init=10000, w_init=None, dt=1e-11,
                  beam="endless", beam_particles=1.1e11, radius_sigma=0.002, bunch_length_sigma=0.25e-9 * 299792458.0,
                  material="copper", sey_max=1.6, e_hat0=300.0, type_b_field=0, b_const=(0., 0., 0.),
                  target=100000, management="global", management_every=50, capacity=None, seed=0,
-                 n_steps_table=2500, sort_every=0, boundFunc=None):
+                 n_steps_table=2500, sort_every=0, boundFunc=None, poisson=None):
         self.grid = Grid(nx, ny, lx, ly, boundType, boundFunc=boundFunc)
         self.dt = float(dt)
         self.target = int(target)
@@ -82,7 +84,10 @@ class Buildup:
         self.em = FurmanEmitter(self.bd, self.P, material=material, seyMax=sey_max, seed=seed + 17)
         if e_hat0 is not None:
             self.em.setEHat0(e_hat0)
-        self.ps = PoissonSolver(self.grid)
+        if poisson is not None and (poisson.gridObj.getNxExt(), poisson.gridObj.getNyExt()) != \
+                (self.grid.getNxExt(), self.grid.getNyExt()):
+            raise ValueError("poisson: a solver for another grid")
+        self.ps = poisson if poisson is not None else PoissonSolver(self.grid)
         beam_cls = LHCBeamEndless if beam == "endless" else LHCBeam
         self.beam = beam_cls(self.grid, self.dt, nParticles=beam_particles, radiusSigma=radius_sigma,
                              bunchLengthSigma=bunch_length_sigma)
@@ -107,6 +112,8 @@ class Buildup:
         _lib.call("oec_history", self.P.c_particles(), self.step_dev.data_ptr(), self._table_len,
                   self.hist_w.data_ptr(), self.hist_n.data_ptr(), self.scratch.data_ptr(), D.stream())
         self.graph = None
+        self._graph_sig = None
+        self._cap_stream = None
         self.steps_done = 0
 
     # ------------------------------------------------------------ pieces
@@ -185,14 +192,15 @@ class Buildup:
                 raise ValueError("beam table exhausted: increase n_steps_table")
             if self.sort_every and step % self.sort_every == 0 and step > 0:
                 self.P.sortByColumn(6)
-            changed = step % self.management_every == 0 and self._manage(step)
+            if step % self.management_every == 0:
+                self._manage(step)
             # steps until the next management / sort point
             nxt = n_steps - k
             for every in (self.management_every, self.sort_every):
                 if every:
                     nxt = min(nxt, every - (step % every))
             if use_graph:
-                self._replay(nxt, rebuild=changed or self.graph is None)
+                self._replay(nxt)
             else:
                 for _ in range(nxt):
                     self._launch_step()
@@ -202,12 +210,43 @@ class Buildup:
         self.steps_done += n_steps
         return t0.elapsed_time(t1) * 1e-3
 
-    def _replay(self, n, rebuild):
-        # A captured step holds raw device pointers; any reallocation
-        # (management, sorting swaps the store) needs a new capture.
-        self.graph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(self.graph):
-            self._launch_step()
+    def _step_signature(self):
+        """Everything a captured step bakes in: device buffers (a
+        reallocation by management or sorting changes them) and the solver
+        settings."""
+        P, bd, em, ps = self.P, self.bd, self.em, self.ps
+        bufs = (P._mask, P._rho_fix, P._wscale, P._status, P._scan_scratch, bd._index, bd._rows, bd._normals,
+                bd._n_abs, bd._scratch, em._work, em._out, em._n_out, self.btab)
+        return (bytes(P.c_particles()), tuple(0 if t is None else t.data_ptr() for t in bufs), bytes(em.c_params()),
+                em.seed, ps.method, ps.precond, ps.warmStart, ps.pcgTol, ps.pcgMaxIter, id(ps.cnn))
+
+    def _capture(self):
+        """Records one time step into a CUDA graph (on a capture stream of its
+        own; torch.cuda.graph's garbage collection per capture would cost
+        more than the step)."""
+        self.ps.prepare()
+        if self._cap_stream is None:
+            self._cap_stream = torch.cuda.Stream()
+        cur = torch.cuda.current_stream()
+        cs = self._cap_stream
+        cs.wait_stream(cur)
+        self.graph = None
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(cs):
+            g.capture_begin()
+            try:
+                self._launch_step()
+            finally:
+                g.capture_end()
+        cur.wait_stream(cs)
+        self.graph = g
+        self._graph_sig = self._step_signature()
+
+    def _replay(self, n):
+        # A captured step holds raw device pointers: capture again when any
+        # of them changed.
+        if self.graph is None or self._graph_sig != self._step_signature():
+            self._capture()
         for _ in range(n):
             self.graph.replay()
 

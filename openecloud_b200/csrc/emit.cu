@@ -223,6 +223,13 @@ __global__ void k_furman_pass2(oec_furman_t f, const double *__restrict__ rows, 
 // ------------------------------------------------------------------ scan
 
 constexpr int kScanT = 1024;
+constexpr int kMaxAbsorbedRows = 1 << 26;
+
+// Blocks of the two-level count scan (at least kScanT partial slots).
+inline int scan_blocks(int cap) {
+    const int nb = (cap + kScanT - 1) / kScanT;
+    return nb > kScanT ? nb : kScanT;
+}
 
 __device__ __forceinline__ int block_scan_excl(int v, int *tot, int *sh) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -261,13 +268,20 @@ __global__ void k_scan_blocks(const int32_t *in, const int32_t *n_p, int cap, in
     if (threadIdx.x == 0) partial[blockIdx.x] = tot;
 }
 
+// Exclusive scan of the nb block totals by one CTA, kScanT at a time with a
+// running carry.
 __global__ void k_scan_partials(int *partial, int nb, int32_t *total) {
     __shared__ int sh[32];
-    int v = threadIdx.x < nb ? partial[threadIdx.x] : 0;
-    int tot;
-    int ex = block_scan_excl(v, &tot, sh);
-    if (threadIdx.x < nb) partial[threadIdx.x] = ex;
-    if (threadIdx.x == 0) *total = tot;
+    int carry = 0;
+    for (int base = 0; base < nb; base += kScanT) {
+        const int i = base + threadIdx.x;
+        const int v = i < nb ? partial[i] : 0;
+        int tot;
+        const int ex = block_scan_excl(v, &tot, sh);
+        if (i < nb) partial[i] = carry + ex;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) *total = carry;
 }
 
 __global__ void k_scan_add(int32_t *out, const int32_t *n_p, int cap, const int *partial) {
@@ -337,10 +351,10 @@ extern "C" int oec_furman_emit(const oec_furman_t *params, const double *rows_de
     if (!params || !rows_dev || !normals_dev || !n_abs_dev || !work_dev || !out_rows_dev || !n_out_dev ||
         !status_dev || cap < 0 || out_cap < 0 || params->m < 1 || params->m > 10)
         return OEC_ERR_INVALID;
-    int nblocks = (cap + kScanT - 1) / kScanT;
-    if (nblocks > kScanT) return OEC_ERR_INVALID;
+    if (cap > kMaxAbsorbedRows) return OEC_ERR_INVALID;
+    const int nblocks = (cap + kScanT - 1) / kScanT;
     cudaStream_t s = as_stream(stream);
-    // work layout: Rec[cap] | split[cap * kSlots] (f64) | nsec[cap] | offset[cap] | partial[1024]
+    // work layout: Rec[cap] | split[cap * kSlots] (f64) | nsec[cap] | offset[cap] | partial[scan_blocks(cap)]
     char *w = static_cast<char *>(work_dev);
     Rec *rec = reinterpret_cast<Rec *>(w);
     double *split = reinterpret_cast<double *>(w + sizeof(Rec) * (size_t)cap);
@@ -367,8 +381,9 @@ extern "C" int oec_furman_emit(const oec_furman_t *params, const double *rows_de
 }
 
 extern "C" int64_t oec_furman_work_bytes(int32_t cap) {
+    if (cap < 0 || cap > kMaxAbsorbedRows) return -1;
     return (int64_t)sizeof(Rec) * cap + (int64_t)sizeof(double) * kSlots * cap + 2 * sizeof(int32_t) * (int64_t)cap +
-           sizeof(int) * 1024 + 256;
+           sizeof(int) * (int64_t)scan_blocks(cap) + 256;
 }
 
 extern "C" int oec_homo_load(const oec_grid_t *grid, const oec_boundary_t *boundary, oec_particles_t *p, int64_t n,

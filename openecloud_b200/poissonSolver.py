@@ -50,10 +50,120 @@ class PcgStats_t(ctypes.Structure):
                 ("rel_residual0", ctypes.c_double)]
 
 
-PRECOND = {"none": 0, "jacobi": 1, "cnn": 2}
+PRECOND = {"none": 0, "jacobi": 1, "cnn": 2, "mg": 3}
+
+
+class MgLevel_t(ctypes.Structure):
+    _P = ctypes.c_void_p
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("ex", _P), ("ey", _P), ("leak", _P), ("dinv", _P),
+                ("inside", _P), ("b", _P), ("x", _P), ("y", _P)]
+
+
+class Mg_t(ctypes.Structure):
+    _P = ctypes.c_void_p
+    _fields_ = [("nlevels", ctypes.c_int32), ("levels", ctypes.POINTER(MgLevel_t)), ("block_level", ctypes.c_int32),
+                ("ncoarse", ctypes.c_int32), ("coarse_idx", _P), ("coarse_inv", _P), ("omega", ctypes.c_float),
+                ("scale", ctypes.c_float)]
+
+
+MG_BLOCK_SMEM = 226 * 1024   # dynamic shared memory of the one-CTA coarse solve
+MG_FLOATS_PER_NODE = 7
+MG_BLOCK_TOP = 1280          # largest level given to the one-CTA solve (one SM's issue rate bounds it)
+
+
+def mg_coarsen(ex, ey, lkx, lky, inside, nx, ny, fx=2, fy=2):
+    """Coarse level of the aggregation multigrid: aggregates of fx x fy nodes
+    (fx, fy in {1, 2}; node (r, c) -> (r // fy, c // fx)) with the
+    piecewise-constant P.  Per direction the coarse operator is the Galerkin
+    product of that direction's part of A divided by the aggregation factor
+    along it, A_c = P^T A_x P / fx + P^T A_y P / fy, which is what
+    rediscretising the FIT operator on cells fx times wider and fy times
+    taller gives (the weight of a face is its length over the distance across
+    it): x-edges between inside nodes of different aggregates add w / fx to
+    the coarse x-edge, y-edges w / fy to the coarse y-edge, edges from an
+    inside node to the fixed outside and the leaks the same to the coarse
+    leak of their direction; edges inside an aggregate cancel.  Keeping the
+    directions apart is what lets a strongly anisotropic grid coarsen along
+    one direction only.  Returns (ex, ey, lkx, lky, inside, nx, ny)."""
+    NX, NY = (nx + fx - 1) // fx, (ny + fy - 1) // fy
+    j, i = np.divmod(np.arange(nx * ny), nx)
+    agg = (j // fy) * NX + (i // fx)
+    inn = np.asarray(inside, bool)
+    exc, eyc = np.zeros(NX * NY), np.zeros(NX * NY)
+    lxc, lyc = np.zeros(NX * NY), np.zeros(NX * NY)
+    ins = np.zeros(NX * NY, bool)
+    ins[agg[inn]] = True
+    np.add.at(lxc, agg[inn], lkx[inn] / fx)
+    np.add.at(lyc, agg[inn], lky[inn] / fy)
+    a_all = np.arange(nx * ny)
+    for w, step, valid, tgt, lk, f in ((ex, 1, i < nx - 1, exc, lxc, fx), (ey, nx, j < ny - 1, eyc, lyc, fy)):
+        a = a_all[valid]
+        b = a + step
+        wa = w[a] / f
+        ia, ib = inn[a], inn[b]
+        cross = ia & ib & (agg[a] != agg[b])
+        np.add.at(tgt, agg[a][cross], wa[cross])
+        la, lb = ia & ~ib, ib & ~ia
+        np.add.at(lk, agg[a][la], wa[la])
+        np.add.at(lk, agg[b][lb], wa[lb])
+    return exc, eyc, lxc, lyc, ins, NX, NY
+
+
+def mg_factors(ex, ey, inside, nx, ny, ratio=2.0):
+    """Aggregation factors (fx, fy) of the next level: coarsen only along the
+    strongly coupled direction while the mean inside-edge weights differ by
+    more than `ratio`, else both ways."""
+    ins = np.asarray(inside, bool)
+    col = np.arange(nx * ny) % nx
+    hx = ins & (col < nx - 1) & np.roll(ins, -1)
+    vy = ins & np.concatenate([ins[nx:], np.zeros(nx, bool)])
+    wx = ex[hx].mean() if hx.any() else 0.0
+    wy = ey[vy].mean() if vy.any() else 0.0
+    if wy > ratio * wx and ny > 1:
+        return 1, 2
+    if wx > ratio * wy and nx > 1:
+        return 2, 1
+    return 2, 2
+
+
+def mg_hierarchy(ex, ey, inside, nx, ny, bottom=100, semi=True):
+    """Levels (ex, ey, leak, inside, nx, ny) of the aggregation multigrid,
+    finest first, coarsened until a level has at most `bottom` nodes, and the
+    block level: the first level of at most MG_BLOCK_TOP nodes from which all
+    coarser ones fit the one-CTA shared-memory solve."""
+    z = np.zeros(nx * ny)
+    cur = (np.asarray(ex, np.float64), np.asarray(ey, np.float64), z, z, np.asarray(inside, bool), nx, ny)
+    lv = [cur[:2] + (z,) + cur[4:]]
+    while cur[5] * cur[6] > bottom and max(cur[5], cur[6]) > 1:
+        e, f, _, _, ins, X, Y = cur
+        cur = mg_coarsen(*cur, *(mg_factors(e, f, ins, X, Y) if semi else (2, 2)))
+        lv.append(cur[:2] + (cur[2] + cur[3],) + cur[4:])
+    sizes = [l[4] * l[5] for l in lv]
+    block = len(lv) - 1
+    while block > 0 and len(lv) - (block - 1) <= 8 and sizes[block - 1] <= MG_BLOCK_TOP and \
+            4 * MG_FLOATS_PER_NODE * sum(sizes[block - 1:]) <= MG_BLOCK_SMEM:
+        block -= 1
+    return lv, block
+
+
+def mg_apply_host(ex, ey, leak, inside, nx, x):
+    """Host restatement of a multigrid level's operator (oec_mg_level_t)."""
+    n = ex.size
+    ins = np.asarray(inside, bool)
+    xm = np.where(ins, x, 0.0)
+    col = np.arange(n) % nx
+    y = leak * xm
+    right = np.where(col + 1 < nx, np.roll(xm, -1), 0.0)
+    left = np.where(col > 0, np.roll(xm, 1), 0.0)
+    up = np.concatenate([xm[nx:], np.zeros(nx)])
+    down = np.concatenate([np.zeros(nx), xm[:-nx]])
+    y = y + ex * (xm - right) + np.where(col > 0, np.roll(ex, 1), 0.0) * (xm - left)
+    y = y + ey * (xm - up) + np.concatenate([np.zeros(nx), ey[:-nx]]) * (xm - down)
+    return np.where(ins, y, 0.0)
 
 _lib.OTHER_DECLARED.update({"oec_lu_solve", "oec_spmv_csr", "oec_trsv_levels", "oec_stencil_apply",
-                            "oec_pcg_work_bytes", "oec_pcg_solve"})
+                            "oec_pcg_work_bytes", "oec_pcg_solve", "oec_mg_apply",
+                            "oec_pcg_solve_async"})
 
 
 def _declare():
@@ -74,6 +184,10 @@ def _declare():
         L.oec_pcg_solve.restype = ctypes.c_int
         L.oec_pcg_solve.argtypes = [ctypes.POINTER(Stencil_t), P, P, ctypes.c_double, ctypes.c_int32,
                                     ctypes.c_int32, P, P, ctypes.POINTER(PcgStats_t), P]
+        L.oec_mg_apply.argtypes = [ctypes.POINTER(Mg_t), P, P, P]
+        L.oec_pcg_solve_async.restype = ctypes.c_int
+        L.oec_pcg_solve_async.argtypes = [ctypes.POINTER(Stencil_t), P, P, ctypes.c_double, ctypes.c_int32,
+                                          ctypes.c_int32, P, P, P, ctypes.POINTER(LU_t), P, P, P]
         L._poisson_declared = True
     return L
 
@@ -172,10 +286,14 @@ class PoissonSolver:
         self.pcgTol = float(pcgTol)
         self.pcgMaxIter = int(pcgMaxIter)
         self.cnn = None          # a trained network (openecloud_b200.cnn) for precond='cnn' / warmStart='cnn'
+        self._mg = None          # multigrid hierarchy for precond='mg' (built on first use)
         self.warmStart = warmStart  # 'previous' (last phi), 'zero' or 'cnn'
-        self.lastStats = None    # PcgStats_t of the last iterative solve
         self.nSolves = 0
-        self.nFallbacks = 0
+        # statistics of the last iterative solve and the count of LU
+        # fallbacks stay on the device (no host round trip per solve)
+        self._stats_dev = D.zeros(ctypes.sizeof(PcgStats_t), torch.uint8)
+        self._fb_count = D.zeros(1, torch.int32)
+        self._pcg_used = False
 
     def _stencil_setup(self, meps, nx, npn):
         """Edge weights of A on the full extended grid (oec_stencil_t)."""
@@ -201,6 +319,52 @@ class PoissonSolver:
         st.scale32 = scale
         self._stencil = st
         self._pcg_work = D.empty(int(_declare().oec_pcg_work_bytes(st.nx, st.ny)), torch.uint8)
+
+    def _mg_setup(self, omega=0.8, scale=1.0, bottom=100):
+        """Aggregation multigrid hierarchy (oec_mg_t) on the scaled f32
+        operator, down to at most `bottom` nodes, whose inside block is
+        inverted densely (f64 on the host, stored in f32).  The host copy of
+        every level (ex, ey, leak, inside, nx, ny) is kept under "host"."""
+        st = self._stencil
+        k = self._keep
+        ex = D.to_numpy(k["ex32"]).astype(np.float64)
+        ey = D.to_numpy(k["ey32"]).astype(np.float64)
+        inside = D.to_numpy(k["inside"]).astype(bool)
+        lv, block = mg_hierarchy(ex, ey, inside, st.nx, st.ny, bottom)
+        e, f, lk, ins, X, Y = lv[-1]
+        idx = np.nonzero(ins)[0]
+        M = np.empty((idx.size, idx.size))
+        for c in range(idx.size):
+            v = np.zeros(X * Y)
+            v[idx[c]] = 1.0
+            M[:, c] = mg_apply_host(e, f, lk, ins, X, v)[idx]
+        keep = []
+        levels = (MgLevel_t * len(lv))()
+        for n_, (e, f, lk, ins, X, Y) in enumerate(lv):
+            i = np.nonzero(ins)[0]
+            col = i % X
+            d = lk[i] + e[i] + f[i] + np.where(col > 0, e[np.maximum(i - 1, 0)], 0.0) + \
+                np.where(i >= X, f[np.maximum(i - X, 0)], 0.0)
+            if np.any(d <= 0.0):
+                raise ValueError("multigrid level with a non-positive diagonal")
+            dinv = np.zeros(X * Y)
+            dinv[i] = 1.0 / d
+            t = {"ex": D.to_device(e, torch.float32), "ey": D.to_device(f, torch.float32),
+                 "leak": D.to_device(lk, torch.float32), "dinv": D.to_device(dinv, torch.float32),
+                 "inside": D.to_device(ins.astype(np.uint8), torch.uint8),
+                 "b": D.zeros(X * Y, torch.float32), "x": D.zeros(X * Y, torch.float32),
+                 "y": D.zeros(X * Y, torch.float32)}
+            if n_ == 0:  # the solver's own f32 operator and diagonal
+                t["ex"], t["ey"], t["dinv"] = k["ex32"], k["ey32"], k["dinv32"]
+            keep.append(t)
+            levels[n_] = MgLevel_t(X, Y, *(D.ptr(t[name]) for name in ("ex", "ey", "leak", "dinv", "inside", "b",
+                                                                       "x", "y")))
+        cidx = D.to_device(idx.astype(np.int32), torch.int32)
+        cinv = D.to_device(np.linalg.inv(M).astype(np.float32), torch.float32)
+        mg = Mg_t(len(lv), levels, block, idx.size, D.ptr(cidx), D.ptr(cinv), omega, scale)
+        self._mg = {"c": mg, "levels": levels, "keep": keep, "cidx": cidx, "cinv": cinv, "nlevels": len(lv),
+                    "block_level": block, "host": lv}
+        return self._mg
 
     def applyOperator(self, x):
         """A x on the inside nodes (device f64 [npExt] in and out)."""
@@ -281,11 +445,36 @@ class PoissonSolver:
         if rc:
             raise _lib.OecError("oec_lu_solve", rc)
 
+    @property
+    def lastStats(self):
+        """PcgStats_t of the last iterative solve (None before the first)."""
+        if not self._pcg_used:
+            return None
+        return PcgStats_t.from_buffer_copy(D.to_numpy(self._stats_dev).tobytes())
+
+    @property
+    def nFallbacks(self):
+        """Iterative solves that missed pcgTol and were redone by LU."""
+        return int(D.to_numpy(self._fb_count)[0])
+
+    def prepare(self):
+        """Builds what the configured iterative solve needs (the multigrid
+        hierarchy) ahead of a CUDA graph capture that records the solve."""
+        if self.method == "pcg" and self.precond == "mg" and self._mg is None:
+            if torch.cuda.is_current_stream_capturing():
+                raise RuntimeError("PoissonSolver.prepare() must run before the graph capture")
+            self._mg_setup()
+
     def _pcg_solve(self, q):
-        """Iterative solve warm-started from the current phi; False if it missed pcgTol."""
+        """Iterative solve warm-started from the current phi, with the LU
+        solve run on the device when it misses pcgTol; enqueued without host
+        synchronisation (and recorded whole when the stream is capturing)."""
         pc = PRECOND[self.precond]
         ctx = None
-        if pc == PRECOND["cnn"]:
+        if pc == PRECOND["mg"]:
+            self.prepare()
+            ctx = ctypes.cast(ctypes.pointer(self._mg["c"]), ctypes.c_void_p)
+        elif pc == PRECOND["cnn"]:
             if self.cnn is None:
                 raise ValueError("precond='cnn' needs a trained network in PoissonSolver.cnn")
             ctx = self.cnn.c_handle()
@@ -297,28 +486,27 @@ class PoissonSolver:
             self.cnn.warm_start(self._stencil.scale32, q, self.phi)
         elif self.warmStart != "previous":
             raise ValueError("warmStart must be 'previous', 'zero' or 'cnn'")
-        st = PcgStats_t()
-        rc = _declare().oec_pcg_solve(ctypes.byref(self._stencil), q.data_ptr(), self.phi.data_ptr(), self.pcgTol,
-                                      self.pcgMaxIter, pc, ctx, self._pcg_work.data_ptr(), ctypes.byref(st),
-                                      D.stream())
+        rc = _declare().oec_pcg_solve_async(ctypes.byref(self._stencil), q.data_ptr(), self.phi.data_ptr(),
+                                            self.pcgTol, self.pcgMaxIter, pc, ctx, self._pcg_work.data_ptr(),
+                                            self._stats_dev.data_ptr(), ctypes.byref(self._lu_t),
+                                            self._work.data_ptr(), self._fb_count.data_ptr(), D.stream())
         if rc:
-            raise _lib.OecError("oec_pcg_solve", rc)
-        self.lastStats = st
-        return bool(st.converged)
+            raise _lib.OecError("oec_pcg_solve_async", rc)
+        self._pcg_used = True
 
     def solveDevice(self, q, method=None):
         """q: device float64 [npExt] charge per node -> device E [2*npExt].
 
-        method 'lu' (default of the instance: self.method) or 'pcg' (falls
-        back to LU when the f64 relative residual misses pcgTol)."""
+        method 'lu' (default of the instance: self.method) or 'pcg' (the
+        device falls back to LU when the f64 relative residual misses
+        pcgTol).  Enqueues work only: no host synchronisation, so a buildup
+        step that contains it can be captured into a CUDA graph."""
         L = _declare()
         s = D.stream()
         method = method or self.method
         self.nSolves += 1
         if method == "pcg":
-            if not self._pcg_solve(q):
-                self.nFallbacks += 1
-                self._lu_solve(q)
+            self._pcg_solve(q)
         elif method == "lu":
             self._lu_solve(q)
         else:

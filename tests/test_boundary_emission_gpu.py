@@ -182,3 +182,20 @@ def test_homo_loader_uniform_inside(gpu):
     assert kstest(r2, "uniform").pvalue > 1e-3
     assert np.all(pd[:, 5] == np.float32(1e5))
     assert np.max(np.abs(pd[:, 2:5])) < 1e-200
+
+
+def test_emission_beyond_one_scan_chunk(gpu):
+    """More absorbed rows than one CTA scans in one pass (1080 x 1112 rows,
+    1173 scan blocks): the secondaries of the first half equal those of an
+    emission of the first half alone (each row's draws are keyed by its own
+    index; the last-particle compatibility switch is off so that no row
+    depends on another)."""
+    z, em, _, rows, _ = _emit_setup(0, n_rep=1112)
+    assert len(rows) > 1024 * 1024
+    em.compat = False
+    big = em.generateSecondaries().cpu().numpy()
+    z, em2, _, rows2, _ = _emit_setup(0, n_rep=556)
+    em2.compat = False
+    small = em2.generateSecondaries().cpu().numpy()
+    assert len(big) > len(small) > 0
+    assert np.array_equal(big[:len(small)], small)

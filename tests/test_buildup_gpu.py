@@ -36,3 +36,34 @@ def test_buildup_line_density_within_reference_spread(gpu):
     assert not bad.any(), (np.nonzero(bad)[0][:10], m_gpu[bad][:5], m_ref[bad][:5])
     # the cloud builds up over the passage as in the reference
     assert m_gpu[-1] / m_gpu[0] > 1.2
+
+
+def test_buildup_step_graph_with_multigrid_pcg(gpu):
+    """The iterative solve recorded inside the captured buildup step (its
+    refinement and inner loops as conditional graph nodes) converges on every
+    replay without a fallback: the last step's phi equals the LU solve of the
+    same charge within what the 1e-8 residual allows, and the run follows the
+    LU run's macro-particle count."""
+    import torch
+    from openecloud_b200 import device as D
+    from openecloud_b200.buildup import Buildup
+    steps = 200
+    lu = Buildup(seed=1001, n_steps_table=steps + 1)
+    lu.run(steps)
+    b = Buildup(seed=1001, n_steps_table=steps + 1)
+    b.ps.method = "pcg"
+    b.ps.precond = "mg"
+    b.run(steps)
+    st = b.status()
+    assert st["n_capacity_drop"] == 0 and st["n_nonfinite"] == 0
+    stats = b.ps.lastStats
+    assert b.ps.nFallbacks == 0 and stats.converged == 1 and stats.rel_residual <= 1e-8, \
+        (b.ps.nFallbacks, stats.converged, stats.rel_residual)
+    phi = b.ps.phi.clone()
+    b.ps._lu_solve(b.rho)
+    torch.cuda.synchronize()
+    ref = D.to_numpy(b.ps.phi)
+    assert np.abs(D.to_numpy(phi) - ref).max() <= 1e-6 * np.abs(ref).max()
+    n_lu, w_lu = lu.history()
+    n_pcg, w_pcg = b.history()
+    assert abs(w_pcg[-1] / w_lu[-1] - 1.0) < 0.05, (w_pcg[-1], w_lu[-1])

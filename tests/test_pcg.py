@@ -49,6 +49,103 @@ def test_stencil_on_polygon_cut_cell_grid():
     assert np.max(np.abs(y - ref)) <= 1e-13 * np.max(np.abs(ref))
 
 
+def _level_matrix(ex, ey, lk, inside, nx, ny):
+    """Sparse operator of a multigrid level over all its nodes (rows and
+    columns of outside nodes empty): leak + incident edge weights on the
+    diagonal, -w between inside neighbours."""
+    import scipy.sparse as spsp
+    n = nx * ny
+    ins = np.asarray(inside, bool)
+    j, i = np.divmod(np.arange(n), nx)
+    d = np.array(lk, dtype=float)
+    rows, cols, vals = [], [], []
+    for w, step, valid in ((ex, 1, i < nx - 1), (ey, nx, j < ny - 1)):
+        a = np.nonzero(valid)[0]
+        b = a + step
+        d[a] += w[a]
+        d[b] += w[a]
+        both = ins[a] & ins[b]
+        rows += [a[both], b[both]]
+        cols += [b[both], a[both]]
+        vals += [-w[a][both], -w[a][both]]
+    d = np.where(ins, d, 0.0)
+    rows.append(np.arange(n))
+    cols.append(np.arange(n))
+    vals.append(d)
+    return spsp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, n))
+
+
+@pytest.mark.parametrize("args", HOST_GRIDS)
+def test_mg_coarse_level_is_directional_galerkin_product(args):
+    """Each coarse multigrid level splits by direction into
+    P^T A_x P / fx + P^T A_y P / fy (piecewise-constant P over fx x fy
+    aggregates; level 0 = the assembled matrix), three levels down; on the
+    anisotropic ellipse the first steps coarsen along y only."""
+    import scipy.sparse as spsp
+    from openecloud_b200.grid import Grid
+    from openecloud_b200.poissonSolver import assemble, mg_coarsen, mg_factors
+    sys_path_oracle()
+    from mg_oracle import parent
+    g = Grid(*args)
+    a, meps, _, ins = assemble(g)
+    nx, ny = g.getNxExt(), g.getNyExt()
+    n = nx * ny
+    mask = np.asarray(g.getInsidePoints()) != 0
+    ex, ey, z = meps[:n], meps[n:], np.zeros(n)
+    Ax, Ay = _level_matrix(ex, z, z, mask, nx, ny), _level_matrix(z, ey, z, mask, nx, ny)
+    A = (Ax + Ay).tocsr()[ins][:, ins]
+    assert abs(A - a).max() <= 1e-12 * abs(a).max()
+    cur = (ex, ey, z, z, mask, nx, ny)
+    factors = []
+    for _ in range(3):
+        fx, fy = mg_factors(cur[0], cur[1], cur[4], cur[5], cur[6])
+        factors.append((fx, fy))
+        nxt = mg_coarsen(*cur, fx, fy)
+        NX, NY = nxt[5], nxt[6]
+        P = spsp.csr_matrix((np.ones(cur[5] * cur[6]), (np.arange(cur[5] * cur[6]), parent(cur[5], cur[6], NX, NY))),
+                            shape=(cur[5] * cur[6], NX * NY))
+        Ax, Ay = (P.T @ Ax @ P) / fx, (P.T @ Ay @ P) / fy
+        zc = np.zeros(NX * NY)
+        for got, want in ((_level_matrix(nxt[0], zc, nxt[2], nxt[4], NX, NY, ), Ax),
+                          (_level_matrix(zc, nxt[1], nxt[3], nxt[4], NX, NY), Ay)):
+            assert abs(got - want).max() <= 1e-12 * abs(want).max()
+        assert np.all(nxt[4] == (np.asarray(P.T @ cur[4].astype(float)) > 0))
+        cur = nxt
+    if args[2] / args[0] > 2 * args[3] / args[1]:  # cells wider than tall: strong y coupling
+        assert factors[0] == (1, 2)
+    elif args[0] == args[1] and args[2] == args[3]:
+        assert factors == [(2, 2)] * 3
+
+
+def test_mg_hierarchy_layout():
+    """Level sizes halve (rounded up) down to at most 100 nodes; the block
+    level is the first of at most MG_BLOCK_TOP nodes from which the coarser
+    levels fit the one-CTA shared-memory solve (7 floats per node, 226 KB),
+    at most 8 levels."""
+    from openecloud_b200.poissonSolver import mg_hierarchy, MG_BLOCK_SMEM, MG_BLOCK_TOP
+    for nx, ny in ((1026, 1026), (130, 130), (66, 66), (26, 22), (515, 130)):
+        yy, xx = np.mgrid[0:ny, 0:nx]
+        inside = ((xx - nx / 2) / (nx / 2 - 1.5)) ** 2 + ((yy - ny / 2) / (ny / 2 - 1.5)) ** 2 < 1
+        lv, block = mg_hierarchy(np.ones(nx * ny), np.ones(nx * ny), inside.ravel(), nx, ny)
+        sizes = [(l[4], l[5]) for l in lv]
+        for (a, b), (c, d) in zip(sizes, sizes[1:]):  # isotropic weights: both directions halve
+            assert (c, d) == ((a + 1) // 2, (b + 1) // 2)
+        assert sizes[-1][0] * sizes[-1][1] <= 100 and (len(sizes) == 1 or sizes[-2][0] * sizes[-2][1] > 100)
+        smem = lambda k: 28 * sum(a * b for a, b in sizes[k:])  # noqa: E731
+        top = lambda k: sizes[k][0] * sizes[k][1]  # noqa: E731
+        assert smem(block) <= MG_BLOCK_SMEM and len(sizes) - block <= 8 and top(block) <= max(MG_BLOCK_TOP, 100)
+        assert block == 0 or smem(block - 1) > MG_BLOCK_SMEM or len(sizes) - block + 1 > 8 or \
+            top(block - 1) > MG_BLOCK_TOP
+
+
+def sys_path_oracle():
+    import os
+    import sys
+    d = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle")
+    if d not in sys.path:
+        sys.path.insert(0, d)
+
+
 def _supports_polygon():
     import inspect
     from openecloud_b200.grid import Grid
@@ -79,7 +176,7 @@ def test_stencil_apply_device(gpu, name):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["rect_24x20", "circle_32", "ellipse_40x24", "circle_128"])
-@pytest.mark.parametrize("precond", ["none", "jacobi"])
+@pytest.mark.parametrize("precond", ["none", "jacobi", "mg"])
 def test_pcg_matches_lu_and_reference(gpu, name, precond):
     from openecloud_b200.poissonSolver import PoissonSolver
     z = golden(f"grid_{name}.npz")
@@ -125,3 +222,78 @@ def test_pcg_warm_start_and_fallback(gpu):
     assert ps2.lastStats.converged == 0 and ps2.nFallbacks == 1
     lu = PoissonSolver(_grid(z))
     assert rel_err(E, lu.solve(q)) <= 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["rect_24x20", "ellipse_40x24", "circle_128"])
+def test_mg_vcycle_matches_oracle(gpu, name):
+    """oec_mg_apply (f32) equals the float64 restatement of the V-cycle on the
+    device's own f32 level weights (the small grids run every level in the
+    one-CTA solve, the 128 circle its finest level in the tiled kernels)."""
+    import ctypes
+    import torch
+    from openecloud_b200 import device as D
+    from openecloud_b200.poissonSolver import PoissonSolver, _declare
+    sys_path_oracle()
+    from mg_oracle import vcycle
+    z = golden(f"grid_{name}.npz")
+    ps = PoissonSolver(_grid(z), method="pcg", precond="mg")
+    mg = ps._mg_setup()
+    host = mg["host"]
+    dinv = [D.to_numpy(k["dinv"]).astype(np.float64) for k in mg["keep"]]
+    assert mg["nlevels"] >= 2 and host[-1][4] * host[-1][5] <= 100
+    ins = host[0][3]
+    r = np.where(ins, np.random.default_rng(5).normal(size=ins.size), 0.0).astype(np.float32)
+    rd = D.to_device(r, torch.float32)
+    zd = D.zeros(r.size, torch.float32)
+    rc = _declare().oec_mg_apply(ctypes.byref(mg["c"]), rd.data_ptr(), zd.data_ptr(), D.stream())
+    assert rc == 0
+    got = D.to_numpy(zd).astype(np.float64)
+    want = vcycle(host, r.astype(np.float64), omega=mg["c"].omega, scale=mg["c"].scale, dinv=dinv)
+    assert np.all(got[~ins] == 0.0)
+    assert np.max(np.abs(got - want)) <= 2e-4 * np.max(np.abs(want))
+
+
+@pytest.mark.gpu
+def test_mg_pcg_iterations(gpu):
+    """One V-cycle per iteration cuts the iteration count of the 128x128
+    circle by well over 5x against Jacobi, to the same 1e-8 residual."""
+    from openecloud_b200.poissonSolver import PoissonSolver
+    z = golden("grid_circle_128.npz")
+    q = z["poisson_q"]
+    its = {}
+    for pc in ("jacobi", "mg"):
+        ps = PoissonSolver(_grid(z), method="pcg", precond=pc, pcgTol=1e-8, pcgMaxIter=20000)
+        ps.solve(q)
+        assert ps.lastStats.converged == 1 and ps.nFallbacks == 0
+        its[pc] = ps.lastStats.iterations
+    assert its["mg"] * 5 < its["jacobi"], its
+
+
+@pytest.mark.gpu
+def test_pcg_synchronous_entry_point(gpu):
+    """oec_pcg_solve (host statistics, one synchronisation) gives the
+    asynchronous solve's result (solveDevice) to within the tolerance."""
+    import ctypes
+    import torch
+    from openecloud_b200 import device as D
+    from openecloud_b200.poissonSolver import PoissonSolver, PcgStats_t, PRECOND, _declare
+    z = golden("grid_circle_128.npz")
+    q = z["poisson_q"]
+    ps = PoissonSolver(_grid(z), method="pcg", precond="mg", pcgTol=1e-8, pcgMaxIter=20000)
+    ps.solve(q)
+    a = ps.lastStats
+    phi_async = ps.getPhi()
+    qd = D.to_device(q, torch.float64)
+    phi = D.zeros(ps.n_nodes, torch.float64)
+    mg = ps._mg
+    st = PcgStats_t()
+    rc = _declare().oec_pcg_solve(ctypes.byref(ps._stencil), qd.data_ptr(), phi.data_ptr(), 1e-8, 20000,
+                                  PRECOND["mg"], ctypes.cast(ctypes.pointer(mg["c"]), ctypes.c_void_p),
+                                  ps._pcg_work.data_ptr(), ctypes.byref(st), D.stream())
+    assert rc == 0
+    # the dot products sum f64 atomics in arrival order: same algorithm, not
+    # the same last bits
+    assert st.converged == 1 and a.converged == 1 and st.rel_residual <= 1e-8
+    assert abs(st.iterations - a.iterations) <= 2 and st.refinements == a.refinements
+    assert np.abs(D.to_numpy(phi) - phi_async).max() <= 1e-7 * np.abs(phi_async).max()
