@@ -17,7 +17,8 @@ reference's passage on one host core (the other half of the headline
 metric); and "production_passage": the 1024x1024 elliptical production
 buildup sampled over 100 steps with the LU and multigrid-PCG solves, with
 the single-solve comparison on that grid (LU against the iterative solve at
-relative residual 1e-8).
+relative residual 1e-8); and "batched_scan": 64 independent runs of uneven
+grids advanced in one graph per batch step, with the autotuner's choices.
 
 N > 1 runs under torchrun, one rank per GPU; every rank advances its own
 2^24 particles (independent shards, no collective on the data path:
@@ -354,6 +355,45 @@ def production_passage(steps=100):
     return out
 
 
+BATCH = ("batched scan: 64 independent buildup runs drawn with seed 4 from {256, 512, 768, 1024}^2 grids over "
+         "circular (R=20 mm) and elliptical (45x18 mm) chambers, deltaMax U(1.2, 2.0), 0.5e11-1.5e11 p/bunch, "
+         "B_y 0-8.33 T, 1e4 initial electrons each, roulette cap 5e5 every 50 steps, dt=1e-11 s")
+
+
+def batched_scan(n_runs=64, steps=100, steady=50):
+    """The batched scan in one graph per batch step (runs on parallel
+    branches); the autotuner picks each grid's Poisson solve, the multigrid
+    block size and the branch width (its trial steps are part of the first
+    `steps`); then `steady` more steps at the chosen width."""
+    import torch
+    from openecloud_b200.autotune import Autotuner
+    from openecloud_b200.batch import BatchedBuildup, scan_configs
+    cfgs = scan_configs(n_runs, n_steps_table=steps + steady + 1)
+    t0 = time.perf_counter()
+    tuner = Autotuner()
+    b = BatchedBuildup(cfgs, tuner=tuner)
+    torch.cuda.synchronize()
+    setup = time.perf_counter() - t0
+    first = b.run(steps)
+    sec = b.run(steady)
+    steps_total = steps + steady
+    psteps = sum(int(h[0][steps:steps_total].sum()) for h in b.histories())
+    widths = next(v for k, v in tuner.choices.items() if k.startswith("branches/"))
+    return {"workload": BATCH, "runs": n_runs, "setup_s": setup, "distinct_grids": len(b.shared),
+            "branch_width": b.branches, "ms_per_batch_step_by_width": widths["ms_per_step"],
+            "first_steps": steps, "first_steps_s": first, "steady_steps": steady,
+            "ms_per_batch_step": sec / steady * 1e3, "run_steps_per_s": n_runs * steady / sec,
+            "particle_steps_per_s": psteps / sec,
+            "poisson_choice": {k.split("/", 1)[1]: v["choice"] for k, v in tuner.choices.items()
+                               if k.startswith("poisson/")},
+            "poisson_ms_per_solve": {k.split("/", 1)[1]: v["ms_per_solve"] for k, v in tuner.choices.items()
+                                     if k.startswith("poisson/")},
+            "mg_block_top": {k.split("/", 1)[1]: v["choice"] for k, v in tuner.choices.items()
+                             if k.startswith("mg_block_top/")},
+            "pcg_fallbacks": sum(r.ps.nFallbacks for r in b.runs if r.ps.method == "pcg"),
+            "timing": "device time (CUDA events); steady = after the autotuner's trial steps"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -530,6 +570,12 @@ def run_ours(args, rank, world, local_rank):
              f"{production['poisson_solve']['lu_ms']:.2f} ms LU, {production['poisson_solve']['mg_cold_ms']:.2f} ms "
              f"MG-PCG cold, {production['poisson_solve']['mg_warm_ms']:.2f} ms warm")
 
+    batch = None
+    if rank == 0 and world == 1 and not args.no_batch:
+        batch = batched_scan()
+        _log(f"batched scan: {batch['runs']} runs, {batch['ms_per_batch_step']:.1f} ms per batch step at width "
+             f"{batch['branch_width']} ({batch['run_steps_per_s']:.0f} run-steps/s), setup {batch['setup_s']:.0f} s")
+
     if rank == 0:
         line = {"metric": METRIC, "value": n * world / (ms_step * 1e-3), "unit": METRIC, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
@@ -552,6 +598,8 @@ def run_ours(args, rank, world, local_rank):
             line["bunch_passage"] = passage
         if production is not None:
             line["production_passage"] = production
+        if batch is not None:
+            line["batched_scan"] = batch
         print(json.dumps(line), flush=True)
 
 
@@ -571,6 +619,7 @@ def main():
     ap.add_argument("--no-passage", action="store_true", help="skip the buildup bunch-passage timing")
     ap.add_argument("--no-production", action="store_true",
                     help="skip the 1024x1024 production passage sample and solve comparison")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 64-run batched scan")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world = int(os.environ.get("WORLD_SIZE", "1"))

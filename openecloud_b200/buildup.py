@@ -55,14 +55,18 @@ class Buildup:
     bounds the device particle store (the run reports a capacity drop in the
     status block instead of writing past it).  `poisson` reuses a
     PoissonSolver built for the same grid (its factorisation is the costly
-    part of the setup on large grids)."""
+    part of the setup on large grids; `PoissonSolver.sibling()` gives another
+    run its own state over the same factors) and `grid` a Grid of the same
+    parameters (read-only geometry, shareable between runs)."""
 
     def __init__(self, nx=128, ny=128, lx=0.04, ly=0.04, boundType=1, n_init=10000, w_init=None, dt=1e-11,
                  beam="endless", beam_particles=1.1e11, radius_sigma=0.002, bunch_length_sigma=0.25e-9 * 299792458.0,
                  material="copper", sey_max=1.6, e_hat0=300.0, type_b_field=0, b_const=(0., 0., 0.),
                  target=100000, management="global", management_every=50, capacity=None, seed=0,
-                 n_steps_table=2500, sort_every=0, boundFunc=None, poisson=None):
-        self.grid = Grid(nx, ny, lx, ly, boundType, boundFunc=boundFunc)
+                 n_steps_table=2500, sort_every=0, boundFunc=None, poisson=None, grid=None):
+        if grid is not None and (grid.nx, grid.ny, grid.lx, grid.ly, grid.boundType) != (nx, ny, lx, ly, boundType):
+            raise ValueError("grid: another grid than nx, ny, lx, ly, boundType describe")
+        self.grid = grid if grid is not None else Grid(nx, ny, lx, ly, boundType, boundFunc=boundFunc)
         self.dt = float(dt)
         self.target = int(target)
         self.management = management

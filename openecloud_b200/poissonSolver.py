@@ -16,6 +16,7 @@ around an f32 flexible PCG on the matrix-free 5-point operator, warm-started
 from the previous phi, Jacobi or learned preconditioner); the LU solve stays
 the fallback whenever the f64 relative residual misses ``pcgTol``.
 """
+import copy
 import ctypes
 
 import numpy as np
@@ -126,7 +127,7 @@ def mg_factors(ex, ey, inside, nx, ny, ratio=2.0):
     return 2, 2
 
 
-def mg_hierarchy(ex, ey, inside, nx, ny, bottom=100, semi=True):
+def mg_hierarchy(ex, ey, inside, nx, ny, bottom=100, semi=True, block_top=None):
     """Levels (ex, ey, leak, inside, nx, ny) of the aggregation multigrid,
     finest first, coarsened until a level has at most `bottom` nodes, and the
     block level: the first level of at most MG_BLOCK_TOP nodes from which all
@@ -140,7 +141,8 @@ def mg_hierarchy(ex, ey, inside, nx, ny, bottom=100, semi=True):
         lv.append(cur[:2] + (cur[2] + cur[3],) + cur[4:])
     sizes = [l[4] * l[5] for l in lv]
     block = len(lv) - 1
-    while block > 0 and len(lv) - (block - 1) <= 8 and sizes[block - 1] <= MG_BLOCK_TOP and \
+    top = MG_BLOCK_TOP if block_top is None else block_top
+    while block > 0 and len(lv) - (block - 1) <= 8 and sizes[block - 1] <= top and \
             4 * MG_FLOATS_PER_NODE * sum(sizes[block - 1:]) <= MG_BLOCK_SMEM:
         block -= 1
     return lv, block
@@ -320,17 +322,21 @@ class PoissonSolver:
         self._stencil = st
         self._pcg_work = D.empty(int(_declare().oec_pcg_work_bytes(st.nx, st.ny)), torch.uint8)
 
-    def _mg_setup(self, omega=0.8, scale=1.0, bottom=100):
+    def _mg_setup(self, omega=0.8, scale=1.0, bottom=100, block_top=None):
         """Aggregation multigrid hierarchy (oec_mg_t) on the scaled f32
         operator, down to at most `bottom` nodes, whose inside block is
-        inverted densely (f64 on the host, stored in f32).  The host copy of
-        every level (ex, ey, leak, inside, nx, ny) is kept under "host"."""
+        inverted densely (f64 on the host, stored in f32); levels of at most
+        `block_top` nodes (default MG_BLOCK_TOP) go to the one-CTA solve.  The
+        operators are shared with sibling solvers; the work vectors are this
+        solver's.  The host copy of every level (ex, ey, leak, inside, nx, ny)
+        is kept under "host"."""
         st = self._stencil
         k = self._keep
         ex = D.to_numpy(k["ex32"]).astype(np.float64)
         ey = D.to_numpy(k["ey32"]).astype(np.float64)
         inside = D.to_numpy(k["inside"]).astype(bool)
-        lv, block = mg_hierarchy(ex, ey, inside, st.nx, st.ny, bottom)
+        lv, block = mg_hierarchy(ex, ey, inside, st.nx, st.ny, bottom,
+                                 block_top=MG_BLOCK_TOP if block_top is None else block_top)
         e, f, lk, ins, X, Y = lv[-1]
         idx = np.nonzero(ins)[0]
         M = np.empty((idx.size, idx.size))
@@ -338,8 +344,7 @@ class PoissonSolver:
             v = np.zeros(X * Y)
             v[idx[c]] = 1.0
             M[:, c] = mg_apply_host(e, f, lk, ins, X, v)[idx]
-        keep = []
-        levels = (MgLevel_t * len(lv))()
+        ops = []
         for n_, (e, f, lk, ins, X, Y) in enumerate(lv):
             i = np.nonzero(ins)[0]
             col = i % X
@@ -349,22 +354,54 @@ class PoissonSolver:
                 raise ValueError("multigrid level with a non-positive diagonal")
             dinv = np.zeros(X * Y)
             dinv[i] = 1.0 / d
-            t = {"ex": D.to_device(e, torch.float32), "ey": D.to_device(f, torch.float32),
+            t = {"nx": X, "ny": Y, "ex": D.to_device(e, torch.float32), "ey": D.to_device(f, torch.float32),
                  "leak": D.to_device(lk, torch.float32), "dinv": D.to_device(dinv, torch.float32),
-                 "inside": D.to_device(ins.astype(np.uint8), torch.uint8),
-                 "b": D.zeros(X * Y, torch.float32), "x": D.zeros(X * Y, torch.float32),
-                 "y": D.zeros(X * Y, torch.float32)}
+                 "inside": D.to_device(ins.astype(np.uint8), torch.uint8)}
             if n_ == 0:  # the solver's own f32 operator and diagonal
                 t["ex"], t["ey"], t["dinv"] = k["ex32"], k["ey32"], k["dinv32"]
-            keep.append(t)
-            levels[n_] = MgLevel_t(X, Y, *(D.ptr(t[name]) for name in ("ex", "ey", "leak", "dinv", "inside", "b",
-                                                                       "x", "y")))
-        cidx = D.to_device(idx.astype(np.int32), torch.int32)
-        cinv = D.to_device(np.linalg.inv(M).astype(np.float32), torch.float32)
-        mg = Mg_t(len(lv), levels, block, idx.size, D.ptr(cidx), D.ptr(cinv), omega, scale)
-        self._mg = {"c": mg, "levels": levels, "keep": keep, "cidx": cidx, "cinv": cinv, "nlevels": len(lv),
-                    "block_level": block, "host": lv}
+            ops.append(t)
+        shared = {"ops": ops, "cidx": D.to_device(idx.astype(np.int32), torch.int32),
+                  "cinv": D.to_device(np.linalg.inv(M).astype(np.float32), torch.float32),
+                  "block_level": block, "omega": omega, "scale": scale, "host": lv}
+        self._mg = self._mg_state(shared)
         return self._mg
+
+    @staticmethod
+    def _mg_state(shared):
+        """This solver's multigrid work vectors and the oec_mg_t over them."""
+        ops = shared["ops"]
+        work = [{name: D.zeros(o["nx"] * o["ny"], torch.float32) for name in ("b", "x", "y")} for o in ops]
+        levels = (MgLevel_t * len(ops))()
+        for n_, (o, w) in enumerate(zip(ops, work)):
+            levels[n_] = MgLevel_t(o["nx"], o["ny"], D.ptr(o["ex"]), D.ptr(o["ey"]), D.ptr(o["leak"]),
+                                   D.ptr(o["dinv"]), D.ptr(o["inside"]), D.ptr(w["b"]), D.ptr(w["x"]),
+                                   D.ptr(w["y"]))
+        mg = Mg_t(len(ops), levels, shared["block_level"], shared["cidx"].shape[0], D.ptr(shared["cidx"]),
+                  D.ptr(shared["cinv"]), shared["omega"], shared["scale"])
+        keep = [dict(o, **w) for o, w in zip(ops, work)]
+        return {"c": mg, "levels": levels, "work": work, "shared": shared, "keep": keep, "nlevels": len(ops),
+                "block_level": shared["block_level"], "host": shared["host"]}
+
+    def sibling(self):
+        """A solver for another run on the same grid: shares the
+        factorisation, the stencil, the field operator and the multigrid
+        operators, and owns its phi, E, work areas and statistics, so
+        siblings may solve at the same time (on different streams, or on the
+        branches of one graph).  A trained network is not shared (its
+        workspace is per network)."""
+        s = copy.copy(self)
+        npn = self.n_nodes
+        s.phi = D.zeros(npn, torch.float64)
+        s.eAtGridPoints = D.zeros(2 * npn, torch.float64)
+        s._work = torch.zeros_like(self._work)
+        s._pcg_work = torch.empty_like(self._pcg_work)
+        s._stats_dev = torch.zeros_like(self._stats_dev)
+        s._fb_count = torch.zeros_like(self._fb_count)
+        s._pcg_used = False
+        s.nSolves = 0
+        s.cnn = None
+        s._mg = None if self._mg is None else PoissonSolver._mg_state(self._mg["shared"])
+        return s
 
     def applyOperator(self, x):
         """A x on the inside nodes (device f64 [npExt] in and out)."""
