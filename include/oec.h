@@ -245,6 +245,40 @@ typedef struct oec_furman {
     int32_t reserved;
 } oec_furman_t;
 
+/* Parameters of the simplified emitters: model 0 = SecElecEmitter with the
+ * stainless parameters of stainlessMod (particleEmitter.pyx:316-352, seyMax
+ * and reflec applied), model 1 = SimpleSecEmitter (:489-597, fixed yields,
+ * electron mass; the other fields unused).  max_ts (1..10) caps the number
+ * of true secondaries of one absorbed particle (the reference has no cap;
+ * a capped particle is counted in status->warn_tsprime). */
+typedef struct oec_secelec {
+    int32_t model, max_ts;
+    double p1EInf, p1Ehat, eEHat, w, p, e1, e2, p1RInf, eR, r, r1, r2;
+    double deltaTSHat, s, eHat0, t1, t2, t3, t4, sigmaETS, muETS, theta0max, deltaERmax, q;
+    double particle_mass;
+} oec_secelec_t;
+
+/* Bytes of `work_dev` oec_secelec_emit needs for `cap` absorbed rows
+ * (cap <= 2^26; -1 beyond). */
+int64_t oec_secelec_work_bytes(int32_t cap);
+
+/* SecElecEmitter / SimpleSecEmitter.generateSecondaries
+ * (particleEmitter.pyx:355-484, :506-597): per absorbed row an elastic
+ * secondary (reversed velocity) with probability delta_E, a rediffused one
+ * (velocity scaled by rand^(1/(2(1+q))), simple: sqrt(rand)) with
+ * probability delta_R, and floor(delta_TS) (+1 with probability of the
+ * fraction) true secondaries: lognormal energies (a uniform split of E0 when
+ * they sum above E0) emitted about the wall normal by theta = asin(rand),
+ * phi = 2 pi rand (simple: uniform 0-5 eV along the reversed velocity).
+ * Output order and arguments as oec_furman_emit; replay_uniforms_dev, if
+ * given, holds 64 uniforms per absorbed row consumed in the reference's
+ * order (a normal deviate = Box-Muller of two). */
+int oec_secelec_emit(const oec_secelec_t *params, const double *rows_dev, const double *normals_dev,
+                     const int32_t *n_abs_dev, int32_t cap, const int32_t *ids_dev, uint64_t seed, uint32_t step,
+                     const int32_t *step_dev, const double *replay_uniforms_dev, void *work_dev,
+                     double *out_rows_dev, int32_t out_cap, int32_t *n_out_dev, oec_status_t *status_dev,
+                     void *stream);
+
 /* Bytes of `work_dev` oec_furman_emit needs for `cap` absorbed rows
  * (cap <= 2^26; -1 beyond). */
 int64_t oec_furman_work_bytes(int32_t cap);
@@ -581,6 +615,22 @@ int oec_point_in_polygon(const double *poly, int32_t n, double x, double y);
 
 /* prepareBoundFuncPoints (grid.pyx:123-159): drop collinear vertices. */
 int oec_polygon_prepare(const double *pts, int32_t n, double *out, int32_t *n_out);
+
+/* ---------------------------------------------------------- fields, diagnostics */
+
+/* multipoleExpansion (magneticField.pyx:23-59): B = [Bx | By | Bz=0] f64
+ * [3*nx*ny] on the extended grid nodes (xmesh_dev [nx], ymesh_dev [ny]: the
+ * node coordinates, Grid.getXMesh/getYMesh) from normal[n_normal] and
+ * skew[n_skew] coefficients in T/m^k (host arrays, order <= 32; a shorter skew
+ * list is padded with zeros, a longer one cut to n_normal). */
+int oec_multipole_field(int32_t nx, int32_t ny, const double *xmesh_dev, const double *ymesh_dev,
+                        const double *normal, int32_t n_normal, const double *skew, int32_t n_skew, double *b_dev,
+                        void *stream);
+
+/* averageEnergy (util.pyx:8-20): sums_dev[0] = sum |v|^2 w, sums_dev[1] =
+ * sum w over the store (f64); the mean energy in eV is
+ * m / (2 e) * sums[0] / sums[1]. */
+int oec_average_energy_sums(const oec_particles_t *p, double *sums_dev, void *stream);
 
 #ifdef __cplusplus
 }

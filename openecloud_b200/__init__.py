@@ -7,6 +7,7 @@ declared in include/oec.h; torch provides device memory and streams.
 """
 from . import _lib, constants, grid_geom  # noqa: F401
 from . import grid, particles, particleBoundary, particleEmitter, particleManagement, poissonSolver  # noqa: F401
-from . import beam, buildup, cnn  # noqa: F401
+from . import beam, buildup, cnn, magneticField, util, autotune, batch  # noqa: F401
 
-__all__ = ["constants", "grid", "particles", "particleBoundary", "particleEmitter", "poissonSolver", "grid_geom"]
+__all__ = ["constants", "grid", "particles", "particleBoundary", "particleEmitter", "poissonSolver", "grid_geom",
+           "magneticField", "util", "beam", "buildup", "batch", "autotune"]

@@ -31,7 +31,6 @@ secondaries, extras appended, tail compaction) and does not sort by default.
 Periodic cell sorting (`sort_every`) helps the deposit's warp aggregation but
 is only order-neutral with the emitter's `compat` switch off.
 """
-import ctypes
 import time
 
 import numpy as np
@@ -42,7 +41,7 @@ from . import device as D
 from .beam import LHCBeam, LHCBeamEndless
 from .grid import Grid
 from .particleBoundary import AbsorbElliptical, AbsorbRectangular, AbsorbArbitraryCutCell
-from .particleEmitter import FurmanEmitter, homoLoader, _declare as _emit_declare
+from .particleEmitter import FurmanEmitter, SecElecEmitter, SimpleSecEmitter, homoLoader
 from .particleManagement import globalRandom, localRandom
 from .particles import Particles
 from .poissonSolver import PoissonSolver, _declare as _poisson_declare
@@ -53,7 +52,13 @@ class Buildup:
 
     Parameters mirror the configuration of example01_basic.py; `capacity`
     bounds the device particle store (the run reports a capacity drop in the
-    status block instead of writing past it).  `poisson` reuses a
+    status block instead of writing past it).  `b_multipoles` / `b_skew`
+    (T/m^n) replace the constant field by the multipole field of
+    magneticField.multipoleExpansion, gathered per particle (typeBField 2).
+    `emitter` picks the secondary-emission model: 'furman' (FurmanEmitter,
+    `material`, `sey_max`, `e_hat0`), 'secelec' (SecElecEmitter, stainless,
+    `sey_max`) or 'simple' (SimpleSecEmitter).
+    `poisson` reuses a
     PoissonSolver built for the same grid (its factorisation is the costly
     part of the setup on large grids; `PoissonSolver.sibling()` gives another
     run its own state over the same factors) and `grid` a Grid of the same
@@ -63,7 +68,8 @@ class Buildup:
                  beam="endless", beam_particles=1.1e11, radius_sigma=0.002, bunch_length_sigma=0.25e-9 * 299792458.0,
                  material="copper", sey_max=1.6, e_hat0=300.0, type_b_field=0, b_const=(0., 0., 0.),
                  target=100000, management="global", management_every=50, capacity=None, seed=0,
-                 n_steps_table=2500, sort_every=0, boundFunc=None, poisson=None, grid=None):
+                 n_steps_table=2500, sort_every=0, boundFunc=None, poisson=None, grid=None, b_multipoles=None,
+                 b_skew=(), emitter="furman"):
         if grid is not None and (grid.nx, grid.ny, grid.lx, grid.ly, grid.boundType) != (nx, ny, lx, ly, boundType):
             raise ValueError("grid: another grid than nx, ny, lx, ly, boundType describe")
         self.grid = grid if grid is not None else Grid(nx, ny, lx, ly, boundType, boundFunc=boundFunc)
@@ -85,9 +91,16 @@ class Buildup:
             self.bd = AbsorbArbitraryCutCell(self.grid, self.P)
         w_init = w_init if w_init is not None else 1e9 / n_init
         homoLoader(self.grid, self.P, self.bd, n_init, w_init, seed=seed)
-        self.em = FurmanEmitter(self.bd, self.P, material=material, seyMax=sey_max, seed=seed + 17)
-        if e_hat0 is not None:
-            self.em.setEHat0(e_hat0)
+        if emitter == "furman":
+            self.em = FurmanEmitter(self.bd, self.P, material=material, seyMax=sey_max, seed=seed + 17)
+            if e_hat0 is not None:
+                self.em.setEHat0(e_hat0)
+        elif emitter == "secelec":
+            self.em = SecElecEmitter(self.bd, self.P, seyMax=sey_max, seed=seed + 17)
+        elif emitter == "simple":
+            self.em = SimpleSecEmitter(self.bd, self.P, seed=seed + 17)
+        else:
+            raise ValueError("emitter must be 'furman', 'secelec' or 'simple'")
         if poisson is not None and (poisson.gridObj.getNxExt(), poisson.gridObj.getNyExt()) != \
                 (self.grid.getNxExt(), self.grid.getNyExt()):
             raise ValueError("poisson: a solver for another grid")
@@ -103,6 +116,13 @@ class Buildup:
         self.rho = D.zeros(G, torch.float64)
         self.etab = D.zeros(8 * G, torch.float32)
         self.btab = None
+        if b_multipoles is not None:
+            # multipole field on the nodes (example04_multipole.py:45), gathered
+            # per particle in the fused kernel (typeBField 2)
+            from .magneticField import multipoleExpansionDevice
+            b = multipoleExpansionDevice(self.grid, b_multipoles, b_skew)
+            self.btab = self.P.fieldTable(self.grid, b, 3)
+            self.type_b = 2
         self.hist_w = D.zeros(self._table_len, torch.float64)
         self.hist_n = D.zeros(self._table_len, torch.int32)
         self.scratch = D.zeros(256, torch.float64)  # oec_history's partial sums
@@ -150,13 +170,7 @@ class Buildup:
                   s)
         _lib.call("oec_wall_interaction", cg, cb, self.dt, bd._rows.data_ptr(), bd._n_abs.data_ptr(), cap,
                   bd._normals.data_ptr(), P._status.data_ptr(), s)
-        rc = _emit_declare().oec_furman_emit(ctypes.byref(em.c_params()), bd._rows.data_ptr(),
-                                             bd._normals.data_ptr(), bd._n_abs.data_ptr(), cap, bd._index.data_ptr(),
-                                             em.seed, 0, self.step_dev.data_ptr(), None, em._work.data_ptr(),
-                                             em._out.data_ptr(),
-                                             em._out.shape[0], em._n_out.data_ptr(), P._status.data_ptr(), s)
-        if rc:
-            raise _lib.OecError("oec_furman_emit", rc)
+        em._launch(cap, 0, self.step_dev, None)
         _lib.call("oec_add_remove", cg, cp, P._mask.data_ptr(), bd._index.data_ptr(), bd._n_abs.data_ptr(),
                   bd._index.shape[0], em._out.data_ptr(), em._n_out.data_ptr(), em._out.shape[0],
                   P._rho_fix.data_ptr(), P._wscale.data_ptr(), P._scan_scratch.data_ptr(), P._status.data_ptr(), s)

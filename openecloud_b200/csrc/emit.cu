@@ -290,6 +290,147 @@ __global__ void k_scan_add(int32_t *out, const int32_t *n_p, int cap, const int 
     if (i < n) out[i] += partial[blockIdx.x];
 }
 
+// ------------------------------------------- simplified emitters
+// SecElecEmitter (particleEmitter.pyx:355-484) and SimpleSecEmitter
+// (:506-597): pass 1 draws the elastic / rediffused / true counts (draws
+// 0, 1, 2), the scan places each row's secondaries, pass 2 writes them
+// (draws from 3 on, in the reference's order).
+constexpr int kSecDraws = 64;  // replay stride: uniforms per absorbed row
+
+struct SRec {
+    double e0;
+    int nE, nR, nT, pad;
+};
+
+__global__ void k_secelec_pass1(oec_secelec_t f, const double *__restrict__ rows, const double *__restrict__ normals,
+                                const int32_t *n_abs, int cap, const int32_t *__restrict__ ids, uint2 key,
+                                uint32_t step, const int32_t *step_dev, const double *__restrict__ replay,
+                                SRec *__restrict__ rec, int32_t *__restrict__ nsec, oec_status_t *status) {
+    const int na = min(*n_abs, cap);
+    const double mass = f.model == 1 ? 9.10938291e-31 : f.particle_mass;
+    const double eF = 0.5 * mass / 1.602176565e-19;
+    int capped = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += gridDim.x * blockDim.x) {
+        const double *r = rows + 6 * (int64_t)i;
+        const double v0 = sqrt(r[2] * r[2] + r[3] * r[3] + r[4] * r[4]);
+        const double e0 = eF * v0 * v0;
+        double dE, dR, dTS;
+        if (f.model == 1) {
+            const double s = 1.813, eHat = 310;
+            dE = 0.05;
+            dR = 0.5;
+            dTS = 1.4 * s * e0 / eHat / (s - 1 + pow(e0 / eHat, s));
+        } else {
+            double th = acos((r[2] * normals[2 * i] + r[3] * normals[2 * i + 1]) / v0);
+            if (th > 0.5 * sf::kPi) th = sf::kPi - th;
+            th = clip(th, 0., f.theta0max);
+            const double ct = cos(th);
+            dE = (f.p1EInf + (f.p1Ehat - f.p1EInf) * exp(-pow(fabs(e0 - f.eEHat) / f.w, f.p) / f.p)) *
+                 (1 + f.e1 * (1 - pow(ct, f.e2)));
+            dR = f.p1RInf * (1 - exp(-pow(e0 / f.eR, f.r))) * (1 + f.r1 * (1 - pow(ct, f.r2)));
+            const double eHat = f.eHat0 * (1 + f.t3 * (1 - pow(ct, f.t4)));
+            dTS = f.deltaTSHat * f.s * e0 / eHat / (f.s - 1 + pow(e0 / eHat, f.s)) * (1 + f.t1 * (1 - pow(ct, f.t2)));
+            const double t = dE + dR;
+            if (t >= f.deltaERmax) {
+                dE = dE / t * f.deltaERmax;
+                dR = dR / t * f.deltaERmax;
+            }
+        }
+        sf::Draws dr{key, ids ? (uint32_t)ids[i] : (uint32_t)i, step + (step_dev ? (uint32_t)*step_dev : 0u),
+                     replay ? replay + (int64_t)i * kSecDraws : nullptr};
+        const int nE = dr.next() <= dE ? 1 : 0;
+        const int nR = dr.next() <= dR ? 1 : 0;
+        // <unsigned int> truncation of the reference (:391, :553), then +1
+        // with the probability of the fraction; a huge yield is capped below
+        int nT = dTS >= 1e9 ? 1000000000 : (dTS > 0.0 ? (int)dTS : 0);
+        if (dr.next() <= dTS - nT) ++nT;
+        if (nT > f.max_ts) {
+            nT = f.max_ts;
+            ++capped;
+        }
+        rec[i] = SRec{e0, nE, nR, nT, 0};
+        nsec[i] = nE + nR + nT;
+    }
+    if (capped) atomicAdd(&status->warn_tsprime, capped);
+}
+
+__device__ __forceinline__ void put_row(double *q, const double *r, double vx, double vy, double vz) {
+    q[0] = r[0];
+    q[1] = r[1];
+    q[2] = vx;
+    q[3] = vy;
+    q[4] = vz;
+    q[5] = r[5];
+}
+
+__global__ void k_secelec_pass2(oec_secelec_t f, const double *__restrict__ rows, const double *__restrict__ normals,
+                                const int32_t *n_abs, int cap, const int32_t *__restrict__ ids, uint2 key,
+                                uint32_t step, const int32_t *step_dev, const double *__restrict__ replay,
+                                const SRec *__restrict__ rec, const int32_t *__restrict__ offset,
+                                double *__restrict__ out, int out_cap, oec_status_t *status) {
+    const int na = min(*n_abs, cap);
+    const double mass = f.model == 1 ? 9.10938291e-31 : f.particle_mass;
+    const double eFi = 1.0 / (0.5 * mass / 1.602176565e-19);
+    int dropped = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += gridDim.x * blockDim.x) {
+        const SRec R = rec[i];
+        if (R.nE + R.nR + R.nT == 0) continue;
+        const double *r = rows + 6 * (int64_t)i;
+        sf::Draws dr{key, ids ? (uint32_t)ids[i] : (uint32_t)i, step + (step_dev ? (uint32_t)*step_dev : 0u),
+                     replay ? replay + (int64_t)i * kSecDraws : nullptr};
+        dr.d = 3;  // draws 0..2 were the counts
+        int o = offset[i];
+        auto slot = [&](void) -> double * {
+            if (o >= out_cap) {
+                ++dropped;
+                ++o;
+                return nullptr;
+            }
+            return out + 6 * (int64_t)(o++);
+        };
+        if (R.nE) {
+            if (double *q = slot()) put_row(q, r, -r[2], -r[3], -r[4]);
+        }
+        if (R.nR) {
+            const double u = dr.next();
+            const double vF = f.model == 1 ? sqrt(u) : sqrt(pow(u, 1. / (1. + f.q)));
+            if (double *q = slot()) put_row(q, r, -r[2] * vF, -r[3] * vF, -r[4] * vF);
+        }
+        const int n = R.nT;
+        if (n <= 0) continue;
+        double eSec[10];
+        if (f.model == 1) {
+            for (int k = 0; k < n; ++k) eSec[k] = dr.next() * 5;
+            for (int k = 0; k < n; ++k) {
+                const double vF = sqrt(eSec[k] / R.e0);
+                if (double *q = slot()) put_row(q, r, -r[2] * vF, -r[3] * vF, -r[4] * vF);
+            }
+            continue;
+        }
+        double eSum = 0.;
+        for (int k = 0; k < n; ++k) {
+            eSec[k] = exp(f.sigmaETS * dr.normal() + f.muETS);
+            eSum += eSec[k];
+        }
+        if (eSum > R.e0)
+            for (int k = 0; k < n; ++k) eSec[k] = dr.next() * R.e0 / n;
+        const double n0 = normals[2 * i], n1 = normals[2 * i + 1];
+        for (int k = 0; k < n; ++k) {
+            const double vs = sqrt(eFi * eSec[k]);
+            const double thS = asin(dr.next());
+            const double cT = cos(thS), sT = sin(thS);
+            const double phS = dr.next() * sf::kPi * 2.;
+            const double cP = cos(phS), sP = sin(phS);
+            const double t1 = cT * n0 - sT * n1, t2 = sT * n0 + cT * n1;
+            if (double *q = slot())
+                put_row(q, r, vs * ((cP + n0 * n0 * (1 - cP)) * t1 + n0 * n1 * (1 - cP) * t2),
+                        vs * ((cP + n1 * n1 * (1 - cP)) * t2 + n0 * n1 * (1 - cP) * t1),
+                        vs * (-sP * n1 * t1 + sP * n0 * t2));
+        }
+    }
+    if (dropped) atomicAdd(&status->n_capacity_drop, dropped);
+}
+
 // ---------------------------------------------------------- homoLoader
 
 // Rejection sampling of uniform positions inside the boundary
@@ -378,6 +519,46 @@ extern "C" int oec_furman_emit(const oec_furman_t *params, const double *rows_de
                                      replay_uniforms_dev, rec, split, off, out_rows_dev, out_cap, status_dev);
     OEC_LAUNCH_CHECK();
     return OEC_OK;
+}
+
+extern "C" int oec_secelec_emit(const oec_secelec_t *params, const double *rows_dev, const double *normals_dev,
+                                const int32_t *n_abs_dev, int32_t cap, const int32_t *ids_dev, uint64_t seed,
+                                uint32_t step, const int32_t *step_dev, const double *replay_uniforms_dev,
+                                void *work_dev, double *out_rows_dev, int32_t out_cap, int32_t *n_out_dev,
+                                oec_status_t *status_dev, void *stream) {
+    if (!params || !rows_dev || !normals_dev || !n_abs_dev || !work_dev || !out_rows_dev || !n_out_dev ||
+        !status_dev || cap < 0 || out_cap < 0 || params->model < 0 || params->model > 1 || params->max_ts < 1 ||
+        params->max_ts > 10 || cap > kMaxAbsorbedRows)
+        return OEC_ERR_INVALID;
+    const int nblocks = (cap + kScanT - 1) / kScanT;
+    cudaStream_t s = as_stream(stream);
+    // work layout: SRec[cap] | nsec[cap] | offset[cap] | partial[scan_blocks(cap)]
+    char *w = static_cast<char *>(work_dev);
+    SRec *rec = reinterpret_cast<SRec *>(w);
+    int32_t *nsec = reinterpret_cast<int32_t *>(w + sizeof(SRec) * (size_t)cap);
+    int32_t *off = nsec + cap;
+    int *partial = off + cap;
+    const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+    const int g = persistent_grid((cap + 127) / 128, 8);
+    k_secelec_pass1<<<g, 128, 0, s>>>(*params, rows_dev, normals_dev, n_abs_dev, cap, ids_dev, key, step, step_dev,
+                                      replay_uniforms_dev, rec, nsec, status_dev);
+    if (cap > 0) {
+        k_scan_blocks<<<nblocks, kScanT, 0, s>>>(nsec, n_abs_dev, cap, off, partial);
+        k_scan_partials<<<1, kScanT, 0, s>>>(partial, nblocks, n_out_dev);
+        k_scan_add<<<nblocks, kScanT, 0, s>>>(off, n_abs_dev, cap, partial);
+    } else {
+        OEC_CUDA_TRY(cudaMemsetAsync(n_out_dev, 0, sizeof(int32_t), s));
+    }
+    k_secelec_pass2<<<g, 128, 0, s>>>(*params, rows_dev, normals_dev, n_abs_dev, cap, ids_dev, key, step, step_dev,
+                                      replay_uniforms_dev, rec, off, out_rows_dev, out_cap, status_dev);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int64_t oec_secelec_work_bytes(int32_t cap) {
+    if (cap < 0 || cap > kMaxAbsorbedRows) return -1;
+    return (int64_t)sizeof(SRec) * cap + 2 * sizeof(int32_t) * (int64_t)cap + sizeof(int) * (int64_t)scan_blocks(cap) +
+           256;
 }
 
 extern "C" int64_t oec_furman_work_bytes(int32_t cap) {

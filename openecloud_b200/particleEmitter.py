@@ -42,7 +42,7 @@ COPPER = dict(p1EInf=0.02, p1Ehat=0.496, eEHat=0., w=60.86, p=1., e1=0.26, e2=2.
               epsN=[2.5, 3.3, 2.5, 2.5, 2.8, 1.3, 1.5, 1.5, 1.5, 1.5],
               pSmallN=[1.5, 1.75, 1., 3.75, 8.5, 11.5, 2.5, 3., 2.5, 3.])
 
-_lib.OTHER_DECLARED.update({"oec_furman_emit", "oec_furman_work_bytes"})
+_lib.OTHER_DECLARED.update({"oec_furman_emit", "oec_furman_work_bytes", "oec_secelec_emit", "oec_secelec_work_bytes"})
 
 
 def _declare():
@@ -54,6 +54,11 @@ def _declare():
                                       ctypes.c_uint32, P, P, P, P, ctypes.c_int32, P, P, P]
         L.oec_furman_work_bytes.restype = ctypes.c_int64
         L.oec_furman_work_bytes.argtypes = [ctypes.c_int32]
+        L.oec_secelec_emit.restype = ctypes.c_int
+        L.oec_secelec_emit.argtypes = [ctypes.POINTER(SecElec_t), P, P, P, ctypes.c_int32, P, ctypes.c_uint64,
+                                       ctypes.c_uint32, P, P, P, P, ctypes.c_int32, P, P, P]
+        L.oec_secelec_work_bytes.restype = ctypes.c_int64
+        L.oec_secelec_work_bytes.argtypes = [ctypes.c_int32]
         L._emit_declared = True
     return L
 
@@ -119,6 +124,21 @@ class FurmanEmitter:
             self._out = D.zeros((self.m * self._cap_abs + 1, 6), torch.float64)
             self._n_out = D.zeros(1, torch.int32)
 
+    def _launch(self, cap, step, step_dev, replay):
+        """One emission over the boundary's first min(n_abs, cap) rows into
+        this emitter's buffers (the step counter added to `step` when given
+        on the device); no host synchronisation."""
+        bd = self.particleBoundaryObj
+        ids = bd._index.data_ptr() if bd._index is not None else None
+        rc = _declare().oec_furman_emit(ctypes.byref(self.c_params()), bd._rows.data_ptr(), bd._normals.data_ptr(),
+                                        bd._n_abs.data_ptr(), cap, ids, self.seed, step & 0xffffffff,
+                                        step_dev.data_ptr() if step_dev is not None else None,
+                                        replay.data_ptr() if replay is not None else None, self._work.data_ptr(),
+                                        self._out.data_ptr(), self._out.shape[0], self._n_out.data_ptr(),
+                                        self.particlesObj._status.data_ptr(), D.stream())
+        if rc:
+            raise _lib.OecError("oec_furman_emit", rc)
+
     def emitDevice(self, replay=None, step=None):
         """Launch the emission for the boundary's absorbed rows; returns the
         device rows buffer and the device count (no host synchronisation)."""
@@ -126,16 +146,8 @@ class FurmanEmitter:
         bd._wall()
         cap = bd._rows.shape[0]
         self.ensure_buffers(cap)
-        P = self.particlesObj
         step = self.step if step is None else int(step)
-        ids = bd._index.data_ptr() if bd._index is not None else None
-        rc = _declare().oec_furman_emit(ctypes.byref(self.c_params()), bd._rows.data_ptr(), bd._normals.data_ptr(),
-                                        bd._n_abs.data_ptr(), cap, ids, self.seed, step & 0xffffffff, None,
-                                        replay.data_ptr() if replay is not None else None, self._work.data_ptr(),
-                                        self._out.data_ptr(), self._out.shape[0], self._n_out.data_ptr(),
-                                        P._status.data_ptr(), D.stream())
-        if rc:
-            raise _lib.OecError("oec_furman_emit", rc)
+        self._launch(cap, step, None, replay)
         self.step += 1
         return self._out, self._n_out
 
@@ -147,6 +159,107 @@ class FurmanEmitter:
 
     def getEmittedParticles(self):
         return D.to_numpy(self._out[:self.secondaryCount])
+
+
+class SecElec_t(ctypes.Structure):
+    _fields_ = [("model", ctypes.c_int32), ("max_ts", ctypes.c_int32)] + \
+        [(k, ctypes.c_double) for k in ("p1EInf", "p1Ehat", "eEHat", "w", "p", "e1", "e2", "p1RInf", "eR", "r", "r1",
+                                        "r2", "deltaTSHat", "s", "eHat0", "t1", "t2", "t3", "t4", "sigmaETS",
+                                        "muETS", "theta0max", "deltaERmax", "q", "particle_mass")]
+
+
+# SecElecEmitter.stainlessMod (particleEmitter.pyx:331-352)
+STAINLESS_SECELEC = dict(p1EInf=0.07, p1Ehat=0.5, eEHat=0., w=100., p=0.9, e1=0.26, e2=2., q=0.4, p1RInf=0.74,
+                         eR=40., r=1., r1=0.26, r2=2., deltaTSHat=1.22, s=1.813, eHat0=310., t3=0.7, t4=1., t1=0.66,
+                         t2=0.8, sigmaETS=1.041, muETS=2.456)
+
+
+class SecElecEmitter:
+    """Reference: particleEmitter.pyx:316-484 -- a simplified Furman model
+    for stainless steel: an elastic and a rediffused secondary with
+    probabilities delta_E and delta_R and a Bernoulli-rounded number of true
+    secondaries with lognormal energies, on the device (`oec_secelec_emit`).
+    Draws come from per-row Philox streams keyed by `seed`, row and step;
+    true secondaries of one absorbed particle are capped at `maxTrue` (the
+    reference has no cap; capped rows count in the status block)."""
+
+    MODEL = 0
+
+    def __init__(self, particleBoundaryObj, particlesObj, seyMax=-1., reflec=-1., seed=0, maxTrue=10):
+        self.particlesObj = particlesObj
+        self.particleBoundaryObj = particleBoundaryObj
+        self.particleMass = particlesObj.getParticleMass()
+        self.seed = int(seed)
+        self.max_ts = int(maxTrue)
+        self.m = self.max_ts + 2  # rows per absorbed particle at most
+        self.step = 0
+        self._work = None
+        self._out = None
+        self._n_out = None
+        self.secondaryCount = 0
+        self.stainlessMod(seyMax, reflec)
+
+    def stainlessMod(self, seyMax, reflec):
+        """particleEmitter.pyx:331-352."""
+        t = dict(STAINLESS_SECELEC, theta0max=84. * pi / 180., deltaERmax=0.99)
+        if seyMax >= 0.5:
+            t["deltaTSHat"] = seyMax - t["p1RInf"] - t["p1EInf"]
+            if t["deltaTSHat"] < 0.:
+                t["deltaTSHat"] = 1.e-6
+                print("WARNING: Maximum SEY too small. Setting true SEY to zero.")
+        if reflec >= 0.:
+            t["p1Ehat"] = reflec
+        self.params = t
+
+    def c_params(self):
+        f = SecElec_t()
+        for k, v in self.params.items():
+            setattr(f, k, float(v))
+        f.model, f.max_ts = self.MODEL, self.max_ts
+        f.particle_mass = self.particleMass
+        return f
+
+    def ensure_buffers(self, cap_abs):
+        L = _declare()
+        if self._work is None or self._cap_abs < cap_abs:
+            self._cap_abs = int(cap_abs)
+            self._work = D.empty(int(L.oec_secelec_work_bytes(self._cap_abs)), torch.uint8)
+            self._out = D.zeros((self.m * self._cap_abs + 1, 6), torch.float64)
+            self._n_out = D.zeros(1, torch.int32)
+
+    def _launch(self, cap, step, step_dev, replay):
+        bd = self.particleBoundaryObj
+        ids = bd._index.data_ptr() if bd._index is not None else None
+        rc = _declare().oec_secelec_emit(ctypes.byref(self.c_params()), bd._rows.data_ptr(), bd._normals.data_ptr(),
+                                         bd._n_abs.data_ptr(), cap, ids, self.seed, step & 0xffffffff,
+                                         step_dev.data_ptr() if step_dev is not None else None,
+                                         replay.data_ptr() if replay is not None else None, self._work.data_ptr(),
+                                         self._out.data_ptr(), self._out.shape[0], self._n_out.data_ptr(),
+                                         self.particlesObj._status.data_ptr(), D.stream())
+        if rc:
+            raise _lib.OecError("oec_secelec_emit", rc)
+
+    emitDevice = FurmanEmitter.emitDevice
+
+    def generateSecondaries(self, replay=None):
+        """The secondaries as a (n, 6) device tensor (replay: injected
+        uniforms, 64 per absorbed row)."""
+        out, n = self.emitDevice(replay=replay)
+        self.secondaryCount = int(n.item())
+        return out[:self.secondaryCount]
+
+    def getEmittedParticles(self):
+        return D.to_numpy(self._out[:self.secondaryCount])
+
+
+class SimpleSecEmitter(SecElecEmitter):
+    """Reference: particleEmitter.pyx:489-597 ("currently only for
+    testing"): fixed yields delta_E = 0.05, delta_R = 0.5 and a stainless-like
+    true yield, secondaries along the reversed incident velocity (true ones
+    with a uniform 0-5 eV energy); seyMax and reflec are ignored, as in the
+    reference."""
+
+    MODEL = 1
 
 
 def homoLoader(gridObj, particlesObj, partBoundObj, macroParticleCount, weightInit, vsigma=10000. * doubleMinVal,

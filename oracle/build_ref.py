@@ -70,6 +70,9 @@ def prepare_sources(src):
     _patch(pe, "    def getEmittedParticles(self):\n        return self.secondaries",
            "    def getEmittedParticles(self):\n        return self.secondaries\n\n"
            "    def setEHat0(self, double value):\n        self.eHat0 = value\n")
+    # SecElecEmitter / SimpleSecEmitter size their output by a double
+    # (nSecSum), which numpy >= 1.12 rejects: cast it to an integer.
+    _patch(pe, "numpy.empty((nSecSum, nCoords)", "numpy.empty((<Py_ssize_t> nSecSum, nCoords)", count=2)
     # matplotlib stub (grid.pyx imports pyplot at module import time).
     mpl = os.path.join(OUT, "matplotlib")
     os.makedirs(mpl, exist_ok=True)

@@ -396,3 +396,131 @@ void orc_homo_loader(int kind, double lx, double ly, int64_t n, double w0, doubl
     }
     for (int64_t i = 0; i < n; ++i) pd[6 * i + 5] = randomize ? w0 * (0.5 + orc_rand()) : w0;
 }
+
+/* ------------------------------------------------------------------------
+ * SecElecEmitter (particleEmitter.pyx:316-484) and SimpleSecEmitter
+ * (:489-597).  orc_secelec_t holds the stainless parameters of stainlessMod
+ * (:331-352) after seyMax / reflec.  Draw order (mode 0 = the reference's):
+ * pass 1 per particle: E decision, R decision, TS rounding (3 draws, :387-394);
+ * pass 2 per particle: R speed factor if R (:435), TS: n normal deviates for
+ * the lognormal energies (:445), n uniforms if their sum exceeds E0 (:448-450),
+ * then theta and phi per TS secondary (:456-458).  SimpleSecEmitter: R speed
+ * factor (:567), n uniform energies (:577), no angles.  mode 1: 64 injected
+ * uniforms per particle consumed in that order from draw 0 (normal = Box-Muller
+ * of two), the GPU kernel's layout.
+ * ------------------------------------------------------------------------ */
+typedef struct {
+    int32_t model; /* 0 SecElecEmitter, 1 SimpleSecEmitter */
+    int32_t max_ts;
+    double p1EInf, p1Ehat, eEHat, w, p, e1, e2, p1RInf, eR, r, r1, r2;
+    double deltaTSHat, s, eHat0, t1, t2, t3, t4, sigmaETS, muETS, theta0max, deltaERmax, q;
+    double particle_mass;
+} orc_secelec_t;
+
+int64_t orc_secelec_emit(const orc_secelec_t *f, const double *ab, const double *nv, int64_t n0, int mode,
+                         const double *uniforms, double *out, int64_t out_cap) {
+    const double qe = 1.602176565e-19;
+    const double mass = f->model == 1 ? 9.10938291e-31 : f->particle_mass;
+    const double eF = 0.5 * mass / qe, eFi = 1. / eF;
+    double *e0 = (double *)malloc(sizeof(double) * (n0 > 0 ? n0 : 1));
+    int *nE = (int *)calloc(n0 > 0 ? n0 : 1, sizeof(int));
+    int *nR = (int *)calloc(n0 > 0 ? n0 : 1, sizeof(int));
+    int *nT = (int *)calloc(n0 > 0 ? n0 : 1, sizeof(int));
+    Src src = {mode, NULL, 0};
+    for (int64_t j = 0; j < n0; ++j) {
+        const double *r = ab + 6 * j;
+        double v0 = sqrt(r[2] * r[2] + r[3] * r[3] + r[4] * r[4]);
+        e0[j] = eF * v0 * v0;
+        double dE, dR, dTS;
+        if (f->model == 1) {
+            const double s = 1.813, eHat = 310;
+            dE = 0.05;
+            dR = 0.5;
+            dTS = 1.4 * s * e0[j] / eHat / (s - 1 + pow(e0[j] / eHat, s));
+        } else {
+            double th = acos((r[2] * nv[2 * j] + r[3] * nv[2 * j + 1]) / v0);
+            if (th > 0.5 * PI) th = PI - th;
+            th = clipd(th, 0., f->theta0max);
+            dE = (f->p1EInf + (f->p1Ehat - f->p1EInf) * exp(-pow(fabs(e0[j] - f->eEHat) / f->w, f->p) / f->p)) *
+                 (1 + f->e1 * (1 - pow(cos(th), f->e2)));
+            dR = f->p1RInf * (1 - exp(-pow(e0[j] / f->eR, f->r))) * (1 + f->r1 * (1 - pow(cos(th), f->r2)));
+            double eHat = f->eHat0 * (1 + f->t3 * (1 - pow(cos(th), f->t4)));
+            dTS = f->deltaTSHat * f->s * e0[j] / eHat / (f->s - 1 + pow(e0[j] / eHat, f->s)) *
+                  (1 + f->t1 * (1 - pow(cos(th), f->t2)));
+            double t = dE + dR;
+            if (t >= f->deltaERmax) { dE = dE / t * f->deltaERmax; dR = dR / t * f->deltaERmax; }
+        }
+        if (mode == 1) { src.u = uniforms + 64 * j; src.d = 0; }
+        if (s_rand(&src) <= dE) nE[j] = 1;
+        if (s_rand(&src) <= dR) nR[j] = 1;
+        unsigned fl = (unsigned)dTS;
+        nT[j] = s_rand(&src) <= (dTS - fl) ? (int)fl + 1 : (int)fl;
+        if (nT[j] > f->max_ts) nT[j] = f->max_ts;
+    }
+    int64_t cur = 0;
+    double eSec[64];
+    for (int64_t j = 0; j < n0; ++j) {
+        const double *r = ab + 6 * j;
+        if (mode == 1) { src.u = uniforms + 64 * j; src.d = 3; }
+        double *q;
+        if (nE[j]) {
+            if (cur < out_cap) {
+                q = out + 6 * cur;
+                q[0] = r[0]; q[1] = r[1]; q[5] = r[5];
+                q[2] = -r[2]; q[3] = -r[3]; q[4] = -r[4];
+            }
+            ++cur;
+        }
+        if (nR[j]) {
+            double vF = f->model == 1 ? sqrt(s_rand(&src)) : sqrt(pow(s_rand(&src), 1. / (1. + f->q)));
+            if (cur < out_cap) {
+                q = out + 6 * cur;
+                q[0] = r[0]; q[1] = r[1]; q[5] = r[5];
+                q[2] = -r[2] * vF; q[3] = -r[3] * vF; q[4] = -r[4] * vF;
+            }
+            ++cur;
+        }
+        int n = nT[j];
+        if (n <= 0) continue;
+        if (f->model == 1) {
+            for (int i = 0; i < n; ++i) eSec[i] = s_rand(&src) * 5;
+            for (int i = 0; i < n; ++i) {
+                double vF = sqrt(eSec[i] / e0[j]);
+                if (cur < out_cap) {
+                    q = out + 6 * cur;
+                    q[0] = r[0]; q[1] = r[1]; q[5] = r[5];
+                    q[2] = -r[2] * vF; q[3] = -r[3] * vF; q[4] = -r[4] * vF;
+                }
+                ++cur;
+            }
+            continue;
+        }
+        double eSum = 0.;
+        for (int i = 0; i < n; ++i) {
+            eSec[i] = exp(f->sigmaETS * s_randn(&src) + f->muETS);
+            eSum += eSec[i];
+        }
+        if (eSum > e0[j])
+            for (int i = 0; i < n; ++i) eSec[i] = s_rand(&src) * e0[j] / n;
+        for (int i = 0; i < n; ++i) {
+            double vs = sqrt(eFi * eSec[i]);
+            double tS = asin(s_rand(&src)), cT = cos(tS), sT = sin(tS);
+            double pS = s_rand(&src) * PI * 2., cP = cos(pS), sP = sin(pS);
+            double n0v = nv[2 * j], n1v = nv[2 * j + 1];
+            double t1 = cT * n0v - sT * n1v, t2 = sT * n0v + cT * n1v;
+            if (cur < out_cap) {
+                q = out + 6 * cur;
+                q[0] = r[0]; q[1] = r[1]; q[5] = r[5];
+                q[2] = vs * ((cP + n0v * n0v * (1 - cP)) * t1 + n0v * n1v * (1 - cP) * t2);
+                q[3] = vs * ((cP + n1v * n1v * (1 - cP)) * t2 + n0v * n1v * (1 - cP) * t1);
+                q[4] = vs * (-sP * n1v * t1 + sP * n0v * t2);
+            }
+            ++cur;
+        }
+    }
+    free(e0);
+    free(nE);
+    free(nR);
+    free(nT);
+    return cur;
+}

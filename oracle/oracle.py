@@ -252,6 +252,59 @@ def furman_emit(params, rows, normals, mode=0, uniforms=None, seed=None):
     return out[:k].copy()
 
 
+class OrcSecElec(ctypes.Structure):
+    _fields_ = [("model", ctypes.c_int32), ("max_ts", ctypes.c_int32)] + \
+        [(k, ctypes.c_double) for k in ("p1EInf", "p1Ehat", "eEHat", "w", "p", "e1", "e2", "p1RInf", "eR", "r", "r1",
+                                        "r2", "deltaTSHat", "s", "eHat0", "t1", "t2", "t3", "t4", "sigmaETS",
+                                        "muETS", "theta0max", "deltaERmax", "q", "particle_mass")]
+
+
+# SecElecEmitter.stainlessMod (particleEmitter.pyx:331-352)
+STAINLESS_SIMPLE = dict(p1EInf=0.07, p1Ehat=0.5, eEHat=0., w=100., p=0.9, e1=0.26, e2=2., q=0.4, p1RInf=0.74,
+                        eR=40., r=1., r1=0.26, r2=2., deltaTSHat=1.22, s=1.813, eHat0=310., t3=0.7, t4=1., t1=0.66,
+                        t2=0.8, sigmaETS=1.041, muETS=2.456)
+
+
+def secelec(model=0, seyMax=-1.0, reflec=-1.0, max_ts=10):
+    """Parameters of SecElecEmitter (model 0, stainlessMod with seyMax /
+    reflec, particleEmitter.pyx:331-352) or SimpleSecEmitter (model 1)."""
+    t = dict(STAINLESS_SIMPLE)
+    t["theta0max"] = 84. * 3.141592653589793 / 180
+    t["deltaERmax"] = 0.99
+    if seyMax >= 0.5:
+        t["deltaTSHat"] = seyMax - t["p1RInf"] - t["p1EInf"]
+        if t["deltaTSHat"] < 0.:
+            t["deltaTSHat"] = 1.e-6
+    if reflec >= 0.:
+        t["p1Ehat"] = reflec
+    f = OrcSecElec()
+    for k, v in t.items():
+        setattr(f, k, v)
+    f.model, f.max_ts = int(model), int(max_ts)
+    f.particle_mass = 9.10938291e-31
+    return f
+
+
+def secelec_emit(params, rows, normals, mode=0, uniforms=None, seed=None):
+    """SecElecEmitter / SimpleSecEmitter.generateSecondaries restated; mode 0:
+    MT stream (seed first), mode 1: uniforms (n, 64)."""
+    L = lib()
+    if not getattr(L, "_secelec_declared", False):
+        L.orc_secelec_emit.restype = _I64
+        L.orc_secelec_emit.argtypes = [ctypes.POINTER(OrcSecElec), _P, _P, _I64, _I, _P, _P, _I64]
+        L._secelec_declared = True
+    rows = _c(rows, np.float64)
+    normals = _c(normals, np.float64)
+    n = rows.shape[0]
+    if seed is not None:
+        L.orc_seed(int(seed))
+    u = _c(uniforms if uniforms is not None else np.zeros((1, 64)), np.float64)
+    cap = (2 + params.max_ts) * max(n, 1)
+    out = np.empty((cap, 6), np.float64)
+    k = L.orc_secelec_emit(ctypes.byref(params), _p(rows), _p(normals), n, int(mode), _p(u), _p(out), cap)
+    return out[:k].copy()
+
+
 def betaincinv(a, b, p):
     furman_emit(furman(), np.zeros((0, 6)), np.zeros((0, 2)))  # declares signatures
     return lib().orc_betaincinv(float(a), float(b), float(p))

@@ -186,14 +186,11 @@ if __name__ == "__main__" and not any(a.startswith("--") for a in sys.argv[1:]):
     main()
 
 
-def emission_golden():
-    """Reference Furman emission on absorbed sets, replayable by the oracle
-    (same MT stream, same seed), plus special-function values."""
+def _emission_absorbed():
+    """The absorbed set of the emission fixtures: 16000 particles near the
+    wall of a 64x64 circular chamber pushed across it (seed 4242)."""
     grid, particles, particleBoundary, poissonSolver, randomGen = _import_reference()
-    import particleEmitter
-    import ref_probe
     rng = np.random.default_rng(4242)
-    out = {}
     g = grid.Grid(64, 64, 0.04, 0.04, 1)
     n = 16000
     dtb = 1e-11
@@ -226,6 +223,17 @@ def emission_golden():
     bd.saveAbsorbed()
     bd.calculateInteractionPoint()
     bd.calculateNormalVectors()
+    return P, bd
+
+
+def emission_golden():
+    """Reference Furman emission on absorbed sets, replayable by the oracle
+    (same MT stream, same seed), plus special-function values."""
+    grid, particles, particleBoundary, poissonSolver, randomGen = _import_reference()
+    import particleEmitter
+    import ref_probe
+    out = {}
+    P, bd = _emission_absorbed()
     out["abs_rows"] = np.asarray(bd.getAbsorbedParticles()).copy()
     out["abs_normals"] = np.asarray(bd.getNormalVectors()).copy()
     cases = [("copper", -1.0, None), ("copper", 1.6, 300.0), ("stainless", 1.8, None)]
@@ -348,3 +356,64 @@ def beam_golden():
 
 if __name__ == "__main__" and "--beam" in sys.argv:
     beam_golden()
+
+
+def extras_golden():
+    """Reference multipoleExpansion on two grids and averageEnergy on a
+    seeded particle set."""
+    grid, particles, particleBoundary, poissonSolver, randomGen = _import_reference()
+    import magneticField
+    import util
+    out = {}
+    cases = [("circle_32", (32, 32, 0.04, 0.04, 1), [0., 5., 0., 0.01], []),
+             ("ellipse_40x24", (40, 24, 0.09, 0.036, 1), [1.2, 0.5, 0.02, 0.003], [0.0, 0.2]),
+             ("rect_24x20", (24, 20, 0.03, 0.02, 0), [0.3, -2.0], [0.1, 0.4, 7.0])]
+    for name, gp, normal, skew in cases:
+        g = grid.Grid(*gp)
+        out[f"mp_{name}_params"] = np.array(gp, dtype=np.float64)
+        out[f"mp_{name}_normal"] = np.array(normal, dtype=np.float64)
+        out[f"mp_{name}_skew"] = np.array(skew, dtype=np.float64)
+        out[f"mp_{name}_b"] = np.asarray(magneticField.multipoleExpansion(g, normal, skew)).copy()
+    rng = np.random.default_rng(777)
+    n = 2000
+    pd = make_particles(rng, n, 0.04, 0.04, 1, 1.0)
+    pd[:, 2:5] = rng.normal(0.0, 2e6, (n, 3))
+    pd[:, 5] = rng.uniform(0.5, 1.5, n) * 1e5
+    P = particles.Particles("electrons", "variableWeight")
+    P.setParticleData(pd.copy())
+    out["ae_particles"] = pd
+    out["ae_energy"] = np.array([util.averageEnergy(P)])
+    path = os.path.join(HERE, "extras.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path))
+
+
+if __name__ == "__main__" and "--extras" in sys.argv:
+    extras_golden()
+
+
+def secelec_golden():
+    """Reference SecElecEmitter (stainless, two settings) and SimpleSecEmitter
+    on the emission fixtures' absorbed set, each after randomGen.seed (the
+    oracle replays the same MT stream).  Needs the build recipe's integer
+    cast of the secondary count (numpy rejects the reference's double)."""
+    grid, particles, particleBoundary, poissonSolver, randomGen = _import_reference()
+    import particleEmitter
+    P, bd = _emission_absorbed()
+    out = {"abs_rows": np.asarray(bd.getAbsorbedParticles()).copy(),
+           "abs_normals": np.asarray(bd.getNormalVectors()).copy()}
+    cases = [(0, -1.0, -1.0, 2000), (0, 1.8, 0.3, 2001), (1, -1.0, -1.0, 2002)]
+    for k, (model, sey, reflec, seed) in enumerate(cases):
+        cls = particleEmitter.SecElecEmitter if model == 0 else particleEmitter.SimpleSecEmitter
+        em = cls(bd, P, seyMax=sey, reflec=reflec)
+        randomGen.seed(seed)
+        out[f"sec{k}"] = np.asarray(em.generateSecondaries()).copy()
+        out[f"case{k}"] = np.array([model, sey, reflec, seed], dtype=np.float64)
+    path = os.path.join(HERE, "secelec.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "absorbed", len(out["abs_rows"]),
+          "secondaries", [len(out[f"sec{k}"]) for k in range(3)])
+
+
+if __name__ == "__main__" and "--secelec" in sys.argv:
+    secelec_golden()
