@@ -27,26 +27,34 @@ def _import_reference():
     return grid, particles, particleBoundary, poissonSolver, randomGen
 
 
-def reference_buildup(seed, n_steps, nx=128, lx=0.04, n_init=10000, dt=1e-11, target=100000, timing=None):
-    """The reference's own loop (example01_basic.py:52-97, Python 3, no plots)
-    on the 128x128 circular chamber; returns (macro counts, sum of weights).
-    With a dict `timing`, timing["seconds"] receives the wall time of the
-    n_steps loop (setup excluded)."""
+def reference_buildup(seed, n_steps, nx=128, lx=0.04, n_init=10000, dt=1e-11, target=100000, timing=None,
+                      ny=None, ly=None, boundType=1, boundFunc=None, w_init=None):
+    """The reference's own loop (example01_basic.py:52-97, Python 3, no plots);
+    by default on the 128x128 circular chamber, else on Grid(nx, ny, lx, ly,
+    boundType, boundFunc) with the matching absorber (rectangular,
+    elliptical or cut-cell, particleBoundary.pyx); returns (macro counts, sum
+    of weights).  With a dict `timing`, timing["seconds"] receives the wall
+    time of the n_steps loop (setup excluded)."""
     grid, particles, particleBoundary, poissonSolver, randomGen = _import_reference()
     import particleEmitter
     import particleManagement
     from beam import LHCBeamEndless
     randomGen.seed(seed)
-    g = grid.Grid(nx, nx, lx, lx, 1)
+    ny = nx if ny is None else ny
+    ly = lx if ly is None else ly
+    g = grid.Grid(nx, ny, lx, ly, boundType, boundFunc=boundFunc) if boundFunc is not None else \
+        grid.Grid(nx, ny, lx, ly, boundType)
     beam = LHCBeamEndless(g, dt, nParticles=1.1e11)
     beam.bunchLengthSigma = 0.25e-9 * 299792458.0          # sigma_t = 0.25 ns
     beam.tBunchLengthSigma = beam.bunchLengthSigma / beam.beamVelocity
     P = particles.Particles("electrons", "variableWeight")
-    bd = particleBoundary.AbsorbElliptical(g, P)
+    absorber = {0: particleBoundary.AbsorbRectangular, 1: particleBoundary.AbsorbElliptical}.get(
+        boundType, particleBoundary.AbsorbArbitraryCutCell)
+    bd = absorber(g, P)
     em = particleEmitter.FurmanEmitter(bd, P, seyMax=1.6)
     em.setEHat0(300.)
     ps = poissonSolver.PoissonSolver(g)
-    particleEmitter.homoLoader(g, P, bd, n_init, 1e9 / n_init)
+    particleEmitter.homoLoader(g, P, bd, n_init, 1e9 / n_init if w_init is None else w_init)
     counts = np.zeros(n_steps + 1, np.int64)
     weight = np.zeros(n_steps + 1)
     t0 = time.perf_counter()

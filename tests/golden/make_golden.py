@@ -417,3 +417,41 @@ def secelec_golden():
 
 if __name__ == "__main__" and "--secelec" in sys.argv:
     secelec_golden()
+
+
+CC_LX, CC_LY = 0.044, 0.036
+
+
+def lhc_bound(x, y):
+    """example05_arbitraryGeometry.py:35-39, as written there (its y test
+    compares y^2 with 0.5 ly, so only the circle of radius lx/2 bounds)."""
+    if x ** 2 + y ** 2 <= (0.5 * CC_LX) ** 2 and y ** 2 < 0.5 * CC_LY:
+        return 1
+    else:
+        return 0
+
+
+CC_RUN = dict(nx=44, ny=36, lx=CC_LX, ly=CC_LY, boundType=3, n_init=44 * 36 * 20, dt=2.155172413795e-11)
+
+
+def buildup_cc_golden(n_seeds=8, n_steps=1160):
+    """The reference loop on example05's chamber (cut-cell boundary from a
+    user boundFunc, AbsorbArbitraryCutCell), c1's beam and emitter, one bunch
+    passage at example05's time step, 8 seeds."""
+    from ref_buildup import reference_buildup
+    W, C = [], []
+    for s in range(n_seeds):
+        c, w = reference_buildup(300 + s, n_steps, boundFunc=lhc_bound, **CC_RUN)
+        W.append(w)
+        C.append(c)
+        print("seed", s, "final count", c[-1], "line density", w[-1], flush=True)
+    out = {"weight": np.array(W)[:, ::10], "count": np.array(C)[:, ::10], "every": np.array(10),
+           "n_steps": np.array(n_steps)}
+    path = os.path.join(HERE, "buildup_cc.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path))
+
+
+if __name__ == "__main__" and "--buildup-cc" in sys.argv:
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    buildup_cc_golden()

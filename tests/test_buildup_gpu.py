@@ -67,3 +67,36 @@ def test_buildup_step_graph_with_multigrid_pcg(gpu):
     n_lu, w_lu = lu.history()
     n_pcg, w_pcg = b.history()
     assert abs(w_pcg[-1] / w_lu[-1] - 1.0) < 0.05, (w_pcg[-1], w_lu[-1])
+
+
+def _lhc_bound(x, y):
+    # example05_arbitraryGeometry.py:35-39 as written (lx = 0.044, ly = 0.036)
+    if x ** 2 + y ** 2 <= (0.5 * 0.044) ** 2 and y ** 2 < 0.5 * 0.036:
+        return 1
+    return 0
+
+
+def test_cut_cell_buildup_within_reference_spread(gpu):
+    """example05's chamber: a cut-cell boundary from a user boundFunc
+    (boundType 3) with AbsorbArbitraryCutCell in the fused kernel, c1's beam
+    and emitter, one bunch passage (1160 steps of 2.155e-11 s): the ensemble
+    mean of 8 device runs stays within twice the reference's seed-to-seed
+    spread (floor 0.2 %)."""
+    from openecloud_b200.buildup import Buildup
+    z = golden("buildup_cc.npz")
+    every, n_steps = int(z["every"]), int(z["n_steps"])
+    ref = z["weight"]
+    runs = []
+    for s in range(8):
+        b = Buildup(nx=44, ny=36, lx=0.044, ly=0.036, boundType=3, boundFunc=_lhc_bound, n_init=44 * 36 * 20,
+                    dt=2.155172413795e-11, seed=2000 + s, n_steps_table=n_steps + 1)
+        b.run(n_steps)
+        st = b.status()
+        assert st["n_capacity_drop"] == 0 and st["n_nonfinite"] == 0
+        runs.append(b.history()[1][::every])
+    m_ref, s_ref = ref.mean(0), ref.std(0, ddof=1)
+    m_gpu = np.array(runs).mean(0)
+    tol = 2 * np.maximum(s_ref, 0.002 * m_ref)
+    bad = np.abs(m_gpu - m_ref) > tol
+    assert not bad.any(), (np.nonzero(bad)[0][:10], m_gpu[bad][:5], m_ref[bad][:5])
+    assert m_gpu[-1] / m_gpu[0] > 1.2
