@@ -497,13 +497,10 @@ def run_ours(args, rank, world, local_rank):
         hp, op_, sp = host.data_ptr(), out.data_ptr(), staging.data_ptr()
 
         def e2e_step():
-            rc = L.oec_particles_upload_host(cg, hp, n, cp, sp, stage_rows, sh)
+            rc = L.oec_push_gather_host(cg, cp, hp, op_, n, sp, stage_rows, et.data_ptr(), None, bconst, dt, qm, 1,
+                                        cb, mask, rho, wsc, st, sh)
             if rc:
-                raise _lib.OecError("oec_particles_upload_host", rc)
-            step()
-            rc = L.oec_particles_download_host(cg, cp, op_, n, sp, stage_rows, sh)
-            if rc:
-                raise _lib.OecError("oec_particles_download_host", rc)
+                raise _lib.OecError("oec_push_gather_host", rc)
 
         e2e_step()
         torch.cuda.synchronize()
@@ -522,8 +519,8 @@ def run_ours(args, rank, world, local_rank):
             ms_e2e = float(t[0])
         e2e = {"value": n * world / (ms_e2e * 1e-3), "unit": METRIC, "h2d_bytes_per_step": int(n * 48),
                "d2h_bytes_per_step": int(n * 48), "ms_per_step": ms_e2e,
-               "path": "oec_particles_upload_host -> oec_push_gather -> oec_particles_download_host, "
-                       "(N,6) f64 rows in pinned host memory"}
+               "path": "oec_push_gather_host: (N,6) f64 rows in pinned host memory -> upload, fused kernel, "
+                       "download in chunks with both copy directions overlapped (3 streams)"}
 
     # ----------------------------------------------------------- roofline
     G = (nx + 2) * (ny + 2)

@@ -105,6 +105,25 @@ int oec_particles_download_host(const oec_grid_t *grid, const oec_particles_t *p
                                 double *aos_host, int64_t n, double *staging_dev,
                                 int64_t staging_rows, void *stream);
 
+/* One step from host rows to host rows: setParticleData + the fused
+ * oec_push_gather + getParticleData (particles.pyx:126, :142 around the
+ * pushes) with the copies overlapped.  The rows go through a ring of 4
+ * staging slots in staging_dev (staging_rows rows of 6 doubles; each slot
+ * holds ((staging_rows - 1) / 4) rounded down to a multiple of 1024 rows, at
+ * least 1024; the row after the slots holds the slots' counts): uploads on
+ * one stream, the conversion, the fused kernel on that chunk of the store and
+ * the conversion back on `stream`, downloads on a third, so both copy
+ * directions run while the kernels do.  rows_out_host may be rows_in_host.
+ * The store ends with count n; rho, the absorbed bits and the status as
+ * oec_push_gather.  Pinned host memory lets the copies overlap.  Returns
+ * when queued; the work is ordered on `stream`.  Overlapping calls race. */
+int oec_push_gather_host(const oec_grid_t *grid, oec_particles_t *p, const double *rows_in_host,
+                         double *rows_out_host, int64_t n, double *staging_dev, int64_t staging_rows,
+                         const float *e_cell_dev, const float *b_cell_dev, const double bconst[3], double dt,
+                         double charge_over_mass, int32_t type_b_field, const oec_boundary_t *boundary,
+                         uint32_t *absorbed_mask_dev, int64_t *rho_fix_dev, const double *wscale_dev,
+                         oec_status_t *status_dev, void *stream);
+
 /* ------------------------------------------- weights, gather, push (A2-A8) */
 
 /* calcGridWeights (particles.pyx:52-56, :400-418): inCell and the four CIC

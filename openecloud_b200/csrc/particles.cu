@@ -1054,12 +1054,14 @@ static FusedArgs make_fused_args(const GridConst &gc, oec_particles_t *p) {
     return a;
 }
 
-extern "C" int oec_push_gather(const oec_grid_t *grid, oec_particles_t *p, const float *e_cell_dev,
-                               const float *b_cell_dev, const double bconst[3], double dt,
-                               double charge_over_mass, int32_t type_b_field,
-                               const oec_boundary_t *boundary, uint32_t *absorbed_mask_dev,
-                               int64_t *rho_fix_dev, const double *wscale_dev,
-                               oec_status_t *status_dev, void *stream) {
+namespace oec {
+namespace {
+
+// Arguments of the fused kernel for the store (or store view) p.
+int push_args(const oec_grid_t *grid, oec_particles_t *p, const float *e_cell_dev, const float *b_cell_dev,
+              const double bconst[3], double dt, double charge_over_mass, int32_t type_b_field,
+              const oec_boundary_t *boundary, uint32_t *absorbed_mask_dev, int64_t *rho_fix_dev,
+              const double *wscale_dev, oec_status_t *status_dev, FusedArgs &a) {
     if (!valid_grid(grid) || !valid_particles(p) || !e_cell_dev || !absorbed_mask_dev || !status_dev)
         return OEC_ERR_INVALID;
     if (type_b_field < 0 || type_b_field > 2) return OEC_ERR_INVALID;
@@ -1068,7 +1070,7 @@ extern "C" int oec_push_gather(const oec_grid_t *grid, oec_particles_t *p, const
     if (rho_fix_dev && !wscale_dev) return OEC_ERR_INVALID;
     GridConst gc = make_grid_const(*grid);
     double zero[3] = {0, 0, 0};
-    FusedArgs a = make_fused_args(gc, p);
+    a = make_fused_args(gc, p);
     a.k = make_push_const(gc, bconst ? bconst : zero, dt, charge_over_mass, type_b_field);
     int rc = make_boundary_const(boundary, gc, a.b);
     if (rc != OEC_OK) return rc;
@@ -1078,18 +1080,38 @@ extern "C" int oec_push_gather(const oec_grid_t *grid, oec_particles_t *p, const
     a.rho = reinterpret_cast<unsigned long long *>(rho_fix_dev);
     a.wscale = wscale_dev;
     a.status = status_dev;
-    cudaStream_t s = as_stream(stream);
-    OEC_CUDA_TRY(cudaMemsetAsync(&status_dev->n_absorbed, 0, sizeof(int32_t), s));
-    if (rho_fix_dev)
-        OEC_CUDA_TRY(cudaMemsetAsync(rho_fix_dev, 0, sizeof(int64_t) * (size_t)gc.G, s));
-    int g = persistent_grid(cap_chunks(p), 8);
-    bool dep = rho_fix_dev != nullptr;
+    return OEC_OK;
+}
+
+void launch_push(const FusedArgs &a, int32_t type_b_field, const oec_particles_t *p, cudaStream_t s) {
+    const int g = persistent_grid(cap_chunks(p), 8);
+    const bool dep = a.rho != nullptr;
     if (type_b_field == 0)
         launch_fused_kind<0>(a, a.b.kind, dep, g, s);
     else if (type_b_field == 1)
         launch_fused_kind<1>(a, a.b.kind, dep, g, s);
     else
         launch_fused_kind<2>(a, a.b.kind, dep, g, s);
+}
+
+}  // namespace
+}  // namespace oec
+
+extern "C" int oec_push_gather(const oec_grid_t *grid, oec_particles_t *p, const float *e_cell_dev,
+                               const float *b_cell_dev, const double bconst[3], double dt,
+                               double charge_over_mass, int32_t type_b_field,
+                               const oec_boundary_t *boundary, uint32_t *absorbed_mask_dev,
+                               int64_t *rho_fix_dev, const double *wscale_dev,
+                               oec_status_t *status_dev, void *stream) {
+    FusedArgs a;
+    int rc = push_args(grid, p, e_cell_dev, b_cell_dev, bconst, dt, charge_over_mass, type_b_field, boundary,
+                       absorbed_mask_dev, rho_fix_dev, wscale_dev, status_dev, a);
+    if (rc != OEC_OK) return rc;
+    cudaStream_t s = as_stream(stream);
+    OEC_CUDA_TRY(cudaMemsetAsync(&status_dev->n_absorbed, 0, sizeof(int32_t), s));
+    if (rho_fix_dev)
+        OEC_CUDA_TRY(cudaMemsetAsync(rho_fix_dev, 0, sizeof(int64_t) * (size_t)grid->nx * grid->ny, s));
+    launch_push(a, type_b_field, p, s);
     OEC_LAUNCH_CHECK();
     return OEC_OK;
 }
@@ -1209,6 +1231,38 @@ Pipe &pipe() {
     return p;
 }
 
+// Ring of staging slots for a whole host-to-host step: uploads on one
+// stream, the kernels on the caller's stream, downloads on a third, so the
+// two copy directions overlap each other and the kernels.
+constexpr int kRing = 4;
+
+struct StepPipe {
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    cudaEvent_t in[kRing], out[kRing], freed[kRing], start = nullptr, done = nullptr;
+    bool ready = false;
+    int init() {
+        if (ready) return OEC_OK;
+        OEC_CUDA_TRY(cudaStreamCreateWithFlags(&h2d, cudaStreamNonBlocking));
+        OEC_CUDA_TRY(cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking));
+        for (int k = 0; k < kRing; ++k) {
+            OEC_CUDA_TRY(cudaEventCreateWithFlags(&in[k], cudaEventDisableTiming));
+            OEC_CUDA_TRY(cudaEventCreateWithFlags(&out[k], cudaEventDisableTiming));
+            OEC_CUDA_TRY(cudaEventCreateWithFlags(&freed[k], cudaEventDisableTiming));
+        }
+        OEC_CUDA_TRY(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
+        OEC_CUDA_TRY(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+        ready = true;
+        return OEC_OK;
+    }
+};
+
+StepPipe &step_pipe() {
+    static StepPipe p;
+    return p;
+}
+
+__global__ void k_set_count(int32_t *count, int32_t value) { *count = value; }
+
 }  // namespace
 }  // namespace oec
 
@@ -1281,5 +1335,75 @@ extern "C" int oec_particles_download_host(const oec_grid_t *grid, const oec_par
     // make `stream` wait for the last host copies so its users see the data
     OEC_CUDA_TRY(cudaEventRecord(pp.copied[0], pp.copy));
     OEC_CUDA_TRY(cudaStreamWaitEvent(s, pp.copied[0], 0));
+    return OEC_OK;
+}
+
+extern "C" int oec_push_gather_host(const oec_grid_t *grid, oec_particles_t *p, const double *rows_in_host,
+                                    double *rows_out_host, int64_t n, double *staging_dev, int64_t staging_rows,
+                                    const float *e_cell_dev, const float *b_cell_dev, const double bconst[3],
+                                    double dt, double charge_over_mass, int32_t type_b_field,
+                                    const oec_boundary_t *boundary, uint32_t *absorbed_mask_dev,
+                                    int64_t *rho_fix_dev, const double *wscale_dev, oec_status_t *status_dev,
+                                    void *stream) {
+    if (!valid_grid(grid) || !valid_particles(p) || n < 0 || (n > 0 && (!rows_in_host || !rows_out_host)) ||
+        !staging_dev || !absorbed_mask_dev || !status_dev)
+        return OEC_ERR_INVALID;
+    if (n > p->capacity) return OEC_ERR_CAPACITY;
+    // slots of C rows (a multiple of kChunk, so every view keeps the float4
+    // groups and the absorbed words aligned) and, after them, a count per slot
+    const int64_t C = ((staging_rows - 1) / kRing) / kChunk * kChunk;
+    if (C < kChunk) return OEC_ERR_INVALID;
+    int32_t *counts = reinterpret_cast<int32_t *>(staging_dev + 6 * kRing * C);
+    {
+        FusedArgs probe;  // argument checks on the whole store
+        int rc = push_args(grid, p, e_cell_dev, b_cell_dev, bconst, dt, charge_over_mass, type_b_field, boundary,
+                           absorbed_mask_dev, rho_fix_dev, wscale_dev, status_dev, probe);
+        if (rc != OEC_OK) return rc;
+    }
+    StepPipe &pp = step_pipe();
+    int rc = pp.init();
+    if (rc != OEC_OK) return rc;
+    cudaStream_t s = as_stream(stream);
+    GridConst gc = make_grid_const(*grid);
+    OEC_CUDA_TRY(cudaMemsetAsync(&status_dev->n_absorbed, 0, sizeof(int32_t), s));
+    if (rho_fix_dev) OEC_CUDA_TRY(cudaMemsetAsync(rho_fix_dev, 0, sizeof(int64_t) * (size_t)gc.G, s));
+    k_set_count<<<1, 1, 0, s>>>(p->count, (int32_t)n);
+    // neither copy stream may run ahead of the work already queued on s
+    OEC_CUDA_TRY(cudaEventRecord(pp.start, s));
+    OEC_CUDA_TRY(cudaStreamWaitEvent(pp.h2d, pp.start, 0));
+    OEC_CUDA_TRY(cudaStreamWaitEvent(pp.d2h, pp.start, 0));
+    int k = 0;
+    for (int64_t off = 0; off < n; off += C, ++k) {
+        const int slot = k % kRing;
+        const int64_t rows = n - off < C ? n - off : C;
+        double *buf = staging_dev + 6 * C * slot;
+        if (k >= kRing) OEC_CUDA_TRY(cudaStreamWaitEvent(pp.h2d, pp.freed[slot], 0));
+        OEC_CUDA_TRY(cudaMemcpyAsync(buf, rows_in_host + 6 * off, sizeof(double) * 6 * rows, cudaMemcpyHostToDevice,
+                                     pp.h2d));
+        OEC_CUDA_TRY(cudaEventRecord(pp.in[slot], pp.h2d));
+        OEC_CUDA_TRY(cudaStreamWaitEvent(s, pp.in[slot], 0));
+        k_from_aos_rows<<<(unsigned)((rows + 255) / 256), 256, 0, s>>>(buf, off, rows, *p, gc.nx, gc.ny, gc.dxi, gc.dyi,
+                                                                       gc.lxh, gc.lyh);
+        k_set_count<<<1, 1, 0, s>>>(counts + slot, (int32_t)rows);
+        const int64_t view_cap = p->capacity - off < C ? p->capacity - off : C;
+        oec_particles_t view{p->cell + off, p->ox + off, p->oy + off, p->vx + off, p->vy + off, p->vz + off,
+                             p->w + off, counts + slot, view_cap};
+        FusedArgs a;
+        rc = push_args(grid, &view, e_cell_dev, b_cell_dev, bconst, dt, charge_over_mass, type_b_field, boundary,
+                       absorbed_mask_dev + off / 32, rho_fix_dev, wscale_dev, status_dev, a);
+        if (rc != OEC_OK) return rc;
+        launch_push(a, type_b_field, &view, s);
+        k_to_aos_rows<<<(unsigned)((rows + 255) / 256), 256, 0, s>>>(*p, off, rows, buf, gc.nx, 1.0f / (float)gc.nx,
+                                                                     gc.dx, gc.dy, gc.lxh, gc.lyh);
+        OEC_LAUNCH_CHECK();
+        OEC_CUDA_TRY(cudaEventRecord(pp.out[slot], s));
+        OEC_CUDA_TRY(cudaStreamWaitEvent(pp.d2h, pp.out[slot], 0));
+        OEC_CUDA_TRY(cudaMemcpyAsync(rows_out_host + 6 * off, buf, sizeof(double) * 6 * rows, cudaMemcpyDeviceToHost,
+                                     pp.d2h));
+        OEC_CUDA_TRY(cudaEventRecord(pp.freed[slot], pp.d2h));
+    }
+    // the caller's stream covers the last download
+    OEC_CUDA_TRY(cudaEventRecord(pp.done, pp.d2h));
+    OEC_CUDA_TRY(cudaStreamWaitEvent(s, pp.done, 0));
     return OEC_OK;
 }

@@ -181,3 +181,66 @@ def test_fused_push_gather_inside_deposit(gpu, name, tb):
     st = P.status()
     assert st["n_absorbed"] == int((ins == 0).sum())
     assert st["n_nonfinite"] == 0
+
+
+def test_push_gather_host_equals_sequential_path(gpu):
+    """oec_push_gather_host (host rows in, host rows out, copies overlapped
+    over a ring of staging slots) gives the rows, deposit, absorbed bits and
+    absorbed count of upload + fused kernel + download, bit for bit, over
+    many chunks (300 000 particles through 16384-row slots, a shared output
+    and an in-place call)."""
+    import torch
+    from openecloud_b200 import _lib
+    from openecloud_b200 import device as D
+    from openecloud_b200 import particleBoundary as PB
+    from openecloud_b200.grid import Grid
+    from openecloud_b200.particles import Particles
+    rng = np.random.default_rng(12)
+    n = 300_000
+    g = Grid(128, 128, 0.04, 0.04, 0)
+    pd = np.empty((n, 6))
+    pd[:, 0] = rng.uniform(-0.0199, 0.0199, n)
+    pd[:, 1] = rng.uniform(-0.0199, 0.0199, n)
+    pd[:, 2:5] = rng.normal(0.0, 3e6, (n, 3))
+    pd[:, 5] = rng.uniform(0.5, 1.5, n) * 1e4
+    E = rng.normal(0.0, 2e4, 2 * g.getNpExt())
+    dt = 2e-11
+
+    def store():
+        P = Particles("electrons", "variableWeight", capacity=n + 1024)
+        P.setParticleData(pd)
+        P.setBConst([0.0, 0.5, 0.0])
+        bd = PB.AbsorbRectangular(g, P)
+        et = P.fieldTable(g, E, 2)
+        P.pushGatherDeposit(g, et, dt, 1, bd)  # deposit scale and buffers
+        P.setParticleData(pd)
+        torch.cuda.synchronize()
+        return P, bd, et
+
+    P, bd, et = store()
+    P.pushGatherDeposit(g, et, dt, 1, bd)
+    ref_rows = P.getParticleData()
+    ref_rho = D.to_numpy(P._rho_fix).copy()
+    ref_mask = D.to_numpy(P._mask).copy()
+    ref_abs = P.status()["n_absorbed"]
+
+    Q, bq, eq = store()
+    L = _lib.lib()
+    rows = 4 * 16384 + 1
+    staging = torch.empty((rows, 6), dtype=torch.float64, device="cuda")
+    host_in = torch.from_numpy(pd.copy()).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    for out in (host_out, host_in):  # a separate output, then in place
+        Q.setParticleData(pd)
+        host_in.copy_(torch.from_numpy(pd))
+        rc = L.oec_push_gather_host(g.c_grid(), Q.c_particles(), host_in.data_ptr(), out.data_ptr(), n,
+                                    staging.data_ptr(), rows, eq.data_ptr(), None, _lib.d3(Q.bConst), dt,
+                                    Q.particleCharge / Q.particleMass, 1, bq.c_boundary(), Q._mask.data_ptr(),
+                                    Q._rho_fix.data_ptr(), Q._wscale.data_ptr(), Q._status.data_ptr(),
+                                    D.stream())
+        assert rc == 0
+        torch.cuda.synchronize()
+        assert np.array_equal(out.numpy(), ref_rows)
+        assert np.array_equal(D.to_numpy(Q._rho_fix), ref_rho)
+        assert np.array_equal(D.to_numpy(Q._mask)[:ref_mask.size], ref_mask)
+        assert Q.status()["n_absorbed"] == ref_abs and Q.getMacroParticleCount() == n
