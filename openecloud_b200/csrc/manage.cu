@@ -85,50 +85,67 @@ __global__ void k_scan_serial_chunks(int *a, int len) {
     }
 }
 
-__global__ void k_scatter(const uint32_t *__restrict__ keys, const int32_t *__restrict__ vals, const int32_t *n_p,
-                          int shift, int ntiles, const int *__restrict__ offs, uint32_t *__restrict__ okeys,
-                          int32_t *__restrict__ ovals) {
+// Exclusive scan of a[0, len) in place by 1024-element blocks (each block's
+// total to partial[block]), then the scan of the block totals, then the add:
+// the digit histograms of a large sort are millions of entries long.
+__global__ void k_scan_tiles(int *a, int len, int *partial) {
     __shared__ int sh[32];
-    __shared__ int dstart[256];
-    __shared__ int dcount[256];
-    __shared__ uint32_t skeys[kTile];
-    __shared__ int32_t svals[kTile];
-    int n = *n_p;
-    int i = blockIdx.x * kTile + threadIdx.x;
-    bool valid = i < n;
-    uint32_t k = valid ? keys[i] : 0xffffffffu;
-    int32_t v = valid ? vals[i] : 0;
-    uint32_t d = (k >> shift) & 255u;
-    // stable local sort by the 8-bit digit: eight stable 1-bit splits
-    for (int b = 0; b < 8; ++b) {
-        int bit = (d >> b) & 1u;
-        int tot;
-        int zeros_before = blk_scan(bit ^ 1, &tot, sh);  // tot = number of zeros
-        int pos = bit ? (tot + (threadIdx.x - zeros_before)) : zeros_before;
-        skeys[pos] = k;
-        svals[pos] = v;
-        __syncthreads();
-        k = skeys[threadIdx.x];
-        v = svals[threadIdx.x];
-        d = (k >> shift) & 255u;
-        __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = i < len ? a[i] : 0;
+    int tot;
+    const int ex = blk_scan(v, &tot, sh);
+    if (i < len) a[i] = ex;
+    if (threadIdx.x == 0) partial[blockIdx.x] = tot;
+}
+
+__global__ void k_scan_add_tiles(int *a, int len, const int *partial) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < len) a[i] += partial[blockIdx.x];
+}
+
+// Stable scatter of one tile (kTile elements, one per thread) by the digit
+// at `shift`: a thread's place among the equal digits of its warp comes
+// from a match over the warp (the lanes below it with the same digit); the
+// counts of every (digit, warp) pair, scanned digit-major, give each warp's
+// start inside its digit, so the order is (digit, warp, lane) = stable.
+__global__ void __launch_bounds__(kTile) k_scatter(const uint32_t *__restrict__ keys,
+                                                   const int32_t *__restrict__ vals, const int32_t *n_p, int shift,
+                                                   int ntiles, const int *__restrict__ offs,
+                                                   uint32_t *__restrict__ okeys, int32_t *__restrict__ ovals) {
+    constexpr int kWarps = kTile / 32;
+    __shared__ int sh[32];
+    __shared__ int cnt[256 * kWarps];  // (digit, warp), digit-major
+    const int n = *n_p;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int i = blockIdx.x * kTile + threadIdx.x;
+    const bool valid = i < n;
+    const uint32_t k = valid ? keys[i] : 0u;
+    const int32_t v = valid ? vals[i] : 0;
+    const int d = valid ? (int)((k >> shift) & 255u) : 256;  // 256: no element
+    for (int e = threadIdx.x; e < 256 * kWarps; e += kTile) cnt[e] = 0;
+    __syncthreads();
+    const unsigned peers = __match_any_sync(kFullMask, d);
+    const int rank = __popc(peers & ((1u << lane) - 1u));
+    if (valid && rank == 0) cnt[d * kWarps + w] = __popc(peers);
+    __syncthreads();
+    // exclusive scan of the 256 * kWarps counts, kWarps per thread... 8 each
+    constexpr int kPerThread = 256 * kWarps / kTile;
+    int local[kPerThread], sum = 0;
+#pragma unroll
+    for (int j = 0; j < kPerThread; ++j) {
+        local[j] = cnt[threadIdx.x * kPerThread + j];
+        sum += local[j];
     }
-    // local start of each digit
-    for (int t = threadIdx.x; t < 256; t += blockDim.x) dcount[t] = 0;
-    __syncthreads();
-    int local_valid = min(kTile, n - blockIdx.x * kTile);
-    if ((int)threadIdx.x < local_valid) atomicAdd(&dcount[d], 1);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int s = 0;
-        for (int t = 0; t < 256; ++t) {
-            dstart[t] = s;
-            s += dcount[t];
-        }
+    int base = blk_scan(sum, nullptr, sh);
+#pragma unroll
+    for (int j = 0; j < kPerThread; ++j) {
+        cnt[threadIdx.x * kPerThread + j] = base;
+        base += local[j];
     }
     __syncthreads();
-    if ((int)threadIdx.x < local_valid) {
-        int dst = offs[d * ntiles + blockIdx.x] + ((int)threadIdx.x - dstart[d]);
+    if (valid) {
+        const int local_pos = cnt[d * kWarps + w] + rank;
+        const int dst = offs[d * ntiles + blockIdx.x] + (local_pos - cnt[d * kWarps]);
         okeys[dst] = k;
         ovals[dst] = v;
     }
@@ -427,18 +444,30 @@ static bool vp2(const oec_particles_t *p) {
     return p && p->cell && p->ox && p->oy && p->vx && p->vy && p->vz && p->w && p->count && p->capacity > 0;
 }
 
+// Blocks of the histogram scan (256 digits x tiles entries, 1024 per block).
+static int64_t hist_scan_blocks(int64_t capacity) {
+    const int64_t tiles = (capacity + kTile - 1) / kTile;
+    return (256 * tiles + 1023) / 1024;
+}
+
 extern "C" int64_t oec_sort_work_bytes(int64_t capacity) {
     int64_t tiles = (capacity + kTile - 1) / kTile;
-    return 4 * capacity * 4 + 256 * tiles * 4 + 256;
+    // keys, vals (twice) | histogram | 256-byte slack (merge counters) | block totals
+    return 4 * capacity * 4 + 256 * tiles * 4 + 256 + 4 * hist_scan_blocks(capacity) + 256;
 }
 
 // Stable radix sort of (keys, vals) pairs, keys in work; `bits` significant key bits.
 static int radix_sort(uint32_t *keys, int32_t *vals, uint32_t *k2, int32_t *v2, int *hist, const int32_t *n_dev,
                       int64_t cap, int bits, cudaStream_t s, uint32_t **kout, int32_t **vout) {
     int ntiles = (int)((cap + kTile - 1) / kTile);
+    const int len = 256 * ntiles, nb = (int)hist_scan_blocks(cap);
+    // block totals after the histogram and its 256-byte slack
+    int *partial = reinterpret_cast<int *>(reinterpret_cast<char *>(hist) + 4 * (int64_t)len + 256);
     for (int shift = 0; shift < bits; shift += 8) {
         k_digit_hist<<<ntiles, kTile, 0, s>>>(keys, n_dev, shift, ntiles, hist);
-        k_scan_serial_chunks<<<1, 1024, 0, s>>>(hist, 256 * ntiles);
+        k_scan_tiles<<<nb, 1024, 0, s>>>(hist, len, partial);
+        k_scan_serial_chunks<<<1, 1024, 0, s>>>(partial, nb);
+        k_scan_add_tiles<<<nb, 1024, 0, s>>>(hist, len, partial);
         k_scatter<<<ntiles, kTile, 0, s>>>(keys, vals, n_dev, shift, ntiles, hist, k2, v2);
         uint32_t *tk = keys;
         keys = k2;
