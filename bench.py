@@ -355,6 +355,103 @@ def production_passage(steps=100):
     return out
 
 
+def component_rooflines(peak, n=1 << 24, n_merge=2_000_000):
+    """Achieved HBM bandwidth of the per-step kernel groups beside the fused
+    push/gather/deposit: (b) the standalone deposit, (c) the inside test, the
+    absorbed-set scan, the wall rows and points, the Furman emission and the
+    hole-refill / tail compaction, (d) the cell-binned merge (localRandom).
+    The microbench store (2^24 electrons, cell-sorted) is pushed once with a
+    20x longer step so that the electrons near the wall leave (about 2 %);
+    algorithmic bytes per kernel / its CUDA-event time."""
+    import torch
+    from openecloud_b200 import _lib
+    from openecloud_b200 import device as D
+    from openecloud_b200.grid import Grid
+    from openecloud_b200.particles import Particles
+    from openecloud_b200.particleBoundary import AbsorbRectangular
+    from openecloud_b200.particleEmitter import FurmanEmitter
+    from openecloud_b200.particleManagement import localRandom
+    s = torch.cuda.current_stream()
+    sh = s.cuda_stream
+
+    def timed(fn, reps=1):
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        for _ in range(reps):
+            fn()
+        b.record(s)
+        b.synchronize()
+        return a.elapsed_time(b) / reps
+
+    def line(name, nbytes, ms, what):
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        return {"kernel": name, "ms": ms, "alg_bytes": int(nbytes), "achieved_gbs": gbs, "frac": gbs / peak,
+                "bytes": what}
+
+    pd, E, (nx, ny, lx, ly) = workload(n, seed=7)
+    g = Grid(nx, ny, lx, ly, 0)
+    G = g.getNpExt()
+    P = Particles("electrons", "variableWeight", capacity=n)
+    P.setParticleData(pd)
+    P.setBConst([0.0, 0.5, 0.0])
+    bd = AbsorbRectangular(g, P)
+    et = P.fieldTable(g, E, 2)
+    P.pushGatherDeposit(g, et, 1e-11, 1, bd)
+    P._hole_buffers()
+    cg, cp, cb = g.c_grid(), P.c_particles(), bd.c_boundary()
+    rho, wsc, st = P._rho_fix.data_ptr(), P._wscale.data_ptr(), P._status.data_ptr()
+    out = []
+    ms = timed(lambda: _lib.call("oec_deposit", cg, cp, rho, wsc, 1, st, sh), reps=5)
+    out.append(line("deposit (oec_deposit)", 16 * n + 16 * G, ms, "cell, ox, oy, w per particle; grid clear + add"))
+    # a long step: the electrons within ~2 cells of the wall leave
+    P.pushGatherDeposit(g, et, 2e-10, 1, bd)
+    ms = timed(lambda: _lib.call("oec_index_inside", cg, cp, cb, P._mask.data_ptr(), st, sh), reps=5)
+    out.append(line("inside test (oec_index_inside)", 12.125 * n, ms, "cell, ox, oy per particle; absorbed bit"))
+    bd.ensure_buffers(n // 8)
+    L = _lib.lib()
+    ms = timed(lambda: _lib.call("oec_absorbed_index", cp, P._mask.data_ptr(), bd._index.data_ptr(),
+                                 bd._index.shape[0], bd._n_abs.data_ptr(), bd._scratch.data_ptr(), st, sh), reps=5)
+    n_abs = int(D.to_numpy(bd._n_abs)[0])
+    out.append(line("absorbed set (oec_absorbed_index)", n / 8 + 4 * n_abs, ms,
+                    f"absorbed bits; {n_abs} indices"))
+    cap = bd._rows.shape[0]
+    ms = timed(lambda: _lib.call("oec_save_absorbed", cg, cp, bd._index.data_ptr(), bd._n_abs.data_ptr(), cap,
+                                 bd._rows.data_ptr(), sh), reps=5)
+    out.append(line("absorbed rows (oec_save_absorbed)", (4 + 28 + 48) * n_abs, ms,
+                    "index, 7 fields gathered, one f64 row written per absorbed particle"))
+    ms = timed(lambda: _lib.call("oec_wall_interaction", cg, cb, 2e-10, bd._rows.data_ptr(), bd._n_abs.data_ptr(),
+                                 cap, bd._normals.data_ptr(), st, sh), reps=1)
+    out.append(line("wall point and normal (oec_wall_interaction)", (48 + 48 + 16) * n_abs, ms,
+                    "row read and written, normal written"))
+    em = FurmanEmitter(bd, P, seyMax=1.6, seed=5)
+    em.ensure_buffers(cap)
+    ms = timed(lambda: em._launch(cap, 0, None, None), reps=3)
+    n_sec = int(D.to_numpy(em._n_out)[0])
+    out.append(line("Furman emission (oec_furman_emit)", (48 + 16) * n_abs + 48 * n_sec, ms,
+                    f"row and normal per absorbed particle, row per secondary ({n_sec})"))
+    moved = min(n_abs, n_sec) + abs(n_sec - n_abs)
+    ms = timed(lambda: _lib.call("oec_add_remove", cg, cp, P._mask.data_ptr(), bd._index.data_ptr(),
+                                 bd._n_abs.data_ptr(), bd._index.shape[0], em._out.data_ptr(), em._n_out.data_ptr(),
+                                 em._out.shape[0], rho, wsc, P._scan_scratch.data_ptr(), st, sh), reps=1)
+    out.append(line("refill and compaction (oec_add_remove)", n / 8 + (48 + 28 + 16) * n_sec + 56 * moved, ms,
+                    "absorbed bits; per secondary a row read, 7 fields written, its deposit; per tail move "
+                    "28 B read + 28 B written"))
+    # (d) cell-binned merge of a 2e6-electron store over 10 % toward a 1.8e6 target
+    pm, _, _ = workload(n_merge, seed=9)
+    pm[:, 5] = np.random.default_rng(9).uniform(0.2, 2.0, n_merge) * 1e3
+    Q = Particles("electrons", "variableWeight", capacity=2 * n_merge)
+    Q.setParticleData(pm)
+    bq = AbsorbRectangular(g, Q)
+    Q._bind(g)
+    torch.cuda.synchronize()
+    ms = timed(lambda: localRandom(g, Q, bq, int(0.9 * n_merge), seed=3))
+    out.append(line("merge (localRandom: weight sort, split, cell-binned merge, compaction)", 48 * 2 * n_merge, ms,
+                    "rows read and written once per particle (the SURVEY's 48 B/particle/event); wall time of "
+                    "the whole call, host decisions included"))
+    return out
+
+
 BATCH = ("batched scan: 64 independent buildup runs drawn with seed 4 from {256, 512, 768, 1024}^2 grids over "
          "circular (R=20 mm) and elliptical (45x18 mm) chambers, deltaMax U(1.2, 2.0), 0.5e11-1.5e11 p/bunch, "
          "B_y 0-8.33 T, 1e4 initial electrons each, roulette cap 5e5 every 50 steps, dt=1e-11 s")
@@ -587,6 +684,11 @@ def run_ours(args, rank, world, local_rank):
              f"{production['poisson_solve']['lu_ms']:.2f} ms LU, {production['poisson_solve']['mg_cold_ms']:.2f} ms "
              f"MG-PCG cold, {production['poisson_solve']['mg_warm_ms']:.2f} ms warm")
 
+    components = None
+    if rank == 0 and world == 1 and not args.no_components:
+        components = component_rooflines(peak)
+        for c in components:
+            _log(f"{c['kernel']}: {c['ms']:.3f} ms, {c['achieved_gbs']:.0f} GB/s ({c['frac']:.2f} of peak)")
     batch = None
     if rank == 0 and world == 1 and not args.no_batch:
         batch = batched_scan()
@@ -617,6 +719,8 @@ def run_ours(args, rank, world, local_rank):
             line["production_passage"] = production
         if batch is not None:
             line["batched_scan"] = batch
+        if components is not None:
+            line["component_rooflines"] = components
         print(json.dumps(line), flush=True)
 
 
@@ -637,6 +741,8 @@ def main():
     ap.add_argument("--no-production", action="store_true",
                     help="skip the 1024x1024 production passage sample and solve comparison")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-run batched scan")
+    ap.add_argument("--no-components", action="store_true",
+                    help="skip the achieved bandwidth of the deposit, boundary, emission and merge kernels")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world = int(os.environ.get("WORLD_SIZE", "1"))

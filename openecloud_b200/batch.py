@@ -33,11 +33,20 @@ class BatchedBuildup:
     """runs: a list of keyword-argument dicts for `Buildup` (grid size,
     chamber, SEY, intensity, field, seed, ...); every run must use the same
     `management_every`.  branches: graph branch width (None: autotuned);
-    poisson: 'lu', 'mg' or None (autotuned per grid)."""
+    poisson: 'lu', 'mg' or None (autotuned per grid); shard: (rank, world)
+    to advance only this rank's share of the runs (one process per GPU, no
+    exchange until `gather_histories`)."""
 
-    def __init__(self, runs, branches=None, poisson=None, tuner=None):
+    def __init__(self, runs, branches=None, poisson=None, tuner=None, shard=None):
         if not runs:
             raise ValueError("no runs")
+        # one GPU of several: this process's share of the runs (shard_runs),
+        # their indices in `indices`; gather_histories collects them at the end
+        self.n_total = len(runs)
+        self.indices = list(range(len(runs))) if shard is None else shard_runs(runs, *shard)
+        runs = [runs[i] for i in self.indices]
+        if not runs:
+            raise ValueError("no runs in this shard")
         self.tuner = tuner or Autotuner()
         every = {int(r.get("management_every", 50)) for r in runs}
         if len(every) != 1:
@@ -200,4 +209,49 @@ def scan_configs(n=64, seed=4, cap=500_000, n_init=10_000, n_steps_table=2501, m
                         sey_max=float(rng.uniform(1.2, 2.0)), beam_particles=float(rng.uniform(0.5e11, 1.5e11)),
                         type_b_field=1 if by > 0 else 0, b_const=(0.0, by, 0.0), seed=1000 + i,
                         n_steps_table=n_steps_table, management_every=management_every))
+    return out
+
+
+def run_cost(cfg):
+    """Relative cost of one run's step: its grid nodes (the Poisson solve and
+    the per-node kernels) plus its macro-electron cap (the particle kernels)."""
+    nx, ny = cfg.get("nx", 128), cfg.get("ny", cfg.get("nx", 128))
+    return (nx + 2) * (ny + 2) + int(cfg.get("target", 100000))
+
+
+def shard_runs(runs, rank, world):
+    """The indices of the runs of `rank` out of `world`: each run, costliest
+    first, goes to the least loaded rank (ties to the lower rank), so every
+    rank gets a similar share of the work without any data exchange during
+    the runs."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("rank must be in [0, world)")
+    order = sorted(range(len(runs)), key=lambda i: (-run_cost(runs[i]), i))
+    load = [0] * world
+    mine = []
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        load[r] += run_cost(runs[i])
+        if r == rank:
+            mine.append(i)
+    return sorted(mine)
+
+
+def gather_histories(indices, histories, n_runs, group=None):
+    """Rank 0 receives every run's (macro count, sum of weights) history in
+    run order (other ranks get None): the one exchange of a sharded scan,
+    after the runs (torch.distributed, any backend)."""
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    local = list(zip(indices, [(np.asarray(n), np.asarray(w)) for n, w in histories]))
+    parts = [None] * world
+    dist.all_gather_object(parts, local, group=group)
+    if dist.get_rank(group) != 0:
+        return None
+    out = [None] * n_runs
+    for part in parts:
+        for i, h in part:
+            out[i] = h
+    if any(h is None for h in out):
+        raise RuntimeError("a run's history is missing")
     return out

@@ -78,3 +78,47 @@ def test_batched_multigrid_runs_and_autotuner(gpu):
     mg.run(steps)
     for b in mg.runs:
         assert b.ps.nFallbacks == 0 and b.ps.lastStats.converged == 1 and b.ps.lastStats.rel_residual <= 1e-8
+
+
+def test_shard_runs_balances_and_covers():
+    from openecloud_b200.batch import run_cost, scan_configs, shard_runs
+    runs = scan_configs(64)
+    for world in (1, 2, 3, 8):
+        parts = [shard_runs(runs, r, world) for r in range(world)]
+        assert sorted(i for p in parts for i in p) == list(range(64))
+        loads = [sum(run_cost(runs[i]) for i in p) for p in parts]
+        assert max(loads) - min(loads) <= max(run_cost(r) for r in runs)
+
+
+def _gather_worker(rank, world, port, runs, q):
+    import os
+    import torch.distributed as dist
+    from openecloud_b200.batch import gather_histories, shard_runs
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    mine = shard_runs(runs, rank, world)
+    hist = [(np.arange(5) + i, np.full(5, 10.0 * i)) for i in mine]  # stand-in histories
+    out = gather_histories(mine, hist, len(runs))
+    if rank == 0:
+        q.put([(int(n[0]), float(w[0])) for n, w in out])
+    dist.destroy_process_group()
+
+
+def test_gather_histories_two_ranks_gloo():
+    import socket
+    import torch.multiprocessing as mp
+    from openecloud_b200.batch import scan_configs
+    runs = scan_configs(10)
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_gather_worker, args=(r, 2, port, runs, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert got == [(i, 10.0 * i) for i in range(10)]
