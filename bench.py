@@ -444,11 +444,13 @@ def component_rooflines(peak, n=1 << 24, n_merge=2_000_000):
     Q.setParticleData(pm)
     bq = AbsorbRectangular(g, Q)
     Q._bind(g)
+    localRandom(g, Q, bq, int(0.9 * n_merge), seed=3)  # first call: work buffers
+    Q.setParticleData(pm)
     torch.cuda.synchronize()
     ms = timed(lambda: localRandom(g, Q, bq, int(0.9 * n_merge), seed=3))
     out.append(line("merge (localRandom: weight sort, split, cell-binned merge, compaction)", 48 * 2 * n_merge, ms,
-                    "rows read and written once per particle (the SURVEY's 48 B/particle/event); wall time of "
-                    "the whole call, host decisions included"))
+                    "rows read and written once per particle (48 B per particle and event); the whole call, "
+                    "its host decisions included, after a first call that sized the work buffers"))
     return out
 
 

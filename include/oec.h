@@ -371,6 +371,12 @@ int oec_weight_stats(const oec_particles_t *p, double *acc_dev, void *stream);
  * duplicates as rows (localRandom split, particleManagement.pyx:130-163). */
 int oec_split_rows(const oec_grid_t *grid, oec_particles_t *p, int32_t n, int32_t k, double *rows_dev, void *stream);
 
+/* _searchSorted (particleManagement.pyx:244-262) twice on the store sorted
+ * by weight (ascending): out_dev[0] / [1] = the reference's answer for lo /
+ * hi (the first index with w > value; 0 as soon as w[0] >= value; n when
+ * w[n-1] <= value). */
+int oec_weight_thresholds(const oec_particles_t *p, double lo, double hi, int32_t *out_dev, void *stream);
+
 /* Binned merge (localRandom :165-236): the first n_cand particles are
  * ordered along a 5-D Morton curve of their weighted phase-space coordinates
  * (x, y, lambda v; one scale for all axes); neighbouring pairs in that order

@@ -82,6 +82,7 @@ SIGNATURES = {
     "oec_roulette_select": [_I32, _I32, _P, _I64, ctypes.c_uint64, ctypes.c_uint32, _P, _P],
     "oec_clone_rows": [_PG, _PP, _I32, _I32, ctypes.c_uint64, ctypes.c_uint32, _P, _P],
     "oec_weight_stats": [_PP, _P, _P],
+    "oec_weight_thresholds": [_PP, _D, _D, _P, _P],
     "oec_split_rows": [_PG, _PP, _I32, _I32, _P, _P],
     "oec_cell_merge": [_PG, _PP, _I32, _I32, _D, _D, _I32, ctypes.c_uint64, ctypes.c_uint32, _D, _P, _P, _P, _P],
     "oec_rhs_with_beam": [_PG, _P, _P, _D, _P, _P, _P, _I32, _P, _P],

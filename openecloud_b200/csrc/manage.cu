@@ -190,6 +190,37 @@ __global__ void k_permute(oec_particles_t p, const int32_t *__restrict__ perm, o
     if (blockIdx.x == 0 && threadIdx.x == 0) *q.count = n;
 }
 
+// ------------------------------------------------------- weight search
+// _searchSorted (particleManagement.pyx:244-262) on the weight-sorted store,
+// one thread per threshold, the reference's loop as written (it answers 0 as
+// soon as a[0] >= value): the first index with a[i] > value.
+__global__ void k_search_sorted2(const float *__restrict__ w, const int32_t *count, double lo, double hi,
+                                 int32_t *out) {
+    const int t = threadIdx.x;
+    if (t > 1) return;
+    const double value = t == 0 ? lo : hi;
+    const int n = *count;
+    int r;
+    if (n <= 0) {
+        r = 0;
+    } else if ((double)w[n - 1] <= value) {
+        r = n;
+    } else if ((double)w[0] >= value) {
+        r = 0;
+    } else {
+        int i0 = 0, i2 = n - 1, i1 = (int)((i2 + i0) * 0.5);
+        while (i1 != i0) {
+            if ((double)w[i1] > value)
+                i2 = i1;
+            else
+                i0 = i1;
+            i1 = (int)((i2 + i0) * 0.5);
+        }
+        r = i1 + 1;
+    }
+    out[t] = r;
+}
+
 // -------------------------------------------------------------- roulette
 
 __global__ void k_scale_w(oec_particles_t p, double factor) {
@@ -506,6 +537,14 @@ extern "C" int oec_sort_particles(oec_particles_t *p, oec_particles_t *tmp, int3
     int rc = radix_sort(keys, vals, k2, v2, hist, p->count, cap, bits, s, &kout, &vout);
     if (rc != OEC_OK) return rc;
     k_permute<<<g, 256, 0, s>>>(*p, vout, *tmp);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int oec_weight_thresholds(const oec_particles_t *p, double lo, double hi, int32_t *out_dev,
+                                     void *stream) {
+    if (!vp2(p) || !out_dev) return OEC_ERR_INVALID;
+    k_search_sorted2<<<1, 32, 0, as_stream(stream)>>>(p->w, p->count, lo, hi, out_dev);
     OEC_LAUNCH_CHECK();
     return OEC_OK;
 }

@@ -29,24 +29,6 @@ def _next_call():
     return _CALLS["n"]
 
 
-def _search_sorted(a, value):
-    """particleManagement.pyx:244-262 (first index with a[i] > value)."""
-    n = a.shape[0]
-    if a[n - 1] <= value:
-        return n
-    if a[0] >= value:
-        return 0
-    i0, i2 = 0, n - 1
-    i1 = int((i2 + i0) * 0.5)
-    while i1 != i0:
-        if a[i1] > value:
-            i2 = i1
-        else:
-            i0 = i1
-        i1 = int((i2 + i0) * 0.5)
-    return i1 + 1
-
-
 def _mask_clear(P):
     fails = D.zeros(1, torch.int32)
     _lib.call("oec_roulette_select", 0, 0, P._mask.data_ptr(), P._mask.shape[0], 0, 0, fails.data_ptr(),
@@ -92,9 +74,13 @@ def localRandom(gridObj, particlesObj, particleBoundaryObj, targetMacroParticleC
     maxT, minT = thresholdFactor * goal, goal / thresholdFactor
     ds = min(gridObj.getDx(), gridObj.getDy())
     P.sortByColumn(5)
-    w = P._soa["w"][:n].double().cpu().numpy()
-    to_merge = _search_sorted(w, minT)
-    to_split = n - _search_sorted(w, maxT)
+    # the two _searchSorted thresholds on the device: 8 bytes come back
+    # instead of the weight array
+    thr = D.zeros(2, torch.int32)
+    _lib.call("oec_weight_thresholds", P.c_particles(), float(minT), float(maxT), thr.data_ptr(), s)
+    lo_idx, hi_idx = (int(x) for x in D.to_numpy(thr))
+    to_merge = lo_idx
+    to_split = n - hi_idx
     if 2 * to_merge + to_split >= n:
         f = 0.95 * n / (2 * to_merge + to_split)
         to_merge, to_split = int(to_merge * f), int(to_split * f)

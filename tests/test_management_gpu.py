@@ -91,3 +91,45 @@ def test_local_random_statistics(gpu, scheme, tag, target):
         return 0.5 * ME / QE * np.sum(np.sum(a[:, 2:5] ** 2, 1) * a[:, 5]) / np.sum(a[:, 5])
     if scheme == 0:
         assert abs(ekin(after) / ekin(before) - 1) < 0.05
+
+
+def _search_sorted_ref(a, value):
+    # particleManagement.pyx:244-262 as written
+    n = a.shape[0]
+    if a[n - 1] <= value:
+        return n
+    if a[0] >= value:
+        return 0
+    i0, i2 = 0, n - 1
+    i1 = int((i2 + i0) * 0.5)
+    while i1 != i0:
+        if a[i1] > value:
+            i2 = i1
+        else:
+            i0 = i1
+        i1 = int((i2 + i0) * 0.5)
+    return i1 + 1
+
+
+def test_weight_thresholds_match_reference_search(gpu):
+    import torch
+    from openecloud_b200 import _lib
+    from openecloud_b200 import device as D
+    from openecloud_b200.grid import Grid
+    from openecloud_b200.particles import Particles
+    rng = np.random.default_rng(8)
+    n = 5000
+    pd = np.zeros((n, 6))
+    pd[:, 0] = rng.uniform(-0.01, 0.01, n)
+    pd[:, 1] = rng.uniform(-0.01, 0.01, n)
+    pd[:, 5] = np.round(rng.uniform(0.5, 3.0, n), 2)  # ties
+    P = Particles("electrons", "variableWeight")
+    P.setParticleData(pd)
+    P._bind(Grid(64, 64, 0.04, 0.04, 1))
+    P.sortByColumn(5)
+    w = D.to_numpy(P._soa["w"][:n]).astype(np.float64)
+    thr = D.zeros(2, torch.int32)
+    for lo, hi in [(1.0, 2.0), (0.1, 9.0), (w[0], w[-1]), (w[17], w[4000]), (1.5, 1.5), (-1.0, 0.4)]:
+        _lib.call("oec_weight_thresholds", P.c_particles(), float(lo), float(hi), thr.data_ptr(), D.stream())
+        got = tuple(int(x) for x in D.to_numpy(thr))
+        assert got == (_search_sorted_ref(w, lo), _search_sorted_ref(w, hi)), (lo, hi, got)
