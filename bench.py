@@ -254,7 +254,7 @@ def gpu_passage():
 
 PRODUCTION = ("production buildup (sampled): 1024x1024 grid over an elliptical chamber with half-axes 45x18 mm, "
               "dipole B_y=8.33 T, 25 ns train of 1.15e11 p/bunch (sigma_r 1 mm, sigma_t 0.25 ns), SEY deltaMax 1.8, "
-              "2e6 initial macro-electrons, kd-tree merge (localRandom) toward 2e6 every 10 steps, dt=5e-12 s; "
+              "2.2e6 initial macro-electrons, kd-tree merge (localRandom) toward 2e6 every 10 steps, dt=5e-12 s; "
               "one bunch passage = 5000 steps")
 
 
@@ -331,7 +331,7 @@ def production_passage(steps=100):
     shared), scaled to a 5000-step passage; plus the config-5 solve
     comparison on the same 1024x1024 elliptical grid."""
     from openecloud_b200.buildup import Buildup
-    kw = dict(nx=1024, ny=1024, lx=0.09, ly=0.036, boundType=1, n_init=2_000_000, w_init=1e3, dt=5e-12,
+    kw = dict(nx=1024, ny=1024, lx=0.09, ly=0.036, boundType=1, n_init=2_200_000, w_init=1e3, dt=5e-12,
               beam_particles=1.15e11, radius_sigma=1e-3, sey_max=1.8, type_b_field=1, b_const=(0., 8.33, 0.),
               target=2_000_000, management="local", management_every=10, n_steps_table=steps + 1, seed=2000)
     t0 = time.perf_counter()
@@ -343,6 +343,7 @@ def production_passage(steps=100):
     t_lu = lu.run(steps)
     out["s_per_passage_lu"] = t_lu / steps * 5000
     out["final_macro_particles_lu"] = int(lu.history()[0][-1])
+    out["management_events_lu"] = lu.n_managed
     m = Buildup(poisson=lu.ps, **kw)
     m.ps.method, m.ps.precond = "pcg", "mg"
     fb0 = m.ps.nFallbacks
@@ -350,6 +351,7 @@ def production_passage(steps=100):
     out["s_per_passage_pcg_mg"] = t_mg / steps * 5000
     out["pcg_mg_fallbacks"] = m.ps.nFallbacks - fb0
     out["final_macro_particles_pcg_mg"] = int(m.history()[0][-1])
+    out["management_events_pcg_mg"] = m.n_managed
     out["timing"] = (f"device time (CUDA events) of the first {steps} steps (management and graph captures "
                      "included) x 5000/steps")
     return out

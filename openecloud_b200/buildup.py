@@ -136,6 +136,7 @@ class Buildup:
         _lib.call("oec_history", self.P.c_particles(), self.step_dev.data_ptr(), self._table_len,
                   self.hist_w.data_ptr(), self.hist_n.data_ptr(), self.scratch.data_ptr(), D.stream())
         self.graph = None
+        self.n_managed = 0       # management events (roulette / merge) so far
         self._graph_sig = None
         self._cap_stream = None
         self.steps_done = 0
@@ -191,6 +192,7 @@ class Buildup:
             else:
                 return False
             self._prepare_deposit()
+            self.n_managed += 1
             return True
         return False
 
