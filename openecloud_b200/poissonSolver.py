@@ -220,12 +220,18 @@ def _level_lists(lev, nlevels):
     return order, ptr
 
 
-def choose_tail(Lcsr, Ucsr, n, launch_us=1.5, gbs=3000.0, max_tail=12288):
+def choose_tail(Lcsr, Ucsr, n, launch_us=8.0, gbs=6000.0, max_tail=16384):
     """Rows handed to the dense tail: minimise the estimated solve time
-    2*levels(head)*launch + 2*(m^2*8 B)/bandwidth over a few candidates."""
+    levels(head) * per-level cost + 2 * (m^2 * 8 B) / bandwidth over a few
+    candidates.  The per-level cost (8 us) and the bandwidth of the dense
+    products were measured on the B200 (128^2 to 1024^2); max_tail bounds the
+    two dense inverses (2 * m^2 * 8 B: 4.3 GB at 16384), and the tail stays
+    within a quarter of the unknowns: on a small grid a larger one streams
+    more through L2 each step than it saves (a 128^2 buildup step ran slower
+    with 6144 tail rows than with 3072 although the solve alone tied)."""
     best = (None, 0)
-    for m in [0, 256, 512, 1024, 2048, 3072, 4096, 6144, 8192, 12288]:
-        if m > min(n, max_tail):
+    for m in [0, 256, 512, 1024, 2048, 3072, 4096, 6144, 8192, 12288, 16384]:
+        if m > min(n // 4, max_tail):
             continue
         h = n - m
         _, nl = _levels(Lcsr, True, h, nrows=h)
