@@ -395,6 +395,9 @@ int oec_cell_merge(const oec_grid_t *grid, oec_particles_t *p, int32_t n_cand, i
 /* Device form of SuperLU's P_r A P_c = L U (poissonSolver.pyx:59).
  * Rows [0, head) of each factor are solved level by level; the last
  * m = n - head rows ("tail") use dense inverses of their triangular blocks.
+ * The head CSR of each factor is stored in level order: its row w is factor
+ * row l_rows[w] (u_rows[w]), and level k holds rows [level_ptr[k],
+ * level_ptr[k+1]) of that order; column indices are factor row numbers.
  * Level pointers are HOST arrays (the launch loop runs on the host); every
  * other pointer is a device pointer. */
 typedef struct oec_lu {
@@ -407,16 +410,27 @@ typedef struct oec_lu {
     int32_t l_nlevels;
     const int32_t *l_level_ptr;/* HOST [l_nlevels+1] */
     const int32_t *l_rows;     /* [head] head rows of L ordered by level */
-    const int32_t *l_ptr, *l_idx; const double *l_val;    /* strict lower L, rows [0,head) */
+    const int32_t *l_ptr, *l_idx; const double *l_val;    /* strict lower L, head rows in level order */
     const int32_t *lc_ptr, *lc_idx; const double *lc_val; /* L[tail, head] */
     const double *tl_inv;      /* [m*m] inverse of unit-lower L[tail,tail], row-major */
     int32_t u_nlevels;
     const int32_t *u_level_ptr;/* HOST [u_nlevels+1], backward order */
     const int32_t *u_rows;     /* [head] */
-    const int32_t *u_ptr, *u_idx; const double *u_val;    /* strict upper U, rows [0,head) */
-    const double *u_diag;      /* [head] */
+    const int32_t *u_ptr, *u_idx; const double *u_val;    /* strict upper U, head rows in level order */
+    const double *u_diag;      /* [head] diagonal of U, in level order */
     const double *tu_inv;      /* [m*m] inverse of U[tail,tail], row-major */
+    int32_t head_path;         /* how the head levels run: OEC_LU_HEAD_* (0: chosen by size) */
 } oec_lu_t;
+
+/* Head-level execution of oec_lu_solve.  AUTO: COOPERATIVE when both factors
+ * have at most 64 head levels, else PER_LEVEL.  ONE_CTA (n <= 28672 and at
+ * most 64 levels) is taken only when asked for: it ties with COOPERATIVE on a
+ * warm L2 and is slower when the factors come from HBM.  A path that does not
+ * fit falls back as AUTO does. */
+#define OEC_LU_HEAD_AUTO 0
+#define OEC_LU_HEAD_PER_LEVEL 1    /* one launch per level, a warp per row */
+#define OEC_LU_HEAD_COOPERATIVE 2  /* one cooperative launch per factor, grid barrier between levels */
+#define OEC_LU_HEAD_ONE_CTA 3      /* one CTA per factor, the vector in shared memory */
 
 /* phi = A^-1 q on the inside nodes, 0 elsewhere (poissonSolver.pyx:85).
  * q_dev, phi_dev: [n_nodes]; work_dev: n + (n - head) doubles. */

@@ -9,11 +9,12 @@
 // Triangular solves.  The factors of a 2-D FIT operator under a minimum-degree
 // ordering have a wide bottom (many independent rows per dependency level)
 // and a long thin top: the separator rows, one or two rows per level.  The
-// rows are split at setup into a "head", solved level by level with one
-// warp per row (one launch per level), and a "tail" of the last m rows,
-// whose triangular block is inverted densely at setup and applied as a
-// matrix-vector product, turning hundreds of one-row levels into one
-// bandwidth-bound pass.
+// rows are split at setup into a "head", solved level by level, and a
+// "tail" of the last m rows, whose triangular block is inverted densely at
+// setup and applied as a matrix-vector product, turning hundreds of one-row
+// levels into one bandwidth-bound pass.  The head levels run in one
+// cooperative launch when they are few, else one launch per level (or, on
+// request, in one CTA with the vector in shared memory).
 #include <math.h>
 #include <stdint.h>
 
@@ -29,22 +30,26 @@ namespace {
 
 constexpr int kWarps = 8;  // warps per CTA in the row kernels
 
-// x[r] = (x[r] - sum_j A[r,j] x[j]) / d[r] for the rows of one level.
+// The head CSR is stored in level order: position w holds factor row
+// rows[w] (its entries ptr[w]..ptr[w+1], its diagonal diag[w]), so a row's
+// record is read with independent loads rather than through rows[w].
+//
+// x[r] = (x[r] - sum_j A[r,j] x[j]) / d[r] for the rows [w0, w1) of one level.
 __global__ void __launch_bounds__(kWarps * 32)
-    k_trsv_rows(const int32_t *__restrict__ rows, int nrows, const int32_t *__restrict__ ptr,
+    k_trsv_rows(const int32_t *__restrict__ rows, int w0, int w1, const int32_t *__restrict__ ptr,
                 const int32_t *__restrict__ idx, const double *__restrict__ val, const double *__restrict__ diag,
                 double *__restrict__ x) {
-    int w = blockIdx.x * kWarps + (threadIdx.x >> 5);
-    int lane = threadIdx.x & 31;
-    if (w >= nrows) return;
-    int r = rows[w];
+    const int w = w0 + blockIdx.x * kWarps + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (w >= w1) return;
+    const int r = rows[w], k1 = ptr[w + 1];
     double s = 0.0;
-    for (int k = ptr[r] + lane; k < ptr[r + 1]; k += 32) s += val[k] * x[idx[k]];
+    for (int k = ptr[w] + lane; k < k1; k += 32) s += val[k] * x[idx[k]];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFullMask, s, o);
     if (lane == 0) {
         double v = x[r] - s;
-        x[r] = diag ? v / diag[r] : v;
+        x[r] = diag ? v / diag[w] : v;
     }
 }
 
@@ -72,24 +77,126 @@ __global__ void __launch_bounds__(kWarps * 32)
     const int w0 = blockIdx.x * kWarps + (threadIdx.x >> 5), nw = gridDim.x * kWarps;
     for (int l = 0; l < lv.n; ++l) {
         for (int w = lv.ptr[l] + w0; w < lv.ptr[l + 1]; w += nw) {
-            const int r = rows[w];
+            const int r = rows[w], k1 = ptr[w + 1];
             double s = 0.0;
-            for (int k = ptr[r] + lane; k < ptr[r + 1]; k += 32) s += val[k] * __ldcg(&x[idx[k]]);
+            for (int k = ptr[w] + lane; k < k1; k += 32) s += val[k] * __ldcg(&x[idx[k]]);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFullMask, s, o);
             if (lane == 0) {
                 const double v = __ldcg(&x[r]) - s;
-                x[r] = diag ? v / diag[r] : v;
+                x[r] = diag ? v / diag[w] : v;
             }
         }
         if (l + 1 < lv.n) grid.sync();
     }
 }
 
-// y[row0 + i] = b[row0 + i] - sum_j C[i,j] x[j]   (tail coupling to the head)
+// Small systems (every unknown fits one CTA's shared memory as f64), on
+// request: each triangle is solved by one 1024-thread CTA with the solution
+// vector in shared memory and __syncthreads between the levels, a fraction of
+// a grid barrier's cost.  One SM has too few loads in flight for the factors'
+// entries, though: at 128^2 (12644 unknowns, 20 levels) it ties with the
+// cooperative launch on a warm L2 (0.172 against 0.166 ms) and loses inside a
+// buildup step, where the other kernels have evicted the factors (2500 steps:
+// 0.78 against 0.71 s), so the automatic choice does not take it.  A level's rows are spread over the CTA with g lanes per
+// row, g the largest power of two up to 32 that keeps the level in one pass
+// (1 for the wide bottom levels; the narrow top levels have the long rows).
+// A level's cost is the latency of its loads, so the record of a thread's
+// first row in the next level (row, entry range, diagonal; none of it
+// depends on x) is loaded while the current level computes.
+constexpr int kBlockThreads = 1024;
+constexpr int kBlockMaxRows = 28672;  // 224 KB of f64
+
+struct RowRec {
+    int r, k0, k1;
+    double d;
+};
+
+__device__ __forceinline__ int level_lanes(int nrows) {
+    int g = 1;
+    while (g < 32 && nrows * (2 * g) <= kBlockThreads) g *= 2;
+    return g;
+}
+
+__device__ __forceinline__ RowRec row_rec(int w, int w1, const int32_t *__restrict__ rows,
+                                          const int32_t *__restrict__ ptr, const double *__restrict__ diag) {
+    RowRec rc{-1, 0, 0, 1.0};
+    if (w < w1) {
+        rc.r = rows[w];
+        rc.k0 = ptr[w];
+        rc.k1 = ptr[w + 1];
+        if (diag) rc.d = diag[w];
+    }
+    return rc;
+}
+
+__device__ __forceinline__ void block_levels(const int32_t *__restrict__ rows, const LevelPtr &lv, int l0,
+                                             const int32_t *__restrict__ ptr, const int32_t *__restrict__ idx,
+                                             const double *__restrict__ val, const double *__restrict__ diag,
+                                             double *xs) {
+    if (l0 >= lv.n) return;
+    int g = level_lanes(lv.ptr[l0 + 1] - lv.ptr[l0]);
+    RowRec nxt = row_rec(lv.ptr[l0] + (int)threadIdx.x / g, lv.ptr[l0 + 1], rows, ptr, diag);
+    for (int l = l0; l < lv.n; ++l) {
+        const int r0 = lv.ptr[l], r1 = lv.ptr[l + 1];
+        const int sub = threadIdx.x & (g - 1), groups = kBlockThreads / g;
+        RowRec cur = nxt;
+        const int gn = l + 1 < lv.n ? level_lanes(lv.ptr[l + 2] - lv.ptr[l + 1]) : 1;
+        if (l + 1 < lv.n) nxt = row_rec(lv.ptr[l + 1] + (int)threadIdx.x / gn, lv.ptr[l + 2], rows, ptr, diag);
+        for (int base = r0; base < r1; base += groups) {  // same trip count in every thread
+            if (base != r0) cur = row_rec(base + (int)threadIdx.x / g, r1, rows, ptr, diag);
+            double s = 0.0;
+            for (int k = cur.k0 + sub; k < cur.k1; k += g) s += val[k] * xs[idx[k]];
+            for (int o = g >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(kFullMask, s, o);
+            if (cur.r >= 0 && sub == 0) {
+                const double v = xs[cur.r] - s;
+                xs[cur.r] = diag ? v / cur.d : v;
+            }
+        }
+        g = gn;
+        __syncthreads();
+    }
+}
+
+// Forward half: gather the permuted right-hand side (c = P_r q), solve the
+// unit-lower head and write y_head to c[0, h) (the tail's rows of c keep
+// their right-hand side).  The first level of a strictly lower triangle has
+// no entries (any entry would be a dependency), so it is skipped.
+__global__ void __launch_bounds__(kBlockThreads)
+    k_lu_block_lower(int n, int h, const int32_t *__restrict__ rhs_node, const double *__restrict__ q,
+                     const int32_t *__restrict__ rows, LevelPtr lv, const int32_t *__restrict__ ptr,
+                     const int32_t *__restrict__ idx, const double *__restrict__ val, double *__restrict__ c) {
+    extern __shared__ double xs[];
+#pragma unroll 4
+    for (int i = threadIdx.x; i < n; i += kBlockThreads) xs[i] = q[rhs_node[i]];
+    __syncthreads();
+    block_levels(rows, lv, 1, ptr, idx, val, nullptr, xs);
+#pragma unroll 4
+    for (int i = threadIdx.x; i < n; i += kBlockThreads) c[i] = xs[i];
+}
+
+// Backward half: z_head from y_head (c[0, h)) and the solved tail (z_tail),
+// then phi[node of unknown i] = z[perm_c[i]] straight from shared memory.
+__global__ void __launch_bounds__(kBlockThreads)
+    k_lu_block_upper(int n, int h, const double *__restrict__ c, const double *__restrict__ ztail,
+                     const int32_t *__restrict__ rows, LevelPtr lv, const int32_t *__restrict__ ptr,
+                     const int32_t *__restrict__ idx, const double *__restrict__ val,
+                     const double *__restrict__ diag, const int32_t *__restrict__ sol_src,
+                     const int32_t *__restrict__ sol_node, double *__restrict__ phi) {
+    extern __shared__ double xs[];
+#pragma unroll 4
+    for (int i = threadIdx.x; i < n; i += kBlockThreads) xs[i] = i < h ? c[i] : ztail[i - h];
+    __syncthreads();
+    block_levels(rows, lv, 0, ptr, idx, val, diag, xs);
+#pragma unroll 4
+    for (int i = threadIdx.x; i < n; i += kBlockThreads) phi[sol_node[i]] = xs[sol_src[i]];
+}
+
+// t[i] = b[i] - sum_j C[i,j] x[j]   (the tail's right-hand side after the head)
 __global__ void __launch_bounds__(kWarps * 32)
-    k_spmv_sub(int nrows, const int32_t *__restrict__ ptr, const int32_t *__restrict__ idx,
-               const double *__restrict__ val, const double *__restrict__ x, double *__restrict__ y) {
+    k_spmv_rhs(int nrows, const int32_t *__restrict__ ptr, const int32_t *__restrict__ idx,
+               const double *__restrict__ val, const double *__restrict__ x, const double *__restrict__ b,
+               double *__restrict__ t) {
     int w = blockIdx.x * kWarps + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
     if (w >= nrows) return;
@@ -97,7 +204,7 @@ __global__ void __launch_bounds__(kWarps * 32)
     for (int k = ptr[w] + lane; k < ptr[w + 1]; k += 32) s += val[k] * x[idx[k]];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFullMask, s, o);
-    if (lane == 0) y[w] -= s;
+    if (lane == 0) t[w] = b[w] - s;
 }
 
 // out[i] = sum_{j in tri(i)} T[i*m + j] in[j]; lower: j <= i, upper: j >= i.
@@ -158,10 +265,47 @@ using namespace oec;
 namespace oec {
 namespace {
 
-// The levels of one triangle: one cooperative launch when they fit the
-// parameter block and the device allows it, else one launch per level.
+LevelPtr level_ptrs(const int32_t *level_ptr, int nlevels) {
+    LevelPtr lv;
+    lv.n = nlevels;
+    for (int l = 0; l <= nlevels; ++l) lv.ptr[l] = level_ptr[l];
+    return lv;
+}
+
+// The whole solve of a small system (n <= kBlockMaxRows, both triangles of at
+// most kCoopMaxLevels head levels): the two one-CTA triangle kernels around
+// the tail's right-hand side and its two dense products.
+int lu_solve_block(const oec_lu_t *lu, const double *q, double *phi, double *c, double *t, cudaStream_t s) {
+    const int n = lu->n, h = lu->head, m = n - h;
+    const size_t smem = sizeof(double) * (size_t)n;
+    static size_t attr_set = 0;  // largest dynamic shared-memory size enabled so far
+    if (smem > 48 * 1024 && smem > attr_set) {
+        OEC_CUDA_TRY(cudaFuncSetAttribute(k_lu_block_lower, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        OEC_CUDA_TRY(cudaFuncSetAttribute(k_lu_block_upper, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = smem;
+    }
+    OEC_CUDA_TRY(cudaMemsetAsync(phi, 0, sizeof(double) * (size_t)lu->n_nodes, s));
+    k_lu_block_lower<<<1, kBlockThreads, smem, s>>>(n, h, lu->rhs_node, q, lu->l_rows,
+                                                    level_ptrs(lu->l_level_ptr, lu->l_nlevels), lu->l_ptr, lu->l_idx,
+                                                    lu->l_val, c);
+    if (m > 0) {
+        k_spmv_rhs<<<warp_blocks(m), kWarps * 32, 0, s>>>(m, lu->lc_ptr, lu->lc_idx, lu->lc_val, c, c + h, t);
+        k_dense_tri<true><<<m, 256, 0, s>>>(m, lu->tl_inv, t, c + h);   // y_tail
+        k_dense_tri<false><<<m, 256, 0, s>>>(m, lu->tu_inv, c + h, t);  // z_tail
+    }
+    k_lu_block_upper<<<1, kBlockThreads, smem, s>>>(n, h, c, t, lu->u_rows,
+                                                    level_ptrs(lu->u_level_ptr, lu->u_nlevels), lu->u_ptr, lu->u_idx,
+                                                    lu->u_val, lu->u_diag, lu->sol_src, lu->sol_node, phi);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+// The levels of one triangle: one cooperative launch when `coop` asks for it,
+// they fit the parameter block and the device allows it, else one launch per
+// level.
 int solve_levels(const int32_t *rows, const int32_t *level_ptr, int nlevels, const int32_t *ptr,
-                 const int32_t *idx, const double *val, const double *diag, double *x, cudaStream_t s) {
+                 const int32_t *idx, const double *val, const double *diag, double *x, bool coop_ok,
+                 cudaStream_t s) {
     if (nlevels <= 0) return OEC_OK;
     static int per_sm = -1;  // resident CTAs per SM of the cooperative kernel (0: no cooperative launch)
     if (per_sm < 0) {
@@ -173,11 +317,9 @@ int solve_levels(const int32_t *rows, const int32_t *level_ptr, int nlevels, con
             per_sm = 0;
         cudaGetLastError();
     }
-    if (per_sm > 0 && nlevels <= kCoopMaxLevels) {
-        LevelPtr lv;
-        lv.n = nlevels;
+    if (coop_ok && per_sm > 0 && nlevels <= kCoopMaxLevels) {
+        LevelPtr lv = level_ptrs(level_ptr, nlevels);
         int widest = 0;
-        for (int l = 0; l <= nlevels; ++l) lv.ptr[l] = level_ptr[l];
         for (int l = 0; l < nlevels; ++l) widest = std::max(widest, level_ptr[l + 1] - level_ptr[l]);
         // one CTA per SM: a wider grid makes every barrier dearer than the
         // extra warps save on the few wide levels
@@ -189,7 +331,7 @@ int solve_levels(const int32_t *rows, const int32_t *level_ptr, int nlevels, con
     }
     for (int l = 0; l < nlevels; ++l) {
         const int r0 = level_ptr[l], r1 = level_ptr[l + 1];
-        k_trsv_rows<<<warp_blocks(r1 - r0), kWarps * 32, 0, s>>>(rows + r0, r1 - r0, ptr, idx, val, diag, x);
+        k_trsv_rows<<<warp_blocks(r1 - r0), kWarps * 32, 0, s>>>(rows, r0, r1, ptr, idx, val, diag, x);
     }
     OEC_LAUNCH_CHECK();
     return OEC_OK;
@@ -207,23 +349,29 @@ extern "C" int oec_lu_solve(const oec_lu_t *lu, const double *q_dev, double *phi
     cudaStream_t s = as_stream(stream);
     double *c = work_dev;      // n: right-hand side, then y, then z (in place)
     double *t = work_dev + n;  // m: tail scratch
+    const int path = lu->head_path;
+    if (path < OEC_LU_HEAD_AUTO || path > OEC_LU_HEAD_ONE_CTA) return OEC_ERR_INVALID;
+    const bool few_levels = lu->l_nlevels <= kCoopMaxLevels && lu->u_nlevels <= kCoopMaxLevels;
+    if (path == OEC_LU_HEAD_ONE_CTA && n <= kBlockMaxRows && few_levels)
+        return lu_solve_block(lu, q_dev, phi_dev, c, t, s);
+    const bool coop = path != OEC_LU_HEAD_PER_LEVEL;
     k_lu_gather<<<persistent_grid((n + 255) / 256, 4), 256, 0, s>>>(n, lu->rhs_node, q_dev, c);
     OEC_LAUNCH_CHECK();
     // forward, head levels (unit lower: no diagonal)
-    int rc = solve_levels(lu->l_rows, lu->l_level_ptr, lu->l_nlevels, lu->l_ptr, lu->l_idx, lu->l_val, nullptr, c, s);
+    int rc = solve_levels(lu->l_rows, lu->l_level_ptr, lu->l_nlevels, lu->l_ptr, lu->l_idx, lu->l_val, nullptr, c,
+                          coop, s);
     if (rc != OEC_OK) return rc;
     if (m > 0) {
-        // t = c_tail - L[tail, head] y_head ; y_tail = TLinv t
-        OEC_CUDA_TRY(cudaMemcpyAsync(t, c + h, sizeof(double) * m, cudaMemcpyDeviceToDevice, s));
-        k_spmv_sub<<<warp_blocks(m), kWarps * 32, 0, s>>>(m, lu->lc_ptr, lu->lc_idx, lu->lc_val, c, t);
+        // t = c_tail - L[tail, head] y_head ; y_tail = TLinv t ; z_tail = TUinv y_tail
+        k_spmv_rhs<<<warp_blocks(m), kWarps * 32, 0, s>>>(m, lu->lc_ptr, lu->lc_idx, lu->lc_val, c, c + h, t);
         k_dense_tri<true><<<m, 256, 0, s>>>(m, lu->tl_inv, t, c + h);
-        // z_tail = TUinv y_tail
-        OEC_CUDA_TRY(cudaMemcpyAsync(t, c + h, sizeof(double) * m, cudaMemcpyDeviceToDevice, s));
-        k_dense_tri<false><<<m, 256, 0, s>>>(m, lu->tu_inv, t, c + h);
+        k_dense_tri<false><<<m, 256, 0, s>>>(m, lu->tu_inv, c + h, t);
+        OEC_CUDA_TRY(cudaMemcpyAsync(c + h, t, sizeof(double) * m, cudaMemcpyDeviceToDevice, s));
         OEC_LAUNCH_CHECK();
     }
     // backward, head levels (rows use every column > row, tail included)
-    rc = solve_levels(lu->u_rows, lu->u_level_ptr, lu->u_nlevels, lu->u_ptr, lu->u_idx, lu->u_val, lu->u_diag, c, s);
+    rc = solve_levels(lu->u_rows, lu->u_level_ptr, lu->u_nlevels, lu->u_ptr, lu->u_idx, lu->u_val, lu->u_diag, c,
+                      coop, s);
     if (rc != OEC_OK) return rc;
     OEC_CUDA_TRY(cudaMemsetAsync(phi_dev, 0, sizeof(double) * (size_t)lu->n_nodes, s));
     k_lu_scatter<<<persistent_grid((n + 255) / 256, 4), 256, 0, s>>>(n, lu->sol_src, lu->sol_node, c, phi_dev);

@@ -36,7 +36,8 @@ class LU_t(ctypes.Structure):
                 ("l_nlevels", ctypes.c_int32), ("l_level_ptr", _P), ("l_rows", _P),
                 ("l_ptr", _P), ("l_idx", _P), ("l_val", _P), ("lc_ptr", _P), ("lc_idx", _P), ("lc_val", _P),
                 ("tl_inv", _P), ("u_nlevels", ctypes.c_int32), ("u_level_ptr", _P), ("u_rows", _P),
-                ("u_ptr", _P), ("u_idx", _P), ("u_val", _P), ("u_diag", _P), ("tu_inv", _P)]
+                ("u_ptr", _P), ("u_idx", _P), ("u_val", _P), ("u_diag", _P), ("tu_inv", _P),
+                ("head_path", ctypes.c_int32)]
 
 
 class Stencil_t(ctypes.Structure):
@@ -443,6 +444,7 @@ class PoissonSolver:
         lev, nl = _levels(Lh, True, h)
         rows, lptr = _level_lists(lev, nl)
         k["l_rows"] = dev(rows)
+        Lh = Lh[rows]  # level order: a row's record is read at its position in the level
         k["l_ptr"], k["l_idx"], k["l_val"] = dev(Lh.indptr), dev(Lh.indices), dev(Lh.data, torch.float64)
         self._l_level_ptr = lptr
         # strict upper U, head rows (all columns > row, tail columns included)
@@ -451,8 +453,9 @@ class PoissonSolver:
         levu, nu = _levels(Uh, False, h)
         rowsu, uptr = _level_lists(levu, nu)
         k["u_rows"] = dev(rowsu)
+        Uh = Uh[rowsu]
         k["u_ptr"], k["u_idx"], k["u_val"] = dev(Uh.indptr), dev(Uh.indices), dev(Uh.data, torch.float64)
-        k["u_diag"] = dev(Uc.diagonal()[:h], torch.float64) if h > 0 else D.zeros(1, torch.float64)
+        k["u_diag"] = dev(Uc.diagonal()[:h][rowsu], torch.float64) if h > 0 else D.zeros(1, torch.float64)
         self._u_level_ptr = uptr
         if m > 0:
             C = Lc[h:, :h].tocsr()

@@ -55,3 +55,36 @@ def test_trsv_levels_host():
             cols = cols[cols < r] if lower else cols[cols > r]
             ref[r] = 1 + (ref[cols].max() if len(cols) else 0)
         assert np.array_equal(lev, ref) and nl == ref.max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N,tail", [(128, 3072), (128, 2048), (128, 1024), (256, 8192), (256, 3072)])
+def test_lu_head_paths_match_host_factor(gpu, N, tail):
+    """Every way of running the head levels -- one CTA with the vector in
+    shared memory (<= 28672 unknowns and <= 64 levels), one cooperative launch
+    (<= 64 levels), one launch per level; a path that does not fit falls back
+    -- agrees with the host solve of the same SuperLU factors.  128^2 has 12644
+    unknowns (20 / 31 / 75 levels at tails 3072 / 2048 / 1024), 256^2 51040
+    (37 / 114 levels at tails 8192 / 3072)."""
+    from openecloud_b200.grid import Grid
+    from openecloud_b200.poissonSolver import PoissonSolver
+    g = Grid(N, N, 0.04, 0.04, 1)
+    ps = PoissonSolver(g, tail=tail)
+    ins = ps.insidePointsInd
+    q = np.zeros(g.getNpExt())
+    q[ins] = np.random.default_rng(N + tail).normal(size=ins.size) * 1e-9
+    ref = ps.ludecom.solve(q[ins])
+    for path in (1, 2, 3, 0):
+        ps._lu_t.head_path = path
+        ps.solve(q)
+        phi = ps.getPhi()
+        err = np.linalg.norm(phi[ins] - ref) / np.linalg.norm(ref)
+        res = np.linalg.norm(ps.systemMatrix.dot(phi[ins]) - q[ins]) / np.linalg.norm(q[ins])
+        assert err <= 1e-9 and res <= 1e-8, (path, ps.levels, err, res)
+
+
+def test_lu_head_path_field_is_last():
+    """oec_lu_t.head_path (C) sits after tu_inv, as the ctypes mirror has it."""
+    from openecloud_b200.poissonSolver import LU_t
+    assert LU_t._fields_[-1] == ("head_path", __import__("ctypes").c_int32)
+    assert LU_t.head_path.offset == LU_t.tu_inv.offset + 8
