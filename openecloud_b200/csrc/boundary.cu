@@ -318,28 +318,46 @@ __global__ void k_place_added(AddArgs a) {
     if (dropped) atomicAdd(&a.status->n_capacity_drop, dropped);
 }
 
+// First index in the ascending holes[0, n) that is >= v.
+__device__ __forceinline__ int holes_lower_bound(const int32_t *__restrict__ holes, int n, int v) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (holes[mid] < v) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
 // Fewer added rows than holes: the kept particles of the tail region
 // [N_new, N) move, in order, into the remaining holes below N_new
-// (particles.pyx:254-269 fills holes from the end the same way).  One CTA.
-__global__ void k_fill_holes(AddArgs a, const uint32_t *__restrict__ mask) {
+// (particles.pyx:254-269 fills holes from the end the same way).  The rank
+// of a kept tail particle p is the count of kept positions in [N_new, p):
+// (p - N_new) minus the holes among them, which a CTA takes for its chunk's
+// start from the ascending holes array (one binary search) and within the
+// chunk from a scan of the absorbed bits, so the chunks move independently
+// (a merge of 2e6 electrons leaves a tail of ~2e5 positions).  Sources are
+// all >= N_new and destinations < N_new: no move overlaps another.
+__global__ void __launch_bounds__(1024) k_fill_holes(AddArgs a, const uint32_t *__restrict__ mask) {
     __shared__ int sh[32];
+    __shared__ int holes_before;  // holes in [N_new, chunk start)
     const int N = a.scratch[0];
     const int A = min(*a.n_holes, a.holes_cap);
     const int S = min(*a.n_add, a.add_cap);
     if (S >= A) return;
     const int Nnew = N - A + S;
-    int taken = 0;  // kept tail particles moved so far
-    for (int base = Nnew; base < N; base += blockDim.x) {
-        int p = base + threadIdx.x;
-        int keep = 0;
-        if (p < N) keep = ((mask[p >> 5] >> (p & 31)) & 1u) ? 0 : 1;
-        int tot;
-        int rank = block_excl_scan(keep, &tot, sh) + taken;
-        if (keep) {
-            int h = a.holes[S + rank];  // ascending: the first holes are those below Nnew
-            copy_particle(a.p, h, p);
+    if (Nnew + (int)blockIdx.x * (int)blockDim.x >= N) return;  // whole CTA, before any barrier
+    const int h0 = holes_lower_bound(a.holes, A, Nnew);
+    for (int c0 = Nnew + blockIdx.x * blockDim.x; c0 < N; c0 += gridDim.x * blockDim.x) {
+        if (threadIdx.x == 0) holes_before = holes_lower_bound(a.holes, A, c0) - h0;
+        const int p = c0 + threadIdx.x;
+        const int absorbed = p < N ? (int)((mask[p >> 5] >> (p & 31)) & 1u) : 1;
+        const int before = block_excl_scan(absorbed, nullptr, sh);  // its barriers publish holes_before
+        if (!absorbed) {
+            const int k = S + (p - Nnew) - (holes_before + before);
+            if (k < A) copy_particle(a.p, a.holes[k], p);
         }
-        taken += tot;
+        __syncthreads();  // holes_before is rewritten by the next chunk
     }
 }
 
@@ -463,7 +481,7 @@ extern "C" int oec_add_remove(const oec_grid_t *grid, oec_particles_t *p, const 
     cudaStream_t s = as_stream(stream);
     int cap = add_cap > 0 ? add_cap : 1;
     k_place_added<<<persistent_grid((cap + 255) / 256, 4), 256, 0, s>>>(a);
-    k_fill_holes<<<1, 1024, 0, s>>>(a, absorbed_mask_dev);
+    k_fill_holes<<<persistent_grid(((int64_t)p->capacity + 1023) / 1024, 2), 1024, 0, s>>>(a, absorbed_mask_dev);
     k_set_count<<<1, 1, 0, s>>>(a);
     OEC_LAUNCH_CHECK();
     return OEC_OK;

@@ -165,6 +165,58 @@ def test_add_remove_set_semantics(gpu):
         assert np.array_equal(key(after), key(expect))
 
 
+def _placement_model(before, add_stored, keep):
+    """particles.pyx:254-269 restated on the host: added rows fill the holes
+    in index order and extra rows are appended; with fewer added rows than
+    holes the kept particles of the tail [N_new, N) move, in order, into the
+    remaining holes below N_new."""
+    n = before.shape[0]
+    holes = np.nonzero(keep == 0)[0]
+    A, S = holes.size, add_stored.shape[0]
+    out = before.copy()
+    if S >= A:
+        out[holes] = add_stored[:A]
+        return np.concatenate([out, add_stored[A:]])
+    out[holes[:S]] = add_stored
+    n_new = n - A + S
+    tail = np.arange(n_new, n)
+    kept_tail = tail[keep[n_new:] == 1]
+    out[holes[S:S + kept_tail.size]] = before[kept_tail]
+    return out[:n_new]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,n_add,frac_keep", [(60000, 2000, 0.7), (200000, 100, 0.95), (50000, 0, 0.5),
+                                               (30000, 9000, 0.7)])
+def test_add_remove_exact_placement(gpu, n, n_add, frac_keep):
+    """The device placement, particle by particle, against the host model over
+    tails of many 1024-position chunks (the fill runs chunk-parallel)."""
+    from openecloud_b200.grid import Grid
+    from openecloud_b200.particles import Particles
+    rng = np.random.default_rng(n + n_add)
+    g = Grid(64, 64, 0.04, 0.04, 0)
+    pd = np.empty((n, 6))
+    pd[:, :2] = rng.uniform(-0.019, 0.019, (n, 2))
+    pd[:, 2:5] = rng.normal(0, 1e5, (n, 3))
+    pd[:, 5] = rng.uniform(1, 2, n)
+    add = np.empty((n_add, 6))
+    add[:, :2] = rng.uniform(-0.019, 0.019, (n_add, 2))
+    add[:, 2:5] = rng.normal(0, 1e5, (n_add, 3))
+    add[:, 5] = rng.uniform(3, 4, n_add)
+    keep = (rng.random(n) < frac_keep).astype(np.uint16)
+    P = Particles("electrons", "variableWeight")
+    P.setParticleData(pd)
+    P._bind(g)
+    before = P.getParticleData()
+    P.addAndRemoveParticles(add, keep)
+    after = P.getParticleData()
+    P2 = Particles("electrons", "variableWeight")
+    P2.setParticleData(add if n_add else np.zeros((1, 6)))
+    P2._bind(g)
+    add_stored = P2.getParticleData()[:n_add]
+    assert np.array_equal(after, _placement_model(before, add_stored, keep))
+
+
 def test_homo_loader_uniform_inside(gpu):
     from scipy.stats import kstest
     from openecloud_b200.grid import Grid
