@@ -521,6 +521,16 @@ typedef struct oec_pcg_stats {
 
 int64_t oec_pcg_work_bytes(int32_t nx, int32_t ny);
 
+/* No counterpart in the reference.  Warm start of the next iterative solve
+ * by linear extrapolation in time: phi <- 2 phi - phi_prev and phi_prev <- the
+ * old phi, elementwise over n doubles (phi holds the last solution, phi_prev
+ * the one before).  history_dev (device int32, start at 0; NULL: always
+ * extrapolate) counts the solutions seen, saturating at 2: below 2 phi is
+ * kept and only copied to phi_prev.  Call it before each solve; enqueued on
+ * the stream, no synchronisation, so a captured step replays it. */
+int oec_warm_start_extrapolate(double *phi_dev, double *phi_prev_dev, int64_t n, int32_t *history_dev,
+                               void *stream);
+
 /* No counterpart in the reference (it only has the direct solve of
  * poissonSolver.pyx:85).  phi = A^-1 q on the inside nodes by f64 iterative
  * refinement around an f32 flexible preconditioned conjugate-gradient solve:

@@ -1078,10 +1078,38 @@ int enqueue_solve(const SolveArgs &a, cudaStream_t s) {
     return rc;
 }
 
+// phi <- 2 phi - prev, prev <- phi (the old phi): the linear extrapolation
+// in time of the last two solutions, in one pass over both vectors.  While
+// fewer than two solutions exist (*hist < 2) phi is kept and only copied to
+// prev.  The count advances in a separate launch so that every CTA of this one
+// reads the same value.
+__global__ void k_extrapolate(double *__restrict__ phi, double *__restrict__ prev, int64_t n,
+                              const int32_t *__restrict__ hist) {
+    const bool extrapolate = hist == nullptr || *hist >= 2;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double a = phi[i];
+        if (extrapolate) phi[i] = 2.0 * a - prev[i];
+        prev[i] = a;
+    }
+}
+
+__global__ void k_history_advance(int32_t *hist) { *hist = min(*hist + 1, 2); }
+
 }  // namespace
 }  // namespace oec
 
 using namespace oec;
+
+extern "C" int oec_warm_start_extrapolate(double *phi_dev, double *phi_prev_dev, int64_t n, int32_t *history_dev,
+                                          void *stream) {
+    if (!phi_dev || !phi_prev_dev || n < 0) return OEC_ERR_INVALID;
+    cudaStream_t s = as_stream(stream);
+    if (n > 0)
+        k_extrapolate<<<persistent_grid((n + 255) / 256, 4), 256, 0, s>>>(phi_dev, phi_prev_dev, n, history_dev);
+    if (history_dev) k_history_advance<<<1, 1, 0, s>>>(history_dev);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
 
 extern "C" int64_t oec_pcg_work_bytes(int32_t nx, int32_t ny) {
     const size_t G = (size_t)nx * (size_t)ny;

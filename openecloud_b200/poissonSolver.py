@@ -13,8 +13,10 @@ Solve (every step, device): the FP64 LU back-substitution of
 the CSR product E = phiToE . phi (``oec_spmv_csr``).  With ``method='pcg'``
 the solve is iterative instead (``oec_pcg_solve``: f64 residual refinement
 around an f32 flexible PCG on the matrix-free 5-point operator, warm-started
-from the previous phi, Jacobi or learned preconditioner); the LU solve stays
-the fallback whenever the f64 relative residual misses ``pcgTol``.
+by default from the linear extrapolation 2 phi_n-1 - phi_n-2 of the last two
+solutions (``oec_warm_start_extrapolate``), Jacobi, multigrid or learned
+preconditioner); the LU solve stays the fallback whenever the f64 relative
+residual misses ``pcgTol``.
 """
 import copy
 import ctypes
@@ -166,7 +168,7 @@ def mg_apply_host(ex, ey, leak, inside, nx, x):
 
 _lib.OTHER_DECLARED.update({"oec_lu_solve", "oec_spmv_csr", "oec_trsv_levels", "oec_stencil_apply",
                             "oec_pcg_work_bytes", "oec_pcg_solve", "oec_mg_apply",
-                            "oec_pcg_solve_async"})
+                            "oec_pcg_solve_async", "oec_warm_start_extrapolate"})
 
 
 def _declare():
@@ -191,6 +193,8 @@ def _declare():
         L.oec_pcg_solve_async.restype = ctypes.c_int
         L.oec_pcg_solve_async.argtypes = [ctypes.POINTER(Stencil_t), P, P, ctypes.c_double, ctypes.c_int32,
                                           ctypes.c_int32, P, P, P, ctypes.POINTER(LU_t), P, P, P]
+        L.oec_warm_start_extrapolate.restype = ctypes.c_int
+        L.oec_warm_start_extrapolate.argtypes = [P, P, ctypes.c_int64, P, P]
         L._poisson_declared = True
     return L
 
@@ -276,7 +280,7 @@ class PoissonSolver:
     """Reference: poissonSolver.pyx:33-67 (setup) and :83-98 (solve, getters)."""
 
     def __init__(self, gridObj, tail=None, method="lu", precond="jacobi", pcgTol=1e-8, pcgMaxIter=4000,
-                 warmStart="previous"):
+                 warmStart="extrapolate"):
         nx = gridObj.getNxExt()
         npn = gridObj.getNpExt()
         self.gridObj = gridObj
@@ -296,7 +300,9 @@ class PoissonSolver:
         self.pcgMaxIter = int(pcgMaxIter)
         self.cnn = None          # a trained network (openecloud_b200.cnn) for precond='cnn' / warmStart='cnn'
         self._mg = None          # multigrid hierarchy for precond='mg' (built on first use)
-        self.warmStart = warmStart  # 'previous' (last phi), 'zero' or 'cnn'
+        self.warmStart = warmStart  # 'previous' (last phi), 'extrapolate' (2 phi_n-1 - phi_n-2), 'zero' or 'cnn'
+        self._phi_prev = None    # phi of the solve before the last ('extrapolate')
+        self._ws_hist = None     # device count of the solutions seen, saturating at 2 ('extrapolate')
         self.nSolves = 0
         # statistics of the last iterative solve and the count of LU
         # fallbacks stay on the device (no host round trip per solve)
@@ -404,6 +410,7 @@ class PoissonSolver:
         s._pcg_work = torch.empty_like(self._pcg_work)
         s._stats_dev = torch.zeros_like(self._stats_dev)
         s._fb_count = torch.zeros_like(self._fb_count)
+        s._phi_prev = s._ws_hist = None
         s._pcg_used = False
         s.nSolves = 0
         s.cnn = None
@@ -510,6 +517,11 @@ class PoissonSolver:
             if torch.cuda.is_current_stream_capturing():
                 raise RuntimeError("PoissonSolver.prepare() must run before the graph capture")
             self._mg_setup()
+        if self.method == "pcg" and self.warmStart == "extrapolate" and self._phi_prev is None:
+            if torch.cuda.is_current_stream_capturing():
+                raise RuntimeError("PoissonSolver.prepare() must run before the graph capture")
+            self._phi_prev = self.phi.clone()
+            self._ws_hist = D.zeros(1, torch.int32)  # the first two solves start from phi itself
 
     def _pcg_solve(self, q):
         """Iterative solve warm-started from the current phi, with the LU
@@ -526,12 +538,18 @@ class PoissonSolver:
             ctx = self.cnn.c_handle()
         if self.warmStart == "zero":
             self.phi.zero_()
+        elif self.warmStart == "extrapolate":
+            self.prepare()
+            rc = _declare().oec_warm_start_extrapolate(self.phi.data_ptr(), self._phi_prev.data_ptr(), self.n_nodes,
+                                                       self._ws_hist.data_ptr(), D.stream())
+            if rc:
+                raise _lib.OecError("oec_warm_start_extrapolate", rc)
         elif self.warmStart == "cnn":
             if self.cnn is None:
                 raise ValueError("warmStart='cnn' needs a trained network in PoissonSolver.cnn")
             self.cnn.warm_start(self._stencil.scale32, q, self.phi)
         elif self.warmStart != "previous":
-            raise ValueError("warmStart must be 'previous', 'zero' or 'cnn'")
+            raise ValueError("warmStart must be 'previous', 'extrapolate', 'zero' or 'cnn'")
         rc = _declare().oec_pcg_solve_async(ctypes.byref(self._stencil), q.data_ptr(), self.phi.data_ptr(),
                                             self.pcgTol, self.pcgMaxIter, pc, ctx, self._pcg_work.data_ptr(),
                                             self._stats_dev.data_ptr(), ctypes.byref(self._lu_t),

@@ -271,6 +271,64 @@ def test_mg_pcg_iterations(gpu):
 
 
 @pytest.mark.gpu
+def test_warm_start_extrapolate_kernel(gpu):
+    """oec_warm_start_extrapolate: phi <- 2 phi - prev and prev <- old phi,
+    exactly (f64); with a history count, the first two calls keep phi."""
+    import ctypes
+    import torch
+    from openecloud_b200 import device as D
+    from openecloud_b200.poissonSolver import _declare
+    rng = np.random.default_rng(12)
+    a, b = rng.normal(size=100_003), rng.normal(size=100_003)
+    phi, prev = D.to_device(a, torch.float64), D.to_device(b, torch.float64)
+    L = _declare()
+    assert L.oec_warm_start_extrapolate(phi.data_ptr(), prev.data_ptr(), a.size, None, D.stream()) == 0
+    assert np.array_equal(D.to_numpy(phi), 2.0 * a - b) and np.array_equal(D.to_numpy(prev), a)
+    assert L.oec_warm_start_extrapolate(None, prev.data_ptr(), 1, None, D.stream()) != 0
+    hist = D.zeros(1, torch.int32)
+    phi, prev = D.to_device(a, torch.float64), D.to_device(b, torch.float64)
+    for k in range(3):
+        assert L.oec_warm_start_extrapolate(phi.data_ptr(), prev.data_ptr(), a.size, hist.data_ptr(), D.stream()) == 0
+        assert int(D.to_numpy(hist)[0]) == min(k + 1, 2)
+        if k < 2:
+            assert np.array_equal(D.to_numpy(phi), a) and np.array_equal(D.to_numpy(prev), a)
+    assert np.array_equal(D.to_numpy(phi), a)  # 2a - a
+
+
+@pytest.mark.gpu
+def test_pcg_extrapolated_warm_start(gpu):
+    """A charge that moves smoothly between solves (a Gaussian drifting by
+    0.2 cell per solve): from the third solve on, the extrapolated guess
+    2 phi_n-1 - phi_n-2 starts closer than the last phi, and both solves end
+    at the LU solution."""
+    from openecloud_b200.poissonSolver import PoissonSolver
+    z = golden("grid_circle_128.npz")
+    g = _grid(z)
+    ins = np.asarray(g.getInsidePoints()) != 0
+    nx = g.getNxExt()
+    j, i = np.divmod(np.arange(g.getNpExt()), nx)
+
+    def charge(t):
+        q = np.exp(-((i - 50.0 - 0.2 * t) ** 2 + (j - 60.0) ** 2) / (2 * 8.0 ** 2)) * 1e-12
+        return np.where(ins, q, 0.0)
+
+    lu = PoissonSolver(g)
+    res0 = {}
+    for ws in ("previous", "extrapolate"):
+        ps = PoissonSolver(g, method="pcg", precond="mg", warmStart=ws)
+        r = []
+        for t in range(6):
+            E = ps.solve(charge(t))
+            st = ps.lastStats
+            assert st.converged == 1 and ps.nFallbacks == 0
+            r.append(st.rel_residual0)
+        assert rel_err(E, lu.solve(charge(5))) <= 1e-6
+        res0[ws] = r
+    for t in range(3, 6):
+        assert res0["extrapolate"][t] < 0.5 * res0["previous"][t], res0
+
+
+@pytest.mark.gpu
 def test_pcg_synchronous_entry_point(gpu):
     """oec_pcg_solve (host statistics, one synchronisation) gives the
     asynchronous solve's result (solveDevice) to within the tolerance."""
