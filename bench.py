@@ -298,6 +298,7 @@ def poisson_comparison(ps, reps=10):
         return e0.elapsed_time(e1) / n
 
     out = {}
+    saved = (ps.method, ps.precond, ps.warmStart)
     ps.method = "lu"
     out["lu_ms"] = timed(lambda: ps.solveDevice(qd), reps)
     phi_lu = D.to_numpy(ps.phi)
@@ -319,7 +320,7 @@ def poisson_comparison(ps, reps=10):
     out["jacobi_cold_ms"] = timed(lambda: ps.solveDevice(qd), 2)
     out["jacobi_cold_iterations"] = ps.lastStats.iterations
     out["fallbacks"] = ps.nFallbacks - fb0
-    ps.method, ps.precond, ps.warmStart = "lu", "jacobi", "previous"
+    ps.method, ps.precond, ps.warmStart = saved
     out["tol"] = 1e-8
     out["timing"] = "device time (CUDA events) per solve, charge resident on the GPU"
     return out
