@@ -420,13 +420,21 @@ typedef struct oec_lu {
     const double *u_diag;      /* [head] diagonal of U, in level order */
     const double *tu_inv;      /* [m*m] inverse of U[tail,tail], row-major */
     int32_t head_path;         /* how the head levels run: OEC_LU_HEAD_* (0: chosen by size) */
+    const int8_t *l_level_lanes; /* HOST [l_nlevels] or NULL: per level, 0 or the lanes per row (1, 2, 4, ..., 32)
+                                    of a level that runs inside a one-CTA run (its rows * lanes <= 1024) */
+    const int8_t *u_level_lanes; /* HOST [u_nlevels] or NULL, likewise for U */
 } oec_lu_t;
 
-/* Head-level execution of oec_lu_solve.  AUTO: COOPERATIVE when both factors
- * have at most 64 head levels, else PER_LEVEL.  ONE_CTA (n <= 28672 and at
- * most 64 levels) is taken only when asked for: it ties with COOPERATIVE on a
- * warm L2 and is slower when the factors come from HBM.  A path that does not
- * fit falls back as AUTO does. */
+/* Head-level execution of oec_lu_solve.  AUTO: every run of two or more
+ * consecutive levels marked in l_level_lanes / u_level_lanes goes to one CTA
+ * (narrow levels: a __syncthreads instead of a launch between them); the
+ * levels between the runs go, segment by segment, to one cooperative launch
+ * (2 to 64 levels) or a launch per level.  PER_LEVEL: a launch per level.
+ * COOPERATIVE: one cooperative launch per factor of at most 64 levels, else a
+ * launch per level.  ONE_CTA (n <= 28672 and at most 64 levels per factor):
+ * each whole factor in one CTA with the vector in shared memory; it ties with
+ * COOPERATIVE on a warm L2 and is slower when the factors come from HBM, so
+ * AUTO does not take it.  A path that does not fit falls back as AUTO does. */
 #define OEC_LU_HEAD_AUTO 0
 #define OEC_LU_HEAD_PER_LEVEL 1    /* one launch per level, a warp per row */
 #define OEC_LU_HEAD_COOPERATIVE 2  /* one cooperative launch per factor, grid barrier between levels */

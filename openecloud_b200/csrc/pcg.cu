@@ -989,6 +989,8 @@ std::string solve_key(const SolveArgs &a, int dev) {
         kb.bytes(a.lu, sizeof(*a.lu));
         kb.bytes(a.lu->l_level_ptr, sizeof(int32_t) * (a.lu->l_nlevels + 1));
         kb.bytes(a.lu->u_level_ptr, sizeof(int32_t) * (a.lu->u_nlevels + 1));
+        if (a.lu->l_level_lanes) kb.bytes(a.lu->l_level_lanes, (size_t)a.lu->l_nlevels);
+        if (a.lu->u_level_lanes) kb.bytes(a.lu->u_level_lanes, (size_t)a.lu->u_nlevels);
     }
     kb.add(a.lu_work);
     kb.add(a.fb_count);

@@ -207,6 +207,93 @@ __global__ void __launch_bounds__(kWarps * 32)
     if (lane == 0) t[w] = b[w] - s;
 }
 
+// Runs of narrow head levels in one CTA.  Most levels of a large factor hold
+// a few rows with short entry lists, so a launch per level costs its launch
+// and drain (~8.5 us at 1024^2) for a chain of three dependent loads; one CTA
+// runs a whole run of such levels with a __syncthreads between them.  The
+// setup marks a level for this when its rows fit one pass of the CTA and its
+// longest row needs few loads per lane; lanes[l] is the lanes per row (a
+// power of two up to 32).  x is read and written in global memory: the
+// earlier levels of the run were written by this CTA (same SM), the rest by
+// earlier launches.
+constexpr int kThinMaxLevels = 2048;
+struct ThinLevels {
+    int n;
+    int ptr[kThinMaxLevels + 1];
+    int8_t lanes[kThinMaxLevels];
+};
+
+// A lane's share of one row of a run level: the row, its entry range and
+// diagonal, and its first kThinPre entries.  None of it depends on x, so the
+// next level's share is loaded while the current level computes and a level
+// waits only for its x values.
+constexpr int kThinPre = 4;
+struct ThinRow {
+    int r, k0, k1;
+    double d;
+    double v[kThinPre];
+    int c[kThinPre];
+};
+
+__device__ __forceinline__ void thin_fetch(ThinRow &t, int w, int w1, int sub, int g,
+                                           const int32_t *__restrict__ rows, const int32_t *__restrict__ ptr,
+                                           const int32_t *__restrict__ idx, const double *__restrict__ val,
+                                           const double *__restrict__ diag) {
+    t.r = -1;
+    if (w < w1) {
+        t.r = rows[w];
+        t.k0 = ptr[w] + sub;
+        t.k1 = ptr[w + 1];
+        t.d = diag ? diag[w] : 1.0;
+#pragma unroll
+        for (int j = 0; j < kThinPre; ++j) {
+            const int k = t.k0 + j * g;
+            if (k < t.k1) {
+                t.v[j] = val[k];
+                t.c[j] = idx[k];
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kBlockThreads)
+    k_trsv_thin(const int32_t *__restrict__ rows, ThinLevels lv, const int32_t *__restrict__ ptr,
+                const int32_t *__restrict__ idx, const double *__restrict__ val, const double *__restrict__ diag,
+                double *x) {
+    const int tid = threadIdx.x;
+    ThinRow nxt;
+    {
+        const int g0 = lv.lanes[0];
+        thin_fetch(nxt, lv.ptr[0] + tid / g0, lv.ptr[1], tid & (g0 - 1), g0, rows, ptr, idx, val, diag);
+    }
+    for (int l = 0; l < lv.n; ++l) {
+        const int g = lv.lanes[l];
+        const int sub = tid & (g - 1), groups = kBlockThreads / g;
+        const int r0 = lv.ptr[l], r1 = lv.ptr[l + 1];
+        ThinRow cur = nxt;
+        if (l + 1 < lv.n) {
+            const int gn = lv.lanes[l + 1];
+            thin_fetch(nxt, lv.ptr[l + 1] + tid / gn, lv.ptr[l + 2], tid & (gn - 1), gn, rows, ptr, idx, val, diag);
+        }
+        for (int base = r0; base < r1; base += groups) {  // one pass as set up; same trip count in every thread
+            if (base != r0) thin_fetch(cur, base + tid / g, r1, sub, g, rows, ptr, idx, val, diag);
+            double s = 0.0;
+            if (cur.r >= 0) {
+#pragma unroll
+                for (int j = 0; j < kThinPre; ++j)
+                    if (cur.k0 + j * g < cur.k1) s += cur.v[j] * x[cur.c[j]];
+                for (int k = cur.k0 + kThinPre * g; k < cur.k1; k += g) s += val[k] * x[idx[k]];
+            }
+            for (int o = g >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(kFullMask, s, o);
+            if (cur.r >= 0 && sub == 0) {
+                const double v = x[cur.r] - s;
+                x[cur.r] = diag ? v / cur.d : v;
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // out[i] = sum_{j in tri(i)} T[i*m + j] in[j]; lower: j <= i, upper: j >= i.
 // One CTA per row; rows are contiguous in memory so the loads coalesce.
 template <bool LOWER>
@@ -301,13 +388,13 @@ int lu_solve_block(const oec_lu_t *lu, const double *q, double *phi, double *c, 
     return OEC_OK;
 }
 
-// The levels of one triangle: one cooperative launch when `coop` asks for it,
-// they fit the parameter block and the device allows it, else one launch per
-// level.
-int solve_levels(const int32_t *rows, const int32_t *level_ptr, int nlevels, const int32_t *ptr,
-                 const int32_t *idx, const double *val, const double *diag, double *x, bool coop_ok,
-                 cudaStream_t s) {
-    if (nlevels <= 0) return OEC_OK;
+inline bool thin_lanes_ok(int g) { return g == 1 || g == 2 || g == 4 || g == 8 || g == 16 || g == 32; }
+
+// Levels [a, b) of one triangle, each its own launch, or one cooperative
+// launch when `coop` allows it, they are at least two and fit the parameter
+// block and the device supports it.
+int solve_wide(const int32_t *rows, const int32_t *level_ptr, int a, int b, const int32_t *ptr, const int32_t *idx,
+               const double *val, const double *diag, double *x, bool coop_ok, cudaStream_t s) {
     static int per_sm = -1;  // resident CTAs per SM of the cooperative kernel (0: no cooperative launch)
     if (per_sm < 0) {
         int dev = 0, coop = 0;
@@ -318,10 +405,11 @@ int solve_levels(const int32_t *rows, const int32_t *level_ptr, int nlevels, con
             per_sm = 0;
         cudaGetLastError();
     }
-    if (coop_ok && per_sm > 0 && nlevels <= kCoopMaxLevels) {
-        LevelPtr lv = level_ptrs(level_ptr, nlevels);
+    const int n = b - a;
+    if (coop_ok && per_sm > 0 && n >= 2 && n <= kCoopMaxLevels) {
+        LevelPtr lv = level_ptrs(level_ptr + a, n);
         int widest = 0;
-        for (int l = 0; l < nlevels; ++l) widest = std::max(widest, level_ptr[l + 1] - level_ptr[l]);
+        for (int l = a; l < b; ++l) widest = std::max(widest, level_ptr[l + 1] - level_ptr[l]);
         // one CTA per SM: a wider grid makes every barrier dearer than the
         // extra warps save on the few wide levels
         const int grid = std::max(1, std::min(sm_count(), (widest + kWarps - 1) / kWarps));
@@ -330,11 +418,43 @@ int solve_levels(const int32_t *rows, const int32_t *level_ptr, int nlevels, con
         OEC_CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_trsv_levels, dim3(grid), dim3(kWarps * 32), args, 0, s));
         return OEC_OK;
     }
-    for (int l = 0; l < nlevels; ++l) {
+    for (int l = a; l < b; ++l) {
         const int r0 = level_ptr[l], r1 = level_ptr[l + 1];
-        k_trsv_rows<<<warp_blocks(r1 - r0), kWarps * 32, 0, s>>>(rows, r0, r1, ptr, idx, val, diag, x);
+        if (r1 > r0) k_trsv_rows<<<warp_blocks(r1 - r0), kWarps * 32, 0, s>>>(rows, r0, r1, ptr, idx, val, diag, x);
     }
     OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+// The levels of one triangle: runs of two or more levels that `lanes` (host,
+// per level; optional) marks for one CTA go to k_trsv_thin, the levels
+// between them to solve_wide.
+int solve_levels(const int32_t *rows, const int32_t *level_ptr, int nlevels, const int8_t *lanes,
+                 const int32_t *ptr, const int32_t *idx, const double *val, const double *diag, double *x,
+                 bool coop_ok, cudaStream_t s) {
+    if (nlevels <= 0) return OEC_OK;
+    auto thin = [&](int l) { return lanes && l < nlevels && thin_lanes_ok(lanes[l]); };
+    int l = 0;
+    while (l < nlevels) {
+        int e = l;
+        while (thin(e) && e - l < kThinMaxLevels) ++e;
+        if (e - l >= 2) {
+            ThinLevels tl;
+            tl.n = e - l;
+            for (int k = 0; k <= tl.n; ++k) tl.ptr[k] = level_ptr[l + k];
+            for (int k = 0; k < tl.n; ++k) tl.lanes[k] = lanes[l + k];
+            k_trsv_thin<<<1, kBlockThreads, 0, s>>>(rows, tl, ptr, idx, val, diag, x);
+            OEC_LAUNCH_CHECK();
+            l = e;
+            continue;
+        }
+        // up to the next run of two marked levels
+        e = l + 1;
+        while (e < nlevels && !(thin(e) && thin(e + 1))) ++e;
+        const int rc = solve_wide(rows, level_ptr, l, e, ptr, idx, val, diag, x, coop_ok, s);
+        if (rc != OEC_OK) return rc;
+        l = e;
+    }
     return OEC_OK;
 }
 
@@ -356,11 +476,12 @@ extern "C" int oec_lu_solve(const oec_lu_t *lu, const double *q_dev, double *phi
     if (path == OEC_LU_HEAD_ONE_CTA && n <= kBlockMaxRows && few_levels)
         return lu_solve_block(lu, q_dev, phi_dev, c, t, s);
     const bool coop = path != OEC_LU_HEAD_PER_LEVEL;
+    const bool runs = path == OEC_LU_HEAD_AUTO || path == OEC_LU_HEAD_ONE_CTA;  // one-CTA runs of marked levels
     k_lu_gather<<<persistent_grid((n + 255) / 256, 4), 256, 0, s>>>(n, lu->rhs_node, q_dev, c);
     OEC_LAUNCH_CHECK();
     // forward, head levels (unit lower: no diagonal)
-    int rc = solve_levels(lu->l_rows, lu->l_level_ptr, lu->l_nlevels, lu->l_ptr, lu->l_idx, lu->l_val, nullptr, c,
-                          coop, s);
+    int rc = solve_levels(lu->l_rows, lu->l_level_ptr, lu->l_nlevels, runs ? lu->l_level_lanes : nullptr, lu->l_ptr,
+                          lu->l_idx, lu->l_val, nullptr, c, coop, s);
     if (rc != OEC_OK) return rc;
     if (m > 0) {
         // t = c_tail - L[tail, head] y_head ; y_tail = TLinv t ; z_tail = TUinv y_tail
@@ -371,8 +492,8 @@ extern "C" int oec_lu_solve(const oec_lu_t *lu, const double *q_dev, double *phi
         OEC_LAUNCH_CHECK();
     }
     // backward, head levels (rows use every column > row, tail included)
-    rc = solve_levels(lu->u_rows, lu->u_level_ptr, lu->u_nlevels, lu->u_ptr, lu->u_idx, lu->u_val, lu->u_diag, c,
-                      coop, s);
+    rc = solve_levels(lu->u_rows, lu->u_level_ptr, lu->u_nlevels, runs ? lu->u_level_lanes : nullptr, lu->u_ptr,
+                      lu->u_idx, lu->u_val, lu->u_diag, c, coop, s);
     if (rc != OEC_OK) return rc;
     OEC_CUDA_TRY(cudaMemsetAsync(phi_dev, 0, sizeof(double) * (size_t)lu->n_nodes, s));
     k_lu_scatter<<<persistent_grid((n + 255) / 256, 4), 256, 0, s>>>(n, lu->sol_src, lu->sol_node, c, phi_dev);

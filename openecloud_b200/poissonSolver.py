@@ -39,7 +39,7 @@ class LU_t(ctypes.Structure):
                 ("l_ptr", _P), ("l_idx", _P), ("l_val", _P), ("lc_ptr", _P), ("lc_idx", _P), ("lc_val", _P),
                 ("tl_inv", _P), ("u_nlevels", ctypes.c_int32), ("u_level_ptr", _P), ("u_rows", _P),
                 ("u_ptr", _P), ("u_idx", _P), ("u_val", _P), ("u_diag", _P), ("tu_inv", _P),
-                ("head_path", ctypes.c_int32)]
+                ("head_path", ctypes.c_int32), ("l_level_lanes", _P), ("u_level_lanes", _P)]
 
 
 class Stencil_t(ctypes.Structure):
@@ -223,6 +223,35 @@ def _level_lists(lev, nlevels):
     ptr = np.zeros(nlevels + 1, np.int32)
     np.cumsum(counts, out=ptr[1:])
     return order, ptr
+
+
+def level_lanes(csr, level_ptr, threads=1024, max_per_lane=16):
+    """Per head level (level-ordered CSR rows): the lanes per row with which
+    one CTA of `threads` threads takes the level in one pass -- the largest
+    power of two up to 32 with rows * lanes <= threads -- or 0 when the level
+    is too wide for that or its longest row would need more than
+    `max_per_lane` loads per lane (such a level keeps a launch of its own)."""
+    level_ptr = np.asarray(level_ptr, np.int64)
+    nl = level_ptr.size - 1
+    lanes = np.zeros(max(nl, 1), np.int8)
+    if nl <= 0:
+        return lanes
+    rows = np.diff(level_ptr)
+    nnz = np.diff(np.asarray(csr.indptr, np.int64))
+    longest = np.zeros(nl, np.int64)
+    ne = rows > 0
+    if nnz.size and ne.any():
+        longest[ne] = np.maximum.reduceat(nnz, level_ptr[:-1][ne])
+    for l in range(nl):
+        r = int(rows[l])
+        if r <= 0 or r > threads:
+            continue
+        g = 1
+        while g < 32 and r * 2 * g <= threads:
+            g *= 2
+        if -(-int(longest[l]) // g) <= max_per_lane:
+            lanes[l] = g
+    return lanes
 
 
 def choose_tail(Lcsr, Ucsr, n, launch_us=8.0, gbs=6000.0, max_tail=16384):
@@ -454,6 +483,7 @@ class PoissonSolver:
         Lh = Lh[rows]  # level order: a row's record is read at its position in the level
         k["l_ptr"], k["l_idx"], k["l_val"] = dev(Lh.indptr), dev(Lh.indices), dev(Lh.data, torch.float64)
         self._l_level_ptr = lptr
+        self._l_level_lanes = level_lanes(Lh, lptr)
         # strict upper U, head rows (all columns > row, tail columns included)
         Uh = spsp.triu(Uc[:h, :], k=1, format="csr")
         Uh.sort_indices()
@@ -464,6 +494,7 @@ class PoissonSolver:
         k["u_ptr"], k["u_idx"], k["u_val"] = dev(Uh.indptr), dev(Uh.indices), dev(Uh.data, torch.float64)
         k["u_diag"] = dev(Uc.diagonal()[:h][rowsu], torch.float64) if h > 0 else D.zeros(1, torch.float64)
         self._u_level_ptr = uptr
+        self._u_level_lanes = level_lanes(Uh, uptr)
         if m > 0:
             C = Lc[h:, :h].tocsr()
             C.sort_indices()
@@ -484,6 +515,8 @@ class PoissonSolver:
             setattr(s, name, D.ptr(k[name]))
         s.l_nlevels, s.l_level_ptr = nl, _np_ptr(self._l_level_ptr).value
         s.u_nlevels, s.u_level_ptr = nu, _np_ptr(self._u_level_ptr).value
+        s.l_level_lanes = _np_ptr(self._l_level_lanes).value
+        s.u_level_lanes = _np_ptr(self._u_level_lanes).value
         self._lu_t = s
         self._work = D.zeros(n + m + 1, torch.float64)
         E = self.phiToEAtGridPoints.tocsr()

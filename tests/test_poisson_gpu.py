@@ -58,14 +58,15 @@ def test_trsv_levels_host():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("N,tail", [(128, 3072), (128, 2048), (128, 1024), (256, 8192), (256, 3072)])
+@pytest.mark.parametrize("N,tail", [(128, 3072), (128, 2048), (128, 1024), (256, 8192), (256, 3072), (512, 8192)])
 def test_lu_head_paths_match_host_factor(gpu, N, tail):
     """Every way of running the head levels -- one CTA with the vector in
     shared memory (<= 28672 unknowns and <= 64 levels), one cooperative launch
     (<= 64 levels), one launch per level; a path that does not fit falls back
     -- agrees with the host solve of the same SuperLU factors.  128^2 has 12644
     unknowns (20 / 31 / 75 levels at tails 3072 / 2048 / 1024), 256^2 51040
-    (37 / 114 levels at tails 8192 / 3072)."""
+    (37 / 114 levels at tails 8192 / 3072), 512^2 205012 (231 levels at tail
+    8192: one-CTA runs between per-level launches)."""
     from openecloud_b200.grid import Grid
     from openecloud_b200.poissonSolver import PoissonSolver
     g = Grid(N, N, 0.04, 0.04, 1)
@@ -83,8 +84,26 @@ def test_lu_head_paths_match_host_factor(gpu, N, tail):
         assert err <= 1e-9 and res <= 1e-8, (path, ps.levels, err, res)
 
 
-def test_lu_head_path_field_is_last():
-    """oec_lu_t.head_path (C) sits after tu_inv, as the ctypes mirror has it."""
+def test_lu_struct_tail_layout():
+    """The last fields of oec_lu_t (C): tu_inv, head_path, l_level_lanes,
+    u_level_lanes, at the offsets the ctypes mirror has."""
+    import ctypes
     from openecloud_b200.poissonSolver import LU_t
-    assert LU_t._fields_[-1] == ("head_path", __import__("ctypes").c_int32)
+    assert [f[0] for f in LU_t._fields_[-4:]] == ["tu_inv", "head_path", "l_level_lanes", "u_level_lanes"]
     assert LU_t.head_path.offset == LU_t.tu_inv.offset + 8
+    assert LU_t.l_level_lanes.offset == LU_t.head_path.offset + 8  # int32 then 4 bytes of padding
+    assert LU_t.u_level_lanes.offset == LU_t.l_level_lanes.offset + 8
+    assert ctypes.sizeof(LU_t) == LU_t.u_level_lanes.offset + 8
+
+
+def test_level_lanes_rule():
+    """level_lanes: one pass of 1024 threads (rows * lanes <= 1024, lanes a
+    power of two up to 32) and at most 16 loads per lane, else 0."""
+    import scipy.sparse as spsp
+    from openecloud_b200.poissonSolver import level_lanes
+    # levels: 1 row of 40 entries, 3 rows of 2, 1500 rows of 1, 300 rows of 20, 20 rows of 600
+    lens = [40] + [2] * 3 + [1] * 1500 + [20] * 300 + [600] * 20
+    indptr = np.concatenate([[0], np.cumsum(lens)])
+    csr = spsp.csr_matrix((np.ones(indptr[-1]), np.zeros(indptr[-1], np.int32), indptr), shape=(len(lens), 1))
+    lptr = np.cumsum([0, 1, 3, 1500, 300, 20])
+    assert level_lanes(csr, lptr).tolist() == [32, 32, 0, 2, 0]
