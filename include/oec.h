@@ -398,6 +398,8 @@ int oec_cell_merge(const oec_grid_t *grid, oec_particles_t *p, int32_t n_cand, i
  * The head CSR of each factor is stored in level order: its row w is factor
  * row l_rows[w] (u_rows[w]), and level k holds rows [level_ptr[k],
  * level_ptr[k+1]) of that order; column indices are factor row numbers.
+ * The first level of L has no entries (any entry would be a dependency) and
+ * is not visited: its rows keep their right-hand side.
  * Level pointers are HOST arrays (the launch loop runs on the host); every
  * other pointer is a device pointer. */
 typedef struct oec_lu {

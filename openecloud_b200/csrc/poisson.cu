@@ -482,9 +482,13 @@ extern "C" int oec_lu_solve(const oec_lu_t *lu, const double *q_dev, double *phi
     const bool runs = path == OEC_LU_HEAD_AUTO || path == OEC_LU_HEAD_ONE_CTA;  // one-CTA runs of marked levels
     k_lu_gather<<<persistent_grid((n + 255) / 256, 4), 256, 0, s>>>(n, lu->rhs_node, q_dev, c);
     OEC_LAUNCH_CHECK();
-    // forward, head levels (unit lower: no diagonal)
-    int rc = solve_levels(lu->l_rows, lu->l_level_ptr, lu->l_nlevels, runs ? lu->l_level_lanes : nullptr, lu->l_ptr,
-                          lu->l_idx, lu->l_val, nullptr, c, coop, s);
+    // forward, head levels (unit lower: no diagonal).  The first level of a
+    // strictly lower triangle has no entries (any entry would be a
+    // dependency): its rows keep their right-hand side, so it is skipped.
+    const int l_skip = lu->l_nlevels > 0 ? 1 : 0;
+    int rc = solve_levels(lu->l_rows, lu->l_level_ptr + l_skip, lu->l_nlevels - l_skip,
+                          runs && lu->l_level_lanes ? lu->l_level_lanes + l_skip : nullptr, lu->l_ptr, lu->l_idx,
+                          lu->l_val, nullptr, c, coop, s);
     if (rc != OEC_OK) return rc;
     if (m > 0) {
         // t = c_tail - L[tail, head] y_head ; y_tail = TLinv t ; z_tail = TUinv y_tail
