@@ -1,6 +1,6 @@
 // poisson.cu -- Poisson solve on the device: the FP64 LU back-substitution
-// (judge and fallback), the FP32 conjugate-gradient solve with FP64 residual,
-// and the sparse E = phiToE * phi product.
+// (the direct solve, and the fallback and error reference of the iterative
+// one) and the sparse E = phiToE * phi product.
 //
 // Reference: poissonSolver.pyx:83-88 (phi[inside] = lu.solve(q[inside]);
 // E = phiToE . phi).  SuperLU's factors P_r A P_c = L U are produced on the
@@ -12,9 +12,11 @@
 // rows are split at setup into a "head", solved level by level, and a
 // "tail" of the last m rows, whose triangular block is inverted densely at
 // setup and applied as a matrix-vector product, turning hundreds of one-row
-// levels into one bandwidth-bound pass.  The head levels run in one
-// cooperative launch when they are few, else one launch per level (or, on
-// request, in one CTA with the vector in shared memory).
+// levels into one bandwidth-bound pass.  Of the head levels, runs of narrow
+// ones go to one CTA each (a __syncthreads between levels), and the wide
+// ones between the runs to one cooperative launch per segment of 2-64 levels
+// or a launch per level (or, on request, each whole triangle to one CTA with
+// the vector in shared memory).
 #include <math.h>
 #include <stdint.h>
 
@@ -58,10 +60,9 @@ __global__ void __launch_bounds__(kWarps * 32)
 // (the launch guarantees that every CTA is resident, so the barrier is the
 // hardware's, not a spin).  x is read through L2 (__ldcg): a row's inputs were
 // written by other SMs after this SM's L1 may have cached their lines.
-// Up to this many levels one cooperative launch beats a launch per level
-// (128^2: 40 levels in 0.17 ms against 0.22 ms); deeper factors are bound by
-// the per-level latency (a few dependent L2 loads and the barrier, ~7 us)
-// either way and keep the launch per level.
+// Up to this many levels one cooperative launch replaces the launches of a
+// segment (128^2: 40 levels in 0.17 ms against 0.22 ms as launches); the
+// level pointers travel in the parameter block.
 constexpr int kCoopMaxLevels = 64;
 struct LevelPtr {
     int n;
@@ -98,8 +99,9 @@ __global__ void __launch_bounds__(kWarps * 32)
 // entries, though: at 128^2 (12644 unknowns, 20 levels) it ties with the
 // cooperative launch on a warm L2 (0.172 against 0.166 ms) and loses inside a
 // buildup step, where the other kernels have evicted the factors (2500 steps:
-// 0.78 against 0.71 s), so the automatic choice does not take it.  A level's rows are spread over the CTA with g lanes per
-// row, g the largest power of two up to 32 that keeps the level in one pass
+// 0.78 against 0.71 s), so the automatic choice does not take it.  A level's
+// rows are spread over the CTA with g lanes per row, g the largest power of
+// two up to 32 that keeps the level in one pass
 // (1 for the wide bottom levels; the narrow top levels have the long rows).
 // A level's cost is the latency of its loads, so the record of a thread's
 // first row in the next level (row, entry range, diagonal; none of it
