@@ -1,7 +1,8 @@
 // pcg.cu -- iterative Poisson solve: f64 iterative refinement around an f32
 // flexible preconditioned conjugate-gradient solve (FCG with one stored
-// direction) on the 5-point FIT
-// operator, with the LU back-substitution (poisson.cu) as judge and fallback.
+// direction) on the 5-point FIT operator, with the LU back-substitution
+// (poisson.cu) as its fallback and the reference its error is measured
+// against.
 //
 // Reference operator: PoissonSolver.__init__ (poissonSolver.pyx:41-58) builds
 // A = S diag(meps) S^T over the inside nodes; A is applied here matrix-free

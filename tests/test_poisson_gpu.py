@@ -96,6 +96,33 @@ def test_lu_struct_tail_layout():
     assert ctypes.sizeof(LU_t) == LU_t.u_level_lanes.offset + 8
 
 
+def test_choose_tail_minimises_the_model():
+    """choose_tail on the 128^2 circle's factors: among its candidates
+    (at most n/4 rows and 16384), the tail with the lowest
+    levels * 8 us + 2 m^2 * 8 B / 6000 GB/s, computed here from the level
+    counts of oec_trsv_levels."""
+    from scipy.sparse.linalg import splu
+    from openecloud_b200.grid import Grid
+    from openecloud_b200.poissonSolver import _levels, assemble, choose_tail
+    a, _, _, _ = assemble(Grid(128, 128, 0.04, 0.04, 1))
+    lu = splu(a, permc_spec="MMD_AT_PLUS_A", diag_pivot_thresh=0.1)
+    n = lu.shape[0]
+    Lc, Uc = lu.L.tocsr(), lu.U.tocsr()
+    Lc.sort_indices()
+    Uc.sort_indices()
+    m = choose_tail(Lc, Uc, n)
+    assert 0 < m <= min(n // 4, 16384)
+
+    def model(t):
+        h = n - t
+        return ((_levels(Lc, True, h, nrows=h)[1] + _levels(Uc, False, h, nrows=h)[1]) * 8e-6 +
+                2 * t * t * 8 / 6000e9)
+    for t in (0, 1024, 2048, 3072):
+        if t <= n // 4:
+            assert model(m) <= model(t) + 1e-12, (m, t)
+    assert m == 3072  # the measured optimum of this grid (0.15 ms; 2048: 0.18, 4096: 0.16)
+
+
 def test_level_lanes_rule():
     """level_lanes: one pass of 1024 threads (rows * lanes <= 1024, lanes a
     power of two up to 32) and at most 16 loads per lane, else 0."""
