@@ -84,6 +84,23 @@ def test_lu_head_paths_match_host_factor(gpu, N, tail):
         assert err <= 1e-9 and res <= 1e-8, (path, ps.levels, err, res)
 
 
+@pytest.mark.gpu
+def test_lu_invalid_head_path_is_rejected(gpu):
+    """An unknown head_path is an argument error before any launch; the
+    solver works again once it is valid."""
+    from openecloud_b200 import _lib
+    from openecloud_b200.poissonSolver import PoissonSolver
+    z = golden("grid_circle_32.npz")
+    ps = PoissonSolver(_grid(z))
+    q = z["poisson_q"]
+    ps._lu_t.head_path = 7
+    with pytest.raises(_lib.OecError):
+        ps.solve(q)
+    ps._lu_t.head_path = 0
+    ps.solve(q)
+    assert rel_err(ps.getPhi(), z["poisson_phi"]) <= 1e-9
+
+
 def test_lu_struct_tail_layout():
     """The last fields of oec_lu_t (C): tu_inv, head_path, l_level_lanes,
     u_level_lanes, at the offsets the ctypes mirror has."""
