@@ -140,6 +140,46 @@ def test_choose_tail_minimises_the_model():
     assert m == 3072  # the measured optimum of this grid (0.15 ms; 2048: 0.18, 4096: 0.16)
 
 
+def test_level_ordered_head_solve_host():
+    """The setup's layout, replayed on the host: the strict-lower and
+    strict-upper head rows of the 128^2 factors, reordered by dependency
+    level, solved level by level through the reordered CSR (row w holds
+    factor row rows[w]; L's first level skipped) equal the triangular solves
+    of scipy on the head block."""
+    import scipy.sparse as spsp
+    from scipy.sparse.linalg import spsolve_triangular, splu
+    from openecloud_b200.grid import Grid
+    from openecloud_b200.poissonSolver import _level_lists, _levels, assemble
+    a, _, _, _ = assemble(Grid(128, 128, 0.04, 0.04, 1))
+    lu = splu(a, permc_spec="MMD_AT_PLUS_A", diag_pivot_thresh=0.1)
+    n = lu.shape[0]
+    h = n - 3072
+    Lc, Uc = lu.L.tocsr(), lu.U.tocsr()
+    rng = np.random.default_rng(5)
+    for lower in (True, False):
+        T = spsp.tril(Lc[:h, :h], k=-1, format="csr") if lower else spsp.triu(Uc[:h, :h], k=1, format="csr")
+        T.sort_indices()
+        diag = np.ones(h) if lower else Uc.diagonal()[:h]
+        lev, nl = _levels(T, lower, h)
+        rows, lptr = _level_lists(lev, nl)
+        Tw = T[rows]  # level order
+        dw = diag[rows]
+        b = rng.normal(size=h)
+        x = b.copy()
+        first = 1 if lower else 0
+        if lower:
+            assert np.diff(Tw.indptr)[lptr[0]:lptr[1]].sum() == 0  # L's first level has no entries
+        for l in range(first, nl):
+            w = np.arange(lptr[l], lptr[l + 1])
+            r = rows[w]
+            sums = np.array([Tw.data[Tw.indptr[k]:Tw.indptr[k + 1]] @ x[Tw.indices[Tw.indptr[k]:Tw.indptr[k + 1]]]
+                             for k in w])
+            x[r] = (x[r] - sums) / dw[w]
+        full = (T + spsp.diags(diag)).tocsr()
+        ref = spsolve_triangular(full, b, lower=lower)
+        assert np.linalg.norm(x - ref) <= 1e-12 * np.linalg.norm(ref), lower
+
+
 def test_level_lanes_rule():
     """level_lanes: one pass of 1024 threads (rows * lanes <= 1024, lanes a
     power of two up to 32) and at most 16 loads per lane, else 0."""
