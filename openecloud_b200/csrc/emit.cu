@@ -290,6 +290,41 @@ __global__ void k_scan_add(int32_t *out, const int32_t *n_p, int cap, const int 
     if (i < n) out[i] += partial[blockIdx.x];
 }
 
+// The same scan in one CTA when the row capacity is small (a buildup step
+// absorbs a few hundred rows of a capacity of tens of thousands): the first
+// n rows, kScanT at a time with a running carry, one launch instead of three.
+// Rows past n keep what they held; the emission passes read only rows < n.
+constexpr int kSmallScanBlocks = 32;
+
+__global__ void __launch_bounds__(kScanT)
+    k_scan_small(const int32_t *in, const int32_t *n_p, int cap, int32_t *out, int32_t *total) {
+    __shared__ int sh[32];
+    const int n = min(*n_p, cap);
+    int carry = 0;
+    for (int base = 0; base < n; base += kScanT) {  // same trip count in every thread
+        const int i = base + threadIdx.x;
+        const int v = i < n ? in[i] : 0;
+        int tot;
+        const int ex = block_scan_excl(v, &tot, sh);
+        if (i < n) out[i] = carry + ex;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+// offsets of the rows' secondaries and their total
+void scan_counts(const int32_t *nsec, const int32_t *n_abs_dev, int cap, int32_t *off, int *partial,
+                 int32_t *n_out_dev, cudaStream_t s) {
+    const int nblocks = (cap + kScanT - 1) / kScanT;
+    if (nblocks <= kSmallScanBlocks) {
+        k_scan_small<<<1, kScanT, 0, s>>>(nsec, n_abs_dev, cap, off, n_out_dev);
+        return;
+    }
+    k_scan_blocks<<<nblocks, kScanT, 0, s>>>(nsec, n_abs_dev, cap, off, partial);
+    k_scan_partials<<<1, kScanT, 0, s>>>(partial, nblocks, n_out_dev);
+    k_scan_add<<<nblocks, kScanT, 0, s>>>(off, n_abs_dev, cap, partial);
+}
+
 // ------------------------------------------- simplified emitters
 // SecElecEmitter (particleEmitter.pyx:355-484) and SimpleSecEmitter
 // (:506-597): pass 1 draws the elastic / rediffused / true counts (draws
@@ -493,7 +528,6 @@ extern "C" int oec_furman_emit(const oec_furman_t *params, const double *rows_de
         !status_dev || cap < 0 || out_cap < 0 || params->m < 1 || params->m > 10)
         return OEC_ERR_INVALID;
     if (cap > kMaxAbsorbedRows) return OEC_ERR_INVALID;
-    const int nblocks = (cap + kScanT - 1) / kScanT;
     cudaStream_t s = as_stream(stream);
     // work layout: Rec[cap] | split[cap * kSlots] (f64) | nsec[cap] | offset[cap] | partial[scan_blocks(cap)]
     char *w = static_cast<char *>(work_dev);
@@ -507,9 +541,7 @@ extern "C" int oec_furman_emit(const oec_furman_t *params, const double *rows_de
     k_furman_pass1<<<g, 128, 0, s>>>(*params, rows_dev, normals_dev, n_abs_dev, cap, ids_dev, key, step, step_dev,
                                      replay_uniforms_dev, rec, nsec, status_dev);
     if (cap > 0) {
-        k_scan_blocks<<<nblocks, kScanT, 0, s>>>(nsec, n_abs_dev, cap, off, partial);
-        k_scan_partials<<<1, kScanT, 0, s>>>(partial, nblocks, n_out_dev);
-        k_scan_add<<<nblocks, kScanT, 0, s>>>(off, n_abs_dev, cap, partial);
+        scan_counts(nsec, n_abs_dev, cap, off, partial, n_out_dev, s);
     } else {
         OEC_CUDA_TRY(cudaMemsetAsync(n_out_dev, 0, sizeof(int32_t), s));
     }
@@ -530,7 +562,6 @@ extern "C" int oec_secelec_emit(const oec_secelec_t *params, const double *rows_
         !status_dev || cap < 0 || out_cap < 0 || params->model < 0 || params->model > 1 || params->max_ts < 1 ||
         params->max_ts > 10 || cap > kMaxAbsorbedRows)
         return OEC_ERR_INVALID;
-    const int nblocks = (cap + kScanT - 1) / kScanT;
     cudaStream_t s = as_stream(stream);
     // work layout: SRec[cap] | nsec[cap] | offset[cap] | partial[scan_blocks(cap)]
     char *w = static_cast<char *>(work_dev);
@@ -543,9 +574,7 @@ extern "C" int oec_secelec_emit(const oec_secelec_t *params, const double *rows_
     k_secelec_pass1<<<g, 128, 0, s>>>(*params, rows_dev, normals_dev, n_abs_dev, cap, ids_dev, key, step, step_dev,
                                       replay_uniforms_dev, rec, nsec, status_dev);
     if (cap > 0) {
-        k_scan_blocks<<<nblocks, kScanT, 0, s>>>(nsec, n_abs_dev, cap, off, partial);
-        k_scan_partials<<<1, kScanT, 0, s>>>(partial, nblocks, n_out_dev);
-        k_scan_add<<<nblocks, kScanT, 0, s>>>(off, n_abs_dev, cap, partial);
+        scan_counts(nsec, n_abs_dev, cap, off, partial, n_out_dev, s);
     } else {
         OEC_CUDA_TRY(cudaMemsetAsync(n_out_dev, 0, sizeof(int32_t), s));
     }
