@@ -42,6 +42,15 @@ ME = 9.10938291e-31
 EPS0 = 8.85418781762e-12
 METRIC = "particle-steps/s"
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
+# the fused kernel, by store size, from an ncu capture of
+#   python bench.py --particles 8388608 --steps 2 --warmup 3 --e2e-steps 0 --no-cpu-baseline --no-passage
+#       --no-production --no-batch --no-components
+# (ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none -k regex:k_push_gather -s 3 -c 1):
+# the particle part scaled by 2 to 2^24 electrons, the grid part (E table and
+# deposit grid, 12.7 MB) added once.
+NCU_TRAFFIC_PER_LAUNCH = {1 << 24: 771791520}
+
 
 # ------------------------------------------------------------- workload
 def workload(n, nodes=512, seed=7):
@@ -146,10 +155,12 @@ def _ref_modules():
         return None
 
 
-def cpu_reference_steps(n_sample, min_seconds, max_steps, min_steps=1):
+def cpu_reference_steps(pd, E, geom, min_seconds, max_steps, min_steps=1, warm=0):
     """Time the compiled reference's own step (weights, deposit, gather, push,
-    wall test) on a bounded sample; falls back to the C oracle port."""
-    pd, E, (nx, ny, lx, ly) = workload(n_sample, seed=11)
+    wall test) on the rows `pd` of the workload, after `warm` untimed steps;
+    falls back to the C oracle port when the reference is not built."""
+    n_sample = pd.shape[0]
+    nx, ny, lx, ly = geom
     mods = _ref_modules()
     steps = 0
     if mods is not None:
@@ -180,7 +191,7 @@ def cpu_reference_steps(n_sample, min_seconds, max_steps, min_steps=1):
             e = O.field_to_particles(p, og, E, 2)
             state["pd"] = O.boris_push(p, e, 1e-11, qm, 1, bconst=[0.0, 0.5, 0.0])
             O.index_inside(state["pd"], og, 0)
-    # Every timed step starts from the same in-grid sample: the reference
+    # Every timed step starts from the same in-grid rows: the reference
     # indexes its grid unchecked (particles.pyx:410-411), so particles may not
     # be left to drift out of the extended grid over many steps.
     def reload():
@@ -188,8 +199,9 @@ def cpu_reference_steps(n_sample, min_seconds, max_steps, min_steps=1):
             P.setParticleData(pd.copy())
         else:
             state["pd"] = pd.copy()
-    reload()
-    step()  # warm caches
+    for _ in range(warm):
+        reload()
+        step()
     dt = 0.0
     t_all = time.perf_counter()
     while steps < min_steps or (time.perf_counter() - t_all < min_seconds and steps < max_steps):
@@ -198,9 +210,18 @@ def cpu_reference_steps(n_sample, min_seconds, max_steps, min_steps=1):
         step()
         dt += time.perf_counter() - t0
         steps += 1
-    return {"value": n_sample * steps / dt, "unit": METRIC, "cores": 1, "kind": kind,
-            "sample": f"{n_sample} particles x {steps} steps of the same workload (512x512 rect, B_y=0.5 T), "
-                      f"single thread ({dt:.1f} s)"}
+    return {"value": n_sample * steps / dt, "unit": METRIC, "cores": 1, "kind": kind, "steps": steps,
+            "sample": f"the whole workload ({n_sample} particles) x {steps} steps, each from the same rows "
+                      f"(512x512 rect, B_y=0.5 T), single thread ({dt:.1f} s)"}
+
+
+def bench_config(n, nx, ny, world):
+    """The workload description both arms print (one config for the ratio)."""
+    return {"workload": "kernel microbench: 2^24 macro-electrons per GPU, 512x512 rect grid 40x40 mm, Maxwellian "
+                        "5 eV, B_y=0.5 T, fused gather+Boris+move+wall test+int64 deposit, dt=1e-11 s",
+            "particles_per_gpu": n, "grid_nodes": [nx + 2, ny + 2],
+            "parallelism": f"{world} independent particle shards",
+            "l2": "inputs 470 MB per step > 126 MB L2 (no flush needed)"}
 
 
 PASSAGE = ("c1 buildup: 128x128 circular chamber R=20 mm, 1e4 initial electrons at rest, endless train "
@@ -513,19 +534,21 @@ def batched_scan(n_runs=64, steps=100, steady=50):
 
 
 def run_reference(args, rank, world):
+    """The compiled reference's own step on the host cores, on the same
+    workload (2^24 electrons, seed 7) as the device arm: `warmup` untimed
+    steps, then `steps` timed ones, each from the same rows."""
     if rank != 0:
         return
-    n_sample = 1 << 22
     t0 = time.perf_counter()
-    res = cpu_reference_steps(n_sample, min_seconds=0.0, max_steps=args.warmup, min_steps=max(1, args.warmup))
-    res = cpu_reference_steps(n_sample, min_seconds=0.0, max_steps=args.steps, min_steps=args.steps)
-    ms = n_sample / res["value"] * 1e3
+    n = args.particles
+    pd, E, geom = workload(n, seed=7)
+    res = cpu_reference_steps(pd, E, geom, min_seconds=0.0, max_steps=args.steps, min_steps=args.steps,
+                              warm=args.warmup)
+    ms = n / res["value"] * 1e3
     line = {"metric": METRIC, "value": res["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "kernel microbench: 2^24 electrons (timed on a 2^22 sample), 512x512 rect "
-                                   "40x40 mm, B_y=0.5 T, weights+deposit+gather+Boris+wall test",
-                       "inputs_vs_L2": "sample 200 MB > L2"},
+            "config": bench_config(n, geom[0], geom[1], world),
             "impl": "reference", "cpu_baseline": {k: res[k] for k in ("kind", "cores", "sample", "value")},
             "e2e": {"value": res["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     cp = cpu_reference_passage()
@@ -661,11 +684,16 @@ def run_ours(args, rank, world, local_rank):
                        "download in chunks with both copy directions overlapped (3 streams)"}
 
     # ----------------------------------------------------------- roofline
+    # Algorithmic bytes of the hot-path step per launch: read and write
+    # x, y, vx, vy, vz (40 B) and read w for the fused deposit (4 B) per
+    # particle, E read once (2 f32 per node), the int64 deposit grid zeroed
+    # and written once (2 x 8 B per node).
     G = (nx + 2) * (ny + 2)
-    bytes_particle = 28 + 24 + 1.0 / 8  # read cell,ox,oy,vx,vy,vz,w; write cell,ox,oy,vx,vy,vz; absorbed bit
-    bytes_grid = 8 * 4 * G + 8 * G + 8 * G  # E corner table read, rho clear + accumulate
-    alg_bytes = n * bytes_particle + bytes_grid
+    alg_bytes = 44 * n + 2 * 4 * G + 2 * 8 * G
     achieved = alg_bytes / (ms_kernel * 1e-3) / 1e9
+    # The bytes this store layout moves: cell index, in-cell offsets and the
+    # absorbed bit on top of the above, and the cell-centric E table.
+    layout_bytes = (28 + 24 + 1.0 / 8) * n + 8 * 4 * G + 8 * G + 8 * G
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peak, peak_src = 6650.0, "fallback"
     if os.path.exists(peaks_path):
@@ -674,20 +702,13 @@ def run_ours(args, rank, world, local_rank):
             peak_src = "measured"
         except Exception:
             pass
-    # DRAM bytes per launch of the fused kernel from the committed ncu summary
-    # (scaled to 2^24 particles there); only meaningful for that size.
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "push_gather_c2.md")
-    if os.path.exists(tpath) and n == 1 << 24:
-        import re
-        m = re.search(r"^traffic_per_launch_bytes:\s*([0-9]+)", open(tpath).read(), re.M)
-        traffic = int(m.group(1)) if m else None
+    traffic = NCU_TRAFFIC_PER_LAUNCH.get(n)
 
     if e2e is not None:
         _log(f"e2e: {e2e['ms_per_step']:.3f} ms/step")
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_reference_steps(1 << 21, min_seconds=10.0, max_steps=200, min_steps=3)
+        cpu = cpu_reference_steps(pd, E, (nx, ny, lx, ly), min_seconds=10.0, max_steps=30, min_steps=3, warm=1)
     passage = None
     if rank == 0 and world == 1 and not args.no_passage:
         passage = gpu_passage()
@@ -720,16 +741,17 @@ def run_ours(args, rank, world, local_rank):
         line = {"metric": METRIC, "value": n * world / (ms_step * 1e-3), "unit": METRIC, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32+i64", "data": "synthetic",
-                "config": {"workload": "kernel microbench: 2^24 macro-electrons per GPU, 512x512 rect grid "
-                                       "40x40 mm, Maxwellian 5 eV, B_y=0.5 T, fused gather+Boris+move+wall "
-                                       "test+int64 deposit, dt=1e-11 s",
-                           "particles_per_gpu": n, "grid_nodes": [nx + 2, ny + 2],
-                           "parallelism": f"{world} independent particle shards",
-                           "l2": "inputs 470 MB per step > 126 MB L2 (no flush needed)"},
+                "config": bench_config(n, nx, ny, world),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic,
                              "kernel": "k_push_gather<1,rect,deposit>", "kernel_ms": ms_kernel,
-                             "alg_bytes_per_launch": alg_bytes, "peak_source": peak_src},
+                             "alg_bytes_per_launch": alg_bytes,
+                             "alg_bytes": "44 B per particle (x, y, vx, vy, vz read and written, w read) + "
+                                          "E 2 x 4 B per node + int64 deposit grid 2 x 8 B per node",
+                             "layout_bytes_per_launch": layout_bytes,
+                             "layout_achieved": layout_bytes / (ms_kernel * 1e-3) / 1e9,
+                             "layout_frac": layout_bytes / (ms_kernel * 1e-3) / 1e9 / peak,
+                             "peak_source": peak_src},
                 "clocks": clk, "e2e": e2e, "gpu_launches": 1 * args.steps,
                 "status": {k: v for k, v in status.items() if v}}
         if cpu is not None:

@@ -52,7 +52,10 @@ typedef struct oec_status {
     int32_t warn_derm;         /* delta_E+delta_R >= cap (particleEmitter.pyx:201-206) */
     int32_t warn_tsprime;      /* delta_TS' >= m (particleEmitter.pyx:209-214) */
     int32_t n_out_of_grid;     /* particles that left the extended grid (absorbed) */
-    int32_t reserved[5];
+    int32_t n_rows_dropped;    /* absorbed particles beyond the absorbed-row capacity of
+                                  oec_wall_interaction: removed without a wall row, so
+                                  they emit no secondaries (the caller must grow the rows) */
+    int32_t reserved[4];
 } oec_status_t;
 
 /* ------------------------------------------------------------ types */

@@ -41,7 +41,7 @@ class Boundary_t(ctypes.Structure):
 
 STATUS_FIELDS = ["n_absorbed", "n_secondaries", "n_nonfinite", "n_clipped", "n_not_found",
                  "n_capacity_drop", "deposit_overflow", "n_wait_timeout", "warn_derm", "warn_tsprime",
-                 "n_out_of_grid"]
+                 "n_out_of_grid", "n_rows_dropped"]
 STATUS_WORDS = 16
 
 _P = ctypes.c_void_p

@@ -169,6 +169,8 @@ class BatchedBuildup:
             k += nxt
         t1.record(s)
         t1.synchronize()
+        for b in self.runs:
+            b._check_rows()
         return t0.elapsed_time(t1) * 1e-3
 
     def _time_replays(self, n, nb):

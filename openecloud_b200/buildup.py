@@ -69,7 +69,7 @@ class Buildup:
                  material="copper", sey_max=1.6, e_hat0=300.0, type_b_field=0, b_const=(0., 0., 0.),
                  target=100000, management="global", management_every=50, capacity=None, seed=0,
                  n_steps_table=2500, sort_every=0, boundFunc=None, poisson=None, grid=None, b_multipoles=None,
-                 b_skew=(), emitter="furman"):
+                 b_skew=(), emitter="furman", abs_cap=None):
         if grid is not None and (grid.nx, grid.ny, grid.lx, grid.ly, grid.boundType) != (nx, ny, lx, ly, boundType):
             raise ValueError("grid: another grid than nx, ny, lx, ly, boundType describe")
         self.grid = grid if grid is not None else Grid(nx, ny, lx, ly, boundType, boundFunc=boundFunc)
@@ -126,8 +126,10 @@ class Buildup:
         self.hist_w = D.zeros(self._table_len, torch.float64)
         self.hist_n = D.zeros(self._table_len, torch.int32)
         self.scratch = D.zeros(256, torch.float64)  # oec_history's partial sums
-        # absorbed rows per step: bounded by a fraction of the capacity
-        self.abs_cap = max(4096, cap // 8)
+        # absorbed rows per step: by default bounded by a fraction of the
+        # capacity; a step that absorbs more is counted on the device
+        # (status n_rows_dropped) and run() raises
+        self.abs_cap = int(abs_cap) if abs_cap is not None else max(4096, cap // 8)
         self.bd.ensure_buffers(self.abs_cap)
         self.em.ensure_buffers(self.bd._rows.shape[0])
         self.P._deposit_buffers(self.grid)
@@ -136,6 +138,7 @@ class Buildup:
         _lib.call("oec_history", self.P.c_particles(), self.step_dev.data_ptr(), self._table_len,
                   self.hist_w.data_ptr(), self.hist_n.data_ptr(), self.scratch.data_ptr(), D.stream())
         self.graph = None
+        self._rows_dropped = 0
         self.n_managed = 0       # management events (roulette / merge) so far
         self._graph_sig = None
         self._cap_stream = None
@@ -182,7 +185,18 @@ class Buildup:
                   self.hist_n.data_ptr(), self.scratch.data_ptr(), s)
         del L
 
+    def _check_rows(self):
+        """Raises if a step absorbed more particles than the absorbed-row
+        buffer holds: those particles were removed without a wall row and
+        emitted no secondaries, so the run under-counts the build-up."""
+        dropped = self.P.status()["n_rows_dropped"]
+        if dropped > self._rows_dropped:
+            self._rows_dropped = dropped
+            raise RuntimeError(f"{dropped} absorbed particles exceeded the absorbed-row capacity ({self.abs_cap} rows "
+                               "per step) and emitted nothing: build the run with a larger abs_cap")
+
     def _manage(self, step):
+        self._check_rows()
         n = self.P.getMacroParticleCount()
         if step > 0 and step % self.management_every == 0 and (n > 1.05 * self.target or n < 0.95 * self.target):
             if self.management == "global":
@@ -228,6 +242,7 @@ class Buildup:
         t1.record(s)
         t1.synchronize()
         self.steps_done += n_steps
+        self._check_rows()
         return t0.elapsed_time(t1) * 1e-3
 
     def _step_signature(self):

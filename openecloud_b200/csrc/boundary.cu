@@ -259,7 +259,11 @@ __device__ bool wall_cutcell(const WallConst &c, double *r, double *nrm, int G) 
 
 __global__ void k_wall(WallConst c, double *__restrict__ rows, const int32_t *n_abs, int cap,
                        double *__restrict__ normals, int G, oec_status_t *status) {
-    int na = *n_abs < cap ? *n_abs : cap;
+    const int total = *n_abs;
+    int na = total < cap ? total : cap;
+    // rows past the capacity were never gathered: those particles leave the
+    // store without a wall point, so they emit nothing; count them
+    if (blockIdx.x == 0 && threadIdx.x == 0 && total > cap) atomicAdd(&status->n_rows_dropped, total - cap);
     int missing = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += gridDim.x * blockDim.x) {
         double *r = rows + 6 * (int64_t)i;

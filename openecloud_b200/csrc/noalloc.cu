@@ -25,6 +25,8 @@
 //    (cudaGetSymbolAddress); make that first call before any stream capture.
 #include <stdint.h>
 
+#include <mutex>
+
 #include "oec_common.cuh"
 
 namespace {
@@ -44,16 +46,22 @@ struct NoAllocAddr {
     bool ready;
 };
 NoAllocAddr g_addr[kMaxDevices];
+std::mutex g_addr_mu;  // guards g_addr: first calls may come from several threads
 
-int noalloc_setup(int dev) {
+// Copies the device's scratch addresses into *out, looking them up on the
+// first call made with that device current.
+int noalloc_setup(int dev, NoAllocAddr *out) {
     if (dev < 0 || dev >= kMaxDevices) return OEC_ERR_INVALID;
-    if (g_addr[dev].ready) return OEC_OK;
-    void *rho = nullptr, *scale = nullptr;
-    if (cudaGetSymbolAddress(&rho, g_noalloc_rho_fix) != cudaSuccess) return OEC_ERR_CUDA;
-    if (cudaGetSymbolAddress(&scale, g_noalloc_wscale) != cudaSuccess) return OEC_ERR_CUDA;
-    g_addr[dev].rho_fix = static_cast<int64_t *>(rho);
-    g_addr[dev].wscale = static_cast<double *>(scale);
-    g_addr[dev].ready = true;
+    std::lock_guard<std::mutex> lock(g_addr_mu);
+    if (!g_addr[dev].ready) {
+        void *rho = nullptr, *scale = nullptr;
+        if (cudaGetSymbolAddress(&rho, g_noalloc_rho_fix) != cudaSuccess) return OEC_ERR_CUDA;
+        if (cudaGetSymbolAddress(&scale, g_noalloc_wscale) != cudaSuccess) return OEC_ERR_CUDA;
+        g_addr[dev].rho_fix = static_cast<int64_t *>(rho);
+        g_addr[dev].wscale = static_cast<double *>(scale);
+        g_addr[dev].ready = true;
+    }
+    *out = g_addr[dev];
     return OEC_OK;
 }
 
@@ -65,9 +73,9 @@ extern "C" int oec_deposit_charge_noalloc(const oec_grid_t *grid, const oec_part
     if ((int64_t)grid->nx * grid->ny > kNoAllocMaxNodes) return OEC_ERR_CAPACITY;
     int dev = 0;
     OEC_CUDA_TRY(cudaGetDevice(&dev));
-    int rc = noalloc_setup(dev);
+    NoAllocAddr a;
+    int rc = noalloc_setup(dev, &a);
     if (rc != OEC_OK) return rc;
-    const NoAllocAddr &a = g_addr[dev];
     // the scale is recomputed and the grid cleared (zero_first = 1) on every
     // call, so nothing of an earlier call's scratch reaches this result
     rc = oec_deposit_scale(p, a.wscale, stream);

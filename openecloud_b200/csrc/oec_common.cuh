@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "oec.h"
 
 #define OEC_CUDA_TRY(expr)                         \
@@ -20,8 +22,27 @@ constexpr unsigned kFullMask = 0xffffffffu;
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
-// Number of SMs of the current device (cached per process; the library is
-// used with one device per process).
+// Devices a process may drive; per-device caches below are indexed by the
+// CUDA device ordinal.
+constexpr int kMaxDevices = 64;
+
+// A figure that is fixed for a device (an attribute, an occupancy limit),
+// computed by `compute` on the first call made with that device current and
+// kept per device.  Slots hold value + 1 (0 = not computed yet); two threads
+// that race on a first call compute and store the same value.
+template <class F>
+int per_device_cached(std::atomic<int> *slots, F compute) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return compute();
+    int v = slots[dev].load(std::memory_order_relaxed);
+    if (v == 0) {
+        v = compute() + 1;
+        slots[dev].store(v, std::memory_order_relaxed);
+    }
+    return v - 1;
+}
+
+// Number of SMs of the current device (cached per device).
 int sm_count();
 
 // Persistent grid: enough CTAs to cover `work_items` CTA-sized chunks, at

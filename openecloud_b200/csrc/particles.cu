@@ -13,19 +13,20 @@
 #include <math.h>
 #include <stdlib.h>
 
+#include <mutex>
+
 #include "oec_common.cuh"
 
 namespace oec {
 
 int sm_count() {
-    static int cached = 0;
-    if (cached == 0) {
+    static std::atomic<int> cached[kMaxDevices];
+    return per_device_cached(cached, [] {
         int dev = 0, n = 0;
         if (cudaGetDevice(&dev) != cudaSuccess) return 148;
         if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 148;
-        cached = n > 0 ? n : 148;
-    }
-    return cached;
+        return n > 0 ? n : 148;
+    });
 }
 
 namespace {
@@ -1002,13 +1003,16 @@ extern "C" int oec_deposit_scale(const oec_particles_t *p, double *wscale_dev, v
 template <int TB, int KIND, bool DEP>
 static void launch_fused(const FusedArgs &a, int grid_unused, cudaStream_t s) {
     (void)grid_unused;
-    static int per_sm = 0;  // resident CTAs per SM for this instantiation
-    if (per_sm == 0) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_push_gather<TB, KIND, DEP>, kThreads, 0) !=
+    // resident CTAs per SM for this instantiation, per device
+    static std::atomic<int> cached[kMaxDevices];
+    const int per_sm = per_device_cached(cached, [] {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_push_gather<TB, KIND, DEP>, kThreads, 0) !=
                 cudaSuccess ||
-            per_sm < 1)
-            per_sm = 1;
-    }
+            b < 1)
+            b = 1;
+        return b;
+    });
     int64_t chunks = ((int64_t)a.capacity + kChunk - 1) / kChunk;
     k_push_gather<TB, KIND, DEP><<<persistent_grid(chunks, per_sm), kThreads, 0, s>>>(a);
 }
@@ -1226,9 +1230,15 @@ struct Pipe {
     }
 };
 
-Pipe &pipe() {
-    static Pipe p;
-    return p;
+// One pipeline per device; g_pipe_mu is held while a call enqueues its
+// copies, so two host threads never interleave their use of the slots.
+std::mutex g_pipe_mu;
+
+Pipe *pipe() {
+    static Pipe p[kMaxDevices];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+    return &p[dev];
 }
 
 // Ring of staging slots for a whole host-to-host step: uploads on one
@@ -1256,9 +1266,11 @@ struct StepPipe {
     }
 };
 
-StepPipe &step_pipe() {
-    static StepPipe p;
-    return p;
+StepPipe *step_pipe() {
+    static StepPipe p[kMaxDevices];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+    return &p[dev];
 }
 
 __global__ void k_set_count(int32_t *count, int32_t value) { *count = value; }
@@ -1273,7 +1285,10 @@ extern "C" int oec_particles_upload_host(const oec_grid_t *grid, const double *a
         staging_rows < 2)
         return OEC_ERR_INVALID;
     if (n > p->capacity) return OEC_ERR_CAPACITY;
-    Pipe &pp = pipe();
+    std::lock_guard<std::mutex> lock(g_pipe_mu);
+    Pipe *ppp = pipe();
+    if (!ppp) return OEC_ERR_CUDA;
+    Pipe &pp = *ppp;
     int rc = pp.init();
     if (rc != OEC_OK) return rc;
     cudaStream_t s = as_stream(stream);
@@ -1308,7 +1323,10 @@ extern "C" int oec_particles_download_host(const oec_grid_t *grid, const oec_par
     if (!valid_grid(grid) || !valid_particles(p) || n < 0 || (n > 0 && (!aos_host || !staging_dev)) ||
         staging_rows < 2 || n > p->capacity)
         return OEC_ERR_INVALID;
-    Pipe &pp = pipe();
+    std::lock_guard<std::mutex> lock(g_pipe_mu);
+    Pipe *ppp = pipe();
+    if (!ppp) return OEC_ERR_CUDA;
+    Pipe &pp = *ppp;
     int rc = pp.init();
     if (rc != OEC_OK) return rc;
     cudaStream_t s = as_stream(stream);
@@ -1360,7 +1378,10 @@ extern "C" int oec_push_gather_host(const oec_grid_t *grid, oec_particles_t *p, 
                            absorbed_mask_dev, rho_fix_dev, wscale_dev, status_dev, probe);
         if (rc != OEC_OK) return rc;
     }
-    StepPipe &pp = step_pipe();
+    std::lock_guard<std::mutex> lock(g_pipe_mu);
+    StepPipe *ppp = step_pipe();
+    if (!ppp) return OEC_ERR_CUDA;
+    StepPipe &pp = *ppp;
     int rc = pp.init();
     if (rc != OEC_OK) return rc;
     cudaStream_t s = as_stream(stream);

@@ -808,8 +808,8 @@ struct SolveArgs {
     int *fb_count;
 };
 
-// Side streams used to fill the bodies of conditional nodes (per device).
-constexpr int kMaxDevices = 16;
+// Side streams used to fill the bodies of conditional nodes (per device);
+// used only under g_cache_mu.
 cudaStream_t g_side[kMaxDevices][4];
 
 int side_stream(int k, cudaStream_t *out) {
@@ -998,47 +998,48 @@ std::string solve_key(const SolveArgs &a, int dev) {
     return kb.k;
 }
 
+// Instantiated solve graphs keyed by their arguments; g_cache_mu also
+// guards the per-device capture and side streams of build_solve.
 constexpr size_t kMaxCachedSolves = 32;
 std::mutex g_cache_mu;
 std::map<std::string, cudaGraphExec_t> g_cache;
 
-// The solve as an instantiated graph (built on first use).
-int cached_solve(const SolveArgs &a, cudaGraphExec_t *out) {
+// Launches the solve as an instantiated graph on s (built on first use).
+// The lock is held through the launch, so no other thread can evict the
+// graph between the lookup and the launch; a graph destroyed by a later
+// eviction still completes the launches already queued.
+int launch_cached_solve(const SolveArgs &a, cudaStream_t s) {
     int dev = 0;
     OEC_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return OEC_ERR_INVALID;
     const std::string key = solve_key(a, dev);
     std::lock_guard<std::mutex> lock(g_cache_mu);
     auto it = g_cache.find(key);
-    if (it != g_cache.end()) {
-        *out = it->second;
-        return OEC_OK;
-    }
-    if (g_cache.size() >= kMaxCachedSolves) {
-        for (auto &e : g_cache) cudaGraphExecDestroy(e.second);
-        g_cache.clear();
-    }
-    cudaStream_t cap;
-    {
+    if (it == g_cache.end()) {
+        if (g_cache.size() >= kMaxCachedSolves) {
+            for (auto &e : g_cache) cudaGraphExecDestroy(e.second);
+            g_cache.clear();
+        }
         // a stream of its own for the top-level capture (the side streams
         // fill the bodies)
         static cudaStream_t g_cap[kMaxDevices] = {};
         if (!g_cap[dev]) OEC_CUDA_TRY(cudaStreamCreateWithFlags(&g_cap[dev], cudaStreamNonBlocking));
-        cap = g_cap[dev];
+        cudaStream_t cap = g_cap[dev];
+        OEC_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeRelaxed));
+        const int rc = build_solve(a, cap);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(cap, &g);
+        if (rc != OEC_OK || ec != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return rc != OEC_OK ? rc : OEC_ERR_CUDA;
+        }
+        cudaGraphExec_t exec;
+        const cudaError_t ei = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        OEC_CUDA_TRY(ei);
+        it = g_cache.emplace(key, exec).first;
     }
-    OEC_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeRelaxed));
-    const int rc = build_solve(a, cap);
-    cudaGraph_t g = nullptr;
-    const cudaError_t ec = cudaStreamEndCapture(cap, &g);
-    if (rc != OEC_OK || ec != cudaSuccess) {
-        if (g) cudaGraphDestroy(g);
-        return rc != OEC_OK ? rc : OEC_ERR_CUDA;
-    }
-    cudaGraphExec_t exec;
-    const cudaError_t ei = cudaGraphInstantiate(&exec, g, 0);
-    cudaGraphDestroy(g);
-    OEC_CUDA_TRY(ei);
-    g_cache.emplace(key, exec);
-    *out = exec;
+    OEC_CUDA_TRY(cudaGraphLaunch(it->second, s));
     return OEC_OK;
 }
 
@@ -1069,11 +1070,10 @@ int enqueue_solve(const SolveArgs &a, cudaStream_t s) {
     OEC_CUDA_TRY(cudaThreadExchangeStreamCaptureMode(&mode));
     int rc;
     if (cs == cudaStreamCaptureStatusActive) {
+        std::lock_guard<std::mutex> lock(g_cache_mu);  // the side streams are shared per device
         rc = build_solve(a, s);
     } else if (cs == cudaStreamCaptureStatusNone) {
-        cudaGraphExec_t exec;
-        rc = cached_solve(a, &exec);
-        if (rc == OEC_OK && cudaGraphLaunch(exec, s) != cudaSuccess) rc = OEC_ERR_CUDA;
+        rc = launch_cached_solve(a, s);
     } else {
         rc = OEC_ERR_INVALID;
     }

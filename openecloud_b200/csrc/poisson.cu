@@ -400,16 +400,17 @@ inline bool thin_lanes_ok(int g) { return g == 1 || g == 2 || g == 4 || g == 8 |
 // block and the device supports it.
 int solve_wide(const int32_t *rows, const int32_t *level_ptr, int a, int b, const int32_t *ptr, const int32_t *idx,
                const double *val, const double *diag, double *x, bool coop_ok, cudaStream_t s) {
-    static int per_sm = -1;  // resident CTAs per SM of the cooperative kernel (0: no cooperative launch)
-    if (per_sm < 0) {
-        int dev = 0, coop = 0;
-        per_sm = 0;
-        if (cudaGetDevice(&dev) == cudaSuccess &&
-            cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess && coop &&
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trsv_levels, kWarps * 32, 0) != cudaSuccess)
-            per_sm = 0;
+    // resident CTAs per SM of the cooperative kernel, per device (0: no cooperative launch)
+    static std::atomic<int> cached[kMaxDevices];
+    const int per_sm = per_device_cached(cached, [] {
+        int dev = 0, coop = 0, b = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_trsv_levels, kWarps * 32, 0) != cudaSuccess)
+            b = 0;
         cudaGetLastError();
-    }
+        return b;
+    });
     const int n = b - a;
     if (coop_ok && per_sm > 0 && n >= 2 && n <= kCoopMaxLevels) {
         LevelPtr lv = level_ptrs(level_ptr + a, n);

@@ -37,7 +37,16 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 SHIM_DIR = os.path.join(HERE, "gsl_shim")
-DEFAULT_SRC = "/root/reference"
+# Where this build environment mounts the reference tree (read-only); the
+# OEC_REFERENCE environment variable or --src names another one.
+MOUNTED_SRC = "/root/reference"
+
+
+def locate():
+    """The reference source tree to build from, or None when it is absent
+    (the GPU hosts carry only the built modules)."""
+    src = os.environ.get("OEC_REFERENCE", MOUNTED_SRC)
+    return src if os.path.isdir(src) else None
 
 MODULES = ["constants", "randomGen", "specFun", "grid", "particles", "particleBoundary",
            "kdTree", "particleManagement", "particleEmitter", "poissonSolver", "magneticField", "util",
@@ -128,9 +137,12 @@ def build(src):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--src", default=os.environ.get("OEC_REFERENCE", DEFAULT_SRC))
+    ap.add_argument("--src", default=None, help="reference source tree (default: OEC_REFERENCE or the mount)")
     args = ap.parse_args()
-    build(args.src)
+    src = args.src or locate()
+    if src is None:
+        raise SystemExit("reference source tree not found: pass --src or set OEC_REFERENCE")
+    build(src)
 
 
 if __name__ == "__main__":

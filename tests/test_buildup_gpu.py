@@ -100,3 +100,35 @@ def test_cut_cell_buildup_within_reference_spread(gpu):
     bad = np.abs(m_gpu - m_ref) > tol
     assert not bad.any(), (np.nonzero(bad)[0][:10], m_gpu[bad][:5], m_ref[bad][:5])
     assert m_gpu[-1] / m_gpu[0] > 1.2
+
+
+def test_absorbed_rows_beyond_capacity_are_reported(gpu):
+    """A step that absorbs more particles than the absorbed-row buffer holds
+    is counted on the device (status n_rows_dropped) and Buildup.run raises
+    instead of silently losing their secondaries; a large enough buffer
+    drops nothing."""
+    from openecloud_b200.buildup import Buildup
+
+    def make(abs_cap):
+        n = 20000
+        b = Buildup(seed=5, n_init=n, n_steps_table=10, abs_cap=abs_cap)
+        rng = np.random.default_rng(5)
+        a = rng.uniform(0.0, 2 * np.pi, n)
+        pd = np.zeros((n, 6))
+        pd[:, 0] = 0.0195 * np.cos(a)   # 0.5 mm inside the 20 mm wall
+        pd[:, 1] = 0.0195 * np.sin(a)
+        pd[:, 2] = 1e8 * np.cos(a)      # 1 mm outward in one 1e-11 s step
+        pd[:, 3] = 1e8 * np.sin(a)
+        pd[:, 5] = 1e9 / n
+        b.P.setParticleData(pd)
+        b._prepare_deposit()
+        return b
+
+    b = make(1024)
+    with pytest.raises(RuntimeError, match="abs_cap"):
+        b.run(1)
+    assert b.status()["n_rows_dropped"] > 0
+    ok = make(30000)
+    ok.run(1)
+    assert ok.status()["n_rows_dropped"] == 0
+    assert ok.status()["n_absorbed"] == 20000
