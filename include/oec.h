@@ -159,6 +159,16 @@ int oec_boris_push(const oec_grid_t *grid, oec_particles_t *p, const double *e_a
  * node can leave the int64 range whatever the particle distribution. */
 int oec_deposit_scale(const oec_particles_t *p, double *wscale_dev, void *stream);
 
+/* The same scale for one shard of a particle store split over several
+ * stores (one per GPU) whose int64 deposits are summed afterwards: bits =
+ * min(50, 62 - ceil(log2(total_capacity))) with total_capacity the sum of
+ * the shards' capacities (>= p->capacity), so the summed grid stays inside
+ * int64.  The shards then take the smallest of their scales (the largest
+ * weight), which keeps every shard's charges exact.  Replaces the charge
+ * scaling of chargeToGrid (particles.pyx:70-77) for a sharded run. */
+int oec_deposit_scale_capacity(const oec_particles_t *p, int64_t total_capacity, double *wscale_dev,
+                               void *stream);
+
 /* THE HOT PATH.  One pass over all particles:
  *   gather E (and B for type 2) at the current position, Boris push
  *   (type 0/1/2), move, inside test of `boundary` at the new position,
@@ -693,6 +703,88 @@ int oec_multipole_field(int32_t nx, int32_t ny, const double *xmesh_dev, const d
  * sum w over the store (f64); the mean energy in eV is
  * m / (2 e) * sums[0] / sums[1]. */
 int oec_average_energy_sums(const oec_particles_t *p, double *sums_dev, void *stream);
+
+/* ------------------------------------- context and owned handles (session.cu)
+ *
+ * The layer above for hosts that bring no GPU framework of their own: a
+ * context owns a device, a CUDA stream, a device status block and every
+ * device allocation made through it (freed by oec_ctx_destroy); a run owns a
+ * whole buildup run in its context.  The caller-owned entry points above
+ * stay the low-level layer (oec_run_particles hands out the store in that
+ * form).  A context and its runs are used from one host thread at a time. */
+typedef struct oec_ctx oec_ctx_t;
+typedef struct oec_run oec_run_t;
+
+/* A context on CUDA device `device` (its own non-blocking stream). */
+int oec_ctx_create(int32_t device, oec_ctx_t **out);
+/* Waits for the context's stream, frees its allocations and runs' memory. */
+int oec_ctx_destroy(oec_ctx_t *ctx);
+/* The context's stream (cudaStream_t) for the low-level entry points. */
+int oec_ctx_stream(oec_ctx_t *ctx, void **stream);
+int oec_ctx_synchronize(oec_ctx_t *ctx);
+/* `bytes` of zeroed device memory owned by the context. */
+int oec_ctx_alloc(oec_ctx_t *ctx, int64_t bytes, void **dev);
+/* Host copy of the context's status block (the anomaly counters of every
+ * run of the context; synchronises its stream). */
+int oec_status(oec_ctx_t *ctx, oec_status_t *out);
+
+/* The LU factors as oec_lu_t lays them out, every pointer a HOST array of
+ * the host-side setup (SuperLU's factors, poissonSolver.pyx:59, in the
+ * head/tail form; tl_inv/tu_inv the dense inverses of the tail blocks).
+ * Sizes: rhs_node/sol_src/sol_node n; l_rows/u_rows/u_diag head; l_ptr/u_ptr
+ * head+1 (nnz = ptr[head]); lc_ptr m+1 (m = n - head); tl_inv/tu_inv m*m. */
+typedef oec_lu_t oec_lu_host_t;
+
+/* One buildup run (example01_basic.py:36-97).  HOST arrays, copied by
+ * oec_run_create (not kept): rows (n_rows x 6 f64, setParticleData),
+ * beam_profile (nx*ny: LHCBeam*.getTransversalProfile, beam.py:47-63),
+ * beam_table (table_len: the beam's charge factor per step, beam.py:68-78 /
+ * :129-136; the run holds table_len - 1 steps and table_len history
+ * entries), the LU factors and the E operator phiToEAtGridPoints as CSR
+ * (2*nx*ny rows, poissonSolver.pyx:63). */
+typedef struct oec_run_desc {
+    oec_grid_t grid;
+    int32_t boundary_kind;      /* OEC_BOUNDARY_RECT or OEC_BOUNDARY_ELLIPSE */
+    int32_t type_b;             /* borisPush typeBField 0 or 1 (bconst) */
+    double dt, charge, mass;
+    double bconst[3];
+    int64_t capacity;           /* particle store (rounded up to a multiple of 1024) */
+    int32_t abs_cap;            /* absorbed rows per step (more: status n_rows_dropped) */
+    int32_t target;             /* globalRandom target */
+    int32_t management_every;   /* globalRandom cadence in steps (+-5 % band) */
+    int32_t table_len;
+    const double *rows;
+    int64_t n_rows;
+    oec_furman_t furman;
+    uint64_t emit_seed;         /* Philox key of the emission */
+    uint64_t manage_seed;       /* Philox key of the roulette (plus the step) */
+    const double *beam_profile;
+    const double *beam_table;
+    oec_lu_host_t lu;
+    const int32_t *e_ptr, *e_idx;
+    const double *e_val;
+} oec_run_desc_t;
+
+/* Allocates the run in ctx and loads its initial particles (their deposit
+ * and the first history entry included); returns when the host arrays may
+ * be released. */
+int oec_run_create(oec_ctx_t *ctx, const oec_run_desc_t *desc, oec_run_t **out);
+/* Advances n_steps time steps: every step the launch sequence of the loop
+ * (beam + electron right-hand side, LU solve, E, fused push/gather/wall
+ * test/deposit, absorbed set, wall rows, Furman emission, refill, history),
+ * from a CUDA graph captured on the first call when use_graph != 0; at every
+ * management_every-th step globalRandom toward target first.  Returns
+ * OEC_ERR_CAPACITY past the beam table.  Synchronises at the end. */
+int oec_run_steps(oec_run_t *run, int32_t n_steps, int32_t use_graph);
+/* The first n history entries: macro count and sum of weights at the start
+ * of each step (example01_basic.py:56-57). */
+int oec_run_history(oec_run_t *run, int32_t *counts_host, double *weights_host, int32_t n);
+/* getParticleData: up to max_rows (N, 6) f64 rows into rows_host; *n = N. */
+int oec_run_get_rows(oec_run_t *run, double *rows_host, int64_t max_rows, int64_t *n);
+/* The run's particle store in the low-level form (device arrays). */
+int oec_run_particles(oec_run_t *run, oec_particles_t *out);
+/* Releases the run's graph; its device memory goes with the context. */
+int oec_run_destroy(oec_run_t *run);
 
 #ifdef __cplusplus
 }

@@ -64,6 +64,7 @@ SIGNATURES = {
     "oec_gather": [_PG, _PP, _P, _I32, _P, _P],
     "oec_boris_push": [_PG, _PP, _P, _P, _P, _D, _D, _I32, _P],
     "oec_deposit_scale": [_PP, _P, _P],
+    "oec_deposit_scale_capacity": [_PP, _I64, _P, _P],
     "oec_push_gather": [_PG, _PP, _P, _P, _P, _D, _D, _I32, _PB, _P, _P, _P, _P, _P],
     "oec_push_gather_host": [_PG, _PP, _P, _P, _I64, _P, _I64, _P, _P, _P, _D, _D, _I32, _PB, _P, _P, _P, _P,
                              _P],

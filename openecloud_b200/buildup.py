@@ -137,6 +137,13 @@ class Buildup:
         self._prepare_deposit()
         _lib.call("oec_history", self.P.c_particles(), self.step_dev.data_ptr(), self._table_len,
                   self.hist_w.data_ptr(), self.hist_n.data_ptr(), self.scratch.data_ptr(), D.stream())
+        # what a checkpoint must match to be resumed by this run
+        self._signature = {"grid": [int(nx), int(ny), float(lx), float(ly), int(boundType)], "dt": self.dt,
+                           "seed": self.seed, "steps_table": self._table_len, "type_b": self.type_b,
+                           "b_const": [float(b) for b in b_const], "emitter": emitter, "sey_max": float(sey_max),
+                           "target": self.target, "management": management,
+                           "management_every": self.management_every, "beam": beam,
+                           "beam_particles": float(beam_particles)}
         self.graph = None
         self._rows_dropped = 0
         self.n_managed = 0       # management events (roulette / merge) so far
@@ -284,6 +291,67 @@ class Buildup:
             self._capture()
         for _ in range(n):
             self.graph.replay()
+
+    # ------------------------------------------------------ checkpoints
+    def save(self, directory):
+        """Writes the reference's outputs (particleData.npy: (N, 6) float64
+        rows; physicalParticleCount.npy and macroParticleCount.npy: the
+        histories so far, example01_basic.py:76-78) and checkpoint.npz, the
+        exact device state from which `load` resumes this run bit for bit."""
+        from . import checkpoint as C
+        P, ps = self.P, self.ps
+        n = P.getMacroParticleCount()
+        hist_n, hist_w = self.history()
+        C.write_reference_outputs(directory, P.getParticleData(), hist_w[:-1], hist_n[:-1])
+        store = {k: D.to_numpy(P.soa()[k][:n]) for k in C.STORE_FIELDS}
+        arrays = {"rho_fix": D.to_numpy(P._rho_fix), "wscale": D.to_numpy(P._wscale),
+                  "status": D.to_numpy(P._status), "step": D.to_numpy(self.step_dev),
+                  "hist_n": D.to_numpy(self.hist_n), "hist_w": D.to_numpy(self.hist_w),
+                  "phi": D.to_numpy(ps.phi),
+                  "phi_prev": D.to_numpy(ps._phi_prev) if ps._phi_prev is not None else None,
+                  "ws_hist": D.to_numpy(ps._ws_hist) if ps._ws_hist is not None else None}
+        counters = {"steps_done": int(self.steps_done), "n_managed": int(self.n_managed),
+                    "rows_dropped": int(self._rows_dropped)}
+        C.write_checkpoint(directory, self._signature, store, arrays, counters)
+
+    def load(self, directory):
+        """Resumes the run saved by `save` into this one (built with the
+        same configuration): the store, deposit, step counter, histories,
+        warm-start state and counters are restored exactly."""
+        from . import checkpoint as C
+        store, arrays, counters = C.read_checkpoint(directory, self._signature)
+        P, ps = self.P, self.ps
+        n = store["cell"].shape[0]
+        P.ensure_capacity(n)
+        for k in C.STORE_FIELDS:
+            P.soa()[k][:n].copy_(torch.from_numpy(store[k]))
+        P._count.fill_(n)
+        P._rho_fix.copy_(torch.from_numpy(arrays["rho_fix"]))
+        P._wscale.copy_(torch.from_numpy(arrays["wscale"]))
+        P._status.copy_(torch.from_numpy(arrays["status"]))
+        self.step_dev.copy_(torch.from_numpy(arrays["step"]))
+        self.hist_n.copy_(torch.from_numpy(arrays["hist_n"]))
+        self.hist_w.copy_(torch.from_numpy(arrays["hist_w"]))
+        ps.phi.copy_(torch.from_numpy(arrays["phi"]))
+        if "phi_prev" in arrays:
+            ps._phi_prev = D.to_device(arrays["phi_prev"], torch.float64)
+            ps._ws_hist = D.to_device(arrays["ws_hist"], torch.int32)
+        else:
+            ps._phi_prev = ps._ws_hist = None
+        self.steps_done = int(counters["steps_done"])
+        self.n_managed = int(counters["n_managed"])
+        self._rows_dropped = int(counters["rows_dropped"])
+        self.graph = None  # the next replay captures again
+        torch.cuda.synchronize()
+
+    def loadParticleData(self, path):
+        """Restarts from a particleData.npy of (N, 6) float64 rows, as the
+        reference restarts through setParticleData (particles.pyx:126): the
+        rows are converted to the FP32 store and deposited again."""
+        from . import checkpoint as C
+        self.P.setParticleData(C.read_particle_data(path))
+        self._prepare_deposit()
+        self.graph = None
 
     def history(self):
         """(macro count, sum of weights) at the start of every step so far."""

@@ -16,6 +16,15 @@
 
 #define OEC_LAUNCH_CHECK() OEC_CUDA_TRY(cudaGetLastError())
 
+// Returns the status of an entry point or helper that did not succeed.
+#ifndef OEC_TRY
+#define OEC_TRY(expr)                    \
+    do {                                 \
+        const int oec_rc_ = (expr);      \
+        if (oec_rc_ != OEC_OK) return oec_rc_; \
+    } while (0)
+#endif
+
 namespace oec {
 
 constexpr unsigned kFullMask = 0xffffffffu;

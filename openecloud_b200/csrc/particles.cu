@@ -266,40 +266,38 @@ __device__ __forceinline__ void add_node4(unsigned long long *rho, int key, int 
 // four nodes fall outside the window is added to the grid directly, so any
 // particle order gives the same exact result.
 //
-// An int64 charge x is held as three 32-bit planes, x = lo + mid*2^21 +
-// hi*2^42 with lo, mid the 21-bit fields of x and hi = x >> 42 (signed), and
-// each plane is summed with fire-and-forget 32-bit shared atomics (a 64-bit
-// shared add would need a compare-and-swap loop or a carry read back).  A node
-// takes at most one add per particle of the chunk (1024), so the lo and mid
-// sums stay below 2^31 and the hi sum, with |x| < 2^52, below 2^20: no plane
-// overflows, and the recombined total is exact.  The hi plane is only touched
-// for charges of 2^42 units or more (small particle stores); the flush skips
-// it when no thread of the CTA wrote it.
+// An int64 charge x of magnitude below 2^41 is held as two 32-bit planes,
+// x = lo + mid*2^21 with lo = x & (2^21 - 1) (unsigned) and mid = x >> 21
+// (signed, |mid| <= 2^20), each summed with fire-and-forget 32-bit shared
+// atomics (a 64-bit shared add would need a compare-and-swap loop).  A node
+// takes at most one add per particle of the chunk (1024), so the lo sum
+// stays below 2^31 and the mid sum inside +-2^30, also when the copies below
+// are summed: no plane overflows and the recombined total is exact.  A value
+// of 2^41 or more (a run of very heavy particles in a small store) goes to
+// the grid directly instead, so the window never needs a third plane.
 //
 // Dense cells put most lanes of a warp on the same few nodes, and same-address
 // shared atomics serialise; each node therefore has kWinCopies copies of its
 // planes, lane l adding to copy l % kWinCopies, and the flush sums the copies.
-// Layout: word (entry * 3 + plane) * kWinCopies + copy.
+// Layout: word (entry * 2 + plane) * kWinCopies + copy.
 constexpr int kWinRows = 16, kWinCols = 24, kWinNodes = kWinRows * kWinCols;
 constexpr int kWinCopies = 4;
-constexpr int kWinWords = kWinNodes * 3 * kWinCopies;
+constexpr int kWinPlanes = 2;
+constexpr int kWinWords = kWinNodes * kWinPlanes * kWinCopies;
 
 struct NodeWindow {
     unsigned *v;   // shared, kWinWords
     int ox, oy;    // node (column, row) of entry 0
-    bool hi_used;  // this thread wrote the hi plane since the last flush
 
-    __device__ __forceinline__ void add_entry(int e, long long x) {
-        const unsigned lo = (unsigned)x & 0x1fffffu;
-        const unsigned mid = (unsigned)(x >> 21) & 0x1fffffu;
-        const unsigned hi = (unsigned)(x >> 42);
-        unsigned *w = v + e * (3 * kWinCopies) + (threadIdx.x & (kWinCopies - 1));
-        if (lo) atomicAdd(w, lo);
-        if (mid) atomicAdd(w + kWinCopies, mid);
-        if (hi) {
-            atomicAdd(w + 2 * kWinCopies, hi);
-            hi_used = true;
+    // x to window entry e (grid node `node` when x is out of the planes' range)
+    __device__ __forceinline__ void add_entry(int e, long long x, unsigned long long *rho, int node) {
+        if ((unsigned long long)(x + (1LL << 41)) >= (1ULL << 42)) {
+            atomicAdd(rho + node, (unsigned long long)x);
+            return;
         }
+        unsigned *w = v + e * (kWinPlanes * kWinCopies) + (threadIdx.x & (kWinCopies - 1));
+        atomicAdd(w, (unsigned)x & 0x1fffffu);
+        atomicAdd(w + kWinCopies, (unsigned)(int)(x >> 21));
     }
 
     __device__ __forceinline__ void add(int key, const double q[4], unsigned long long *rho, int nx,
@@ -309,10 +307,10 @@ struct NodeWindow {
         const int rx = ix - ox, ry = iy - oy;
         if ((unsigned)rx < (unsigned)(kWinCols - 1) && (unsigned)ry < (unsigned)(kWinRows - 1)) {
             const int e = ry * kWinCols + rx;
-            add_entry(e, __double2ll_rn(q[0]));
-            add_entry(e + 1, __double2ll_rn(q[1]));
-            add_entry(e + kWinCols, __double2ll_rn(q[2]));
-            add_entry(e + kWinCols + 1, __double2ll_rn(q[3]));
+            add_entry(e, __double2ll_rn(q[0]), rho, key);
+            add_entry(e + 1, __double2ll_rn(q[1]), rho, key + 1);
+            add_entry(e + kWinCols, __double2ll_rn(q[2]), rho, key + nx);
+            add_entry(e + kWinCols + 1, __double2ll_rn(q[3]), rho, key + nx + 1);
         } else {
             add_node4(rho, key, nx, q);
         }
@@ -332,24 +330,18 @@ __device__ __forceinline__ void window_anchor(NodeWindow &nw, int first, int nce
 __device__ __forceinline__ unsigned sum4(const uint4 &a) { return a.x + a.y + a.z + a.w; }
 
 // Send the window's nonzero nodes to the grid and clear it (all threads of
-// the CTA, after a barrier that follows the last add; any_hi = some thread
-// wrote the hi plane).  Only entries that a valid cell wrote are nonzero, so
-// every node sent is on the grid.
-__device__ __forceinline__ void window_flush(const NodeWindow &nw, bool any_hi, unsigned long long *rho, int nx) {
+// the CTA, after a barrier that follows the last add).  Only entries that a
+// valid cell wrote are nonzero, so every node sent is on the grid.
+__device__ __forceinline__ void window_flush(const NodeWindow &nw, unsigned long long *rho, int nx) {
     static_assert(kWinCopies == 4, "flush reads the copies of a plane as one uint4");
     const uint4 z = make_uint4(0u, 0u, 0u, 0u);
     for (int e = threadIdx.x; e < kWinNodes; e += blockDim.x) {
-        uint4 *w = reinterpret_cast<uint4 *>(nw.v + e * (3 * kWinCopies));
+        uint4 *w = reinterpret_cast<uint4 *>(nw.v + e * (kWinPlanes * kWinCopies));
         const unsigned lo = sum4(w[0]), mid = sum4(w[1]);
-        unsigned hi = 0u;
-        if (any_hi) {
-            hi = sum4(w[2]);
-            w[2] = z;
-        }
-        if (lo | mid | hi) {
+        if (lo | mid) {
             w[0] = z;
             w[1] = z;
-            const long long x = (long long)lo + ((long long)mid << 21) + (long long)(int)hi * (1LL << 42);
+            const long long x = (long long)lo + (long long)(int)mid * (1LL << 21);
             if (x != 0) atomicAdd(rho + (nw.oy + e / kWinCols) * nx + nw.ox + e % kWinCols, (unsigned long long)x);
         }
     }
@@ -591,8 +583,8 @@ __global__ void __launch_bounds__(kThreads, fused_min_blocks(TB, KIND)) k_push_g
     const int nchunks = (n + kChunk - 1) / kChunk;
     const double wscale = DEP ? *a.wscale : 0.0;
     Tally t;
-    NodeWindow nw{win, 0, 0, false};
-    NodeWindow prev{win, 0, 0, false};  // the previous chunk's window and anchor
+    NodeWindow nw{win, 0, 0};
+    NodeWindow prev{win, 0, 0};  // the previous chunk's window and anchor
     bool have_prev = false;
     int parity = 0;
     if (DEP)
@@ -609,9 +601,8 @@ __global__ void __launch_bounds__(kThreads, fused_min_blocks(TB, KIND)) k_push_g
         if (DEP) {
             w4 = reinterpret_cast<const float4 *>(a.w)[q];
             if (threadIdx.x == 0) first_cell[parity] = c4.x;
-            const bool any_hi = __syncthreads_or(nw.hi_used);
-            nw.hi_used = false;
-            if (have_prev) window_flush(prev, any_hi, a.rho, a.nx);
+            __syncthreads();
+            if (have_prev) window_flush(prev, a.rho, a.nx);
             nw.v = win + parity * kWinWords;
             window_anchor(nw, first_cell[parity], a.ncell, a.nx, a.nx_magic);
         }
@@ -625,8 +616,8 @@ __global__ void __launch_bounds__(kThreads, fused_min_blocks(TB, KIND)) k_push_g
         }
     }
     if (DEP) {
-        const bool any_hi = __syncthreads_or(nw.hi_used);
-        if (have_prev) window_flush(prev, any_hi, a.rho, a.nx);
+        __syncthreads();
+        if (have_prev) window_flush(prev, a.rho, a.nx);
     }
     publish_tally<KIND>(a, t);
 }
@@ -643,7 +634,7 @@ __global__ void __launch_bounds__(kThreads)
     const int n = min(*count, capacity);
     const double wscale = *wscale_p;
     const int nchunks = (n + kChunk - 1) / kChunk;
-    NodeWindow nw{win, 0, 0, false};
+    NodeWindow nw{win, 0, 0};
     for (int e = threadIdx.x; e < kWinWords; e += kThreads) win[e] = 0u;
     for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
         const int q = chunk * kThreads + threadIdx.x;
@@ -670,9 +661,8 @@ __global__ void __launch_bounds__(kThreads)
             }
         }
         acc.deposit(nw, rho, nx, nx_magic);
-        const bool any_hi = __syncthreads_or(nw.hi_used);
-        nw.hi_used = false;
-        window_flush(nw, any_hi, rho, nx);
+        __syncthreads();
+        window_flush(nw, rho, nx);
     }
 }
 
@@ -978,26 +968,33 @@ extern "C" int oec_boris_push(const oec_grid_t *grid, oec_particles_t *p, const 
     return OEC_OK;
 }
 
-static int deposit_bits(const oec_particles_t *p) {
+static int deposit_bits(int64_t capacity) {
     // A node sums at most `capacity` particles of at most 2^bits units:
     // capacity * 2^bits <= 2^62 keeps every node inside int64.  At most 50
     // bits so that the f64 corner products stay exact to well below a unit.
     int lc = 0;
-    while ((int64_t(1) << lc) < p->capacity) ++lc;
+    while ((int64_t(1) << lc) < capacity) ++lc;
     int bits = 62 - lc;
     return bits > 50 ? 50 : bits;
 }
 
-extern "C" int oec_deposit_scale(const oec_particles_t *p, double *wscale_dev, void *stream) {
-    if (!valid_particles(p) || !wscale_dev) return OEC_ERR_INVALID;
+extern "C" int oec_deposit_scale_capacity(const oec_particles_t *p, int64_t total_capacity, double *wscale_dev,
+                                          void *stream) {
+    if (!valid_particles(p) || !wscale_dev || total_capacity < p->capacity || total_capacity > (int64_t(1) << 40))
+        return OEC_ERR_INVALID;
     cudaStream_t s = as_stream(stream);
     OEC_CUDA_TRY(cudaMemsetAsync(wscale_dev, 0, sizeof(double), s));
     k_wmax<<<persistent_grid(cap_chunks(p), 4), kThreads, 0, s>>>(p->w, p->count,
                                                                    reinterpret_cast<int *>(wscale_dev));
     OEC_LAUNCH_CHECK();
-    k_wscale<<<1, 1, 0, s>>>(wscale_dev, deposit_bits(p));
+    k_wscale<<<1, 1, 0, s>>>(wscale_dev, deposit_bits(total_capacity));
     OEC_LAUNCH_CHECK();
     return OEC_OK;
+}
+
+extern "C" int oec_deposit_scale(const oec_particles_t *p, double *wscale_dev, void *stream) {
+    if (!valid_particles(p)) return OEC_ERR_INVALID;
+    return oec_deposit_scale_capacity(p, p->capacity, wscale_dev, stream);
 }
 
 template <int TB, int KIND, bool DEP>

@@ -874,12 +874,6 @@ int capture_graph(cudaStream_t s, cudaGraph_t *g) {
     return cs == cudaStreamCaptureStatusActive ? OEC_OK : OEC_ERR_INVALID;
 }
 
-#define OEC_TRY(expr)                  \
-    do {                               \
-        const int oec_rc_ = (expr);    \
-        if (oec_rc_ != OEC_OK) return oec_rc_; \
-    } while (0)
-
 // Records the whole solve into the capture of s.
 int build_solve(const SolveArgs &a, cudaStream_t s) {
     const oec_stencil_t *st = a.st;

@@ -29,17 +29,8 @@ import torch
 from . import _lib
 from . import device as D
 from .constants import epsilon_0
-
-
-class LU_t(ctypes.Structure):
-    _P = ctypes.c_void_p
-    _fields_ = [("n", ctypes.c_int32), ("head", ctypes.c_int32), ("n_nodes", ctypes.c_int32),
-                ("rhs_node", _P), ("sol_src", _P), ("sol_node", _P),
-                ("l_nlevels", ctypes.c_int32), ("l_level_ptr", _P), ("l_rows", _P),
-                ("l_ptr", _P), ("l_idx", _P), ("l_val", _P), ("lc_ptr", _P), ("lc_idx", _P), ("lc_val", _P),
-                ("tl_inv", _P), ("u_nlevels", ctypes.c_int32), ("u_level_ptr", _P), ("u_rows", _P),
-                ("u_ptr", _P), ("u_idx", _P), ("u_val", _P), ("u_diag", _P), ("tu_inv", _P),
-                ("head_path", ctypes.c_int32), ("l_level_lanes", _P), ("u_level_lanes", _P)]
+from .lu_setup import (LU_t, _level_lists, _levels, _np_ptr, assemble, choose_tail,  # noqa: F401
+                       level_lanes, lu_host_arrays, lu_struct)
 
 
 class Stencil_t(ctypes.Structure):
@@ -198,98 +189,6 @@ def _declare():
         L._poisson_declared = True
     return L
 
-
-def _np_ptr(a):
-    return a.ctypes.data_as(ctypes.c_void_p)
-
-
-def _levels(csr, lower, ncols_dep, nrows=None):
-    L = _declare()
-    nrows = csr.shape[0] if nrows is None else nrows
-    ptr = np.ascontiguousarray(csr.indptr[:nrows + 1], np.int32)
-    idx = np.ascontiguousarray(csr.indices, np.int32)
-    lev = np.zeros(max(nrows, 1), np.int32)
-    nl = ctypes.c_int32(0)
-    rc = L.oec_trsv_levels(nrows, _np_ptr(ptr), _np_ptr(idx), 1 if lower else 0, ncols_dep, _np_ptr(lev),
-                           ctypes.byref(nl))
-    if rc:
-        raise _lib.OecError("oec_trsv_levels", rc)
-    return lev[:nrows], nl.value
-
-
-def _level_lists(lev, nlevels):
-    order = np.argsort(lev, kind="stable").astype(np.int32)
-    counts = np.bincount(lev, minlength=nlevels + 1)[1:]
-    ptr = np.zeros(nlevels + 1, np.int32)
-    np.cumsum(counts, out=ptr[1:])
-    return order, ptr
-
-
-def level_lanes(csr, level_ptr, threads=1024, max_per_lane=16):
-    """Per head level (level-ordered CSR rows): the lanes per row with which
-    one CTA of `threads` threads takes the level in one pass -- the largest
-    power of two up to 32 with rows * lanes <= threads -- or 0 when the level
-    is too wide for that or its longest row would need more than
-    `max_per_lane` loads per lane (such a level keeps a launch of its own)."""
-    level_ptr = np.asarray(level_ptr, np.int64)
-    nl = level_ptr.size - 1
-    lanes = np.zeros(max(nl, 1), np.int8)
-    if nl <= 0:
-        return lanes
-    rows = np.diff(level_ptr)
-    nnz = np.diff(np.asarray(csr.indptr, np.int64))
-    longest = np.zeros(nl, np.int64)
-    ne = rows > 0
-    if nnz.size and ne.any():
-        longest[ne] = np.maximum.reduceat(nnz, level_ptr[:-1][ne])
-    for l in range(nl):
-        r = int(rows[l])
-        if r <= 0 or r > threads:
-            continue
-        g = 1
-        while g < 32 and r * 2 * g <= threads:
-            g *= 2
-        if -(-int(longest[l]) // g) <= max_per_lane:
-            lanes[l] = g
-    return lanes
-
-
-def choose_tail(Lcsr, Ucsr, n, launch_us=8.0, gbs=6000.0, max_tail=16384):
-    """Rows handed to the dense tail: minimise the estimated solve time
-    levels(head) * per-level cost + 2 * (m^2 * 8 B) / bandwidth over a few
-    candidates.  The per-level cost (8 us) and the bandwidth of the dense
-    products were measured on the B200 (128^2 to 1024^2); max_tail bounds the
-    two dense inverses (2 * m^2 * 8 B: 4.3 GB at 16384), and the tail stays
-    within a quarter of the unknowns: on a small grid a larger one streams
-    more through L2 each step than it saves (a 128^2 buildup step ran slower
-    with 6144 tail rows than with 3072 although the solve alone tied)."""
-    best = (None, 0)
-    for m in [0, 256, 512, 1024, 2048, 3072, 4096, 6144, 8192, 12288, 16384]:
-        if m > min(n // 4, max_tail):
-            continue
-        h = n - m
-        _, nl = _levels(Lcsr, True, h, nrows=h)
-        _, nu = _levels(Ucsr, False, h, nrows=h)
-        t = (nl + nu) * launch_us * 1e-6 + 2 * (m * m * 8) / (gbs * 1e9)
-        if best[0] is None or t < best[0]:
-            best = (t, m)
-    return best[1]
-
-
-def assemble(gridObj):
-    """poissonSolver.pyx:41-58: A = S diag(meps) S^T over the inside nodes.
-
-    Returns (A as CSC, meps [2*npExt] edge weights (x edges then y edges),
-    S = [Px | Py] and the inside node indices)."""
-    nx = gridObj.getNxExt()
-    npn = gridObj.getNpExt()
-    inside = np.nonzero(gridObj.getInsidePoints())[0]
-    pxmt = spsp.identity(npn) - spsp.eye(npn, npn, -1)
-    pymt = spsp.identity(npn) - spsp.eye(npn, npn, -int(nx))
-    st = spsp.hstack([pxmt, pymt])
-    meps = epsilon_0 * np.asarray(gridObj.getDsi()) * np.roll(gridObj.getDst(), npn)
-    a = st.dot(spsp.diags(meps, 0).dot(st.transpose()))[:, inside].tocsc()[inside, :]
-    return a, meps, st, inside
 
 
 def stencil_apply_host(meps, inside_mask, nx, x):
@@ -456,73 +355,36 @@ class PoissonSolver:
 
     # -------------------------------------------------------------- setup
     def _device_setup(self, tail):
-        lu = self.ludecom
-        n = lu.shape[0]
-        Lc = lu.L.tocsr()
-        Uc = lu.U.tocsr()
-        Lc.sort_indices()
-        Uc.sort_indices()
-        m = choose_tail(Lc, Uc, n) if tail is None else int(min(max(tail, 0), n))
-        h = n - m
-        self.tail = m
-        ins = self.insidePointsInd.astype(np.int32)
-        inv_pr = np.empty(n, np.int64)
-        inv_pr[lu.perm_r] = np.arange(n)
-        dev = lambda a, dt=torch.int32: D.to_device(np.ascontiguousarray(a), dt)  # noqa: E731
+        """Uploads the head/tail form of the factors (lu_setup.lu_host_arrays);
+        the tail blocks are inverted on the device."""
+        a = lu_host_arrays(self.ludecom, self.insidePointsInd, self.n_nodes, tail, inverses=False)
+        self.tail = m = a["tail"]
         self._keep = {}
         k = self._keep
-        k["rhs_node"] = dev(ins[inv_pr])
-        k["sol_src"] = dev(lu.perm_c.astype(np.int32))
-        k["sol_node"] = dev(ins)
-        # strict lower L, head rows
-        Lh = spsp.tril(Lc[:h, :], k=-1, format="csr")
-        Lh.sort_indices()
-        lev, nl = _levels(Lh, True, h)
-        rows, lptr = _level_lists(lev, nl)
-        k["l_rows"] = dev(rows)
-        Lh = Lh[rows]  # level order: a row's record is read at its position in the level
-        k["l_ptr"], k["l_idx"], k["l_val"] = dev(Lh.indptr), dev(Lh.indices), dev(Lh.data, torch.float64)
-        self._l_level_ptr = lptr
-        self._l_level_lanes = level_lanes(Lh, lptr)
-        # strict upper U, head rows (all columns > row, tail columns included)
-        Uh = spsp.triu(Uc[:h, :], k=1, format="csr")
-        Uh.sort_indices()
-        levu, nu = _levels(Uh, False, h)
-        rowsu, uptr = _level_lists(levu, nu)
-        k["u_rows"] = dev(rowsu)
-        Uh = Uh[rowsu]
-        k["u_ptr"], k["u_idx"], k["u_val"] = dev(Uh.indptr), dev(Uh.indices), dev(Uh.data, torch.float64)
-        k["u_diag"] = dev(Uc.diagonal()[:h][rowsu], torch.float64) if h > 0 else D.zeros(1, torch.float64)
-        self._u_level_ptr = uptr
-        self._u_level_lanes = level_lanes(Uh, uptr)
+        for name in ("rhs_node", "sol_src", "sol_node", "l_rows", "l_ptr", "l_idx", "u_rows", "u_ptr", "u_idx",
+                     "lc_ptr", "lc_idx"):
+            if name in a:
+                k[name] = D.to_device(a[name], torch.int32)
+        for name in ("l_val", "u_val", "u_diag", "lc_val"):
+            if name in a:
+                k[name] = D.to_device(a[name], torch.float64)
         if m > 0:
-            C = Lc[h:, :h].tocsr()
-            C.sort_indices()
-            k["lc_ptr"], k["lc_idx"], k["lc_val"] = dev(C.indptr), dev(C.indices), dev(C.data, torch.float64)
-            TL = D.to_device(Lc[h:, h:].toarray(), torch.float64)
-            TU = D.to_device(Uc[h:, h:].toarray(), torch.float64)
+            TL = D.to_device(a.pop("TL"), torch.float64)
+            TU = D.to_device(a.pop("TU"), torch.float64)
             eye = torch.eye(m, dtype=torch.float64, device=D.device())
             k["tl_inv"] = torch.linalg.solve_triangular(TL, eye, upper=False, unitriangular=True).contiguous()
             k["tu_inv"] = torch.linalg.solve_triangular(TU, eye, upper=True).contiguous()
             del TL, TU, eye
-        else:
-            for name in ("lc_ptr", "lc_idx", "lc_val", "tl_inv", "tu_inv"):
-                k[name] = None
-        s = LU_t()
-        s.n, s.head, s.n_nodes = n, h, self.n_nodes
-        for name in ("rhs_node", "sol_src", "sol_node", "l_rows", "l_ptr", "l_idx", "l_val", "lc_ptr", "lc_idx",
-                     "lc_val", "tl_inv", "u_rows", "u_ptr", "u_idx", "u_val", "u_diag", "tu_inv"):
-            setattr(s, name, D.ptr(k[name]))
-        s.l_nlevels, s.l_level_ptr = nl, _np_ptr(self._l_level_ptr).value
-        s.u_nlevels, s.u_level_ptr = nu, _np_ptr(self._u_level_ptr).value
-        s.l_level_lanes = _np_ptr(self._l_level_lanes).value
-        s.u_level_lanes = _np_ptr(self._u_level_lanes).value
-        self._lu_t = s
-        self._work = D.zeros(n + m + 1, torch.float64)
+        self._lu_host = a  # keeps the host level lists the solve reads
+        self._l_level_ptr, self._u_level_ptr = a["l_level_ptr"], a["u_level_ptr"]
+        self._l_level_lanes, self._u_level_lanes = a["l_level_lanes"], a["u_level_lanes"]
+        self._lu_t = lu_struct(a, lambda name: D.ptr(k.get(name)))
+        self._work = D.zeros(a["n"] + m + 1, torch.float64)
         E = self.phiToEAtGridPoints.tocsr()
         E.sort_indices()
-        k["e_ptr"], k["e_idx"], k["e_val"] = dev(E.indptr), dev(E.indices), dev(E.data, torch.float64)
-        self.levels = (nl, nu)
+        k["e_ptr"], k["e_idx"] = D.to_device(E.indptr, torch.int32), D.to_device(E.indices, torch.int32)
+        k["e_val"] = D.to_device(E.data, torch.float64)
+        self.levels = (a["l_nlevels"], a["u_nlevels"])
 
     # -------------------------------------------------------------- solve
     def _lu_solve(self, q):

@@ -371,3 +371,46 @@ def local_random(pd, target, g, kind=1, seed=None, threshold=2., lambda_factor=1
                                    float(threshold), float(lambda_factor), float(dis_limit), int(scheme),
                                    int(leaf), _p(scratch))
     return a[:k].copy()
+
+
+# ------------------------------------------------- fixed-point deposit
+def deposit_bits(total_capacity):
+    """Fixed-point bits of a particle's charge: capacity * 2^bits <= 2^62
+    keeps any node inside int64; at most 50."""
+    lc = 0
+    while (1 << lc) < total_capacity:
+        lc += 1
+    return min(50, 62 - lc)
+
+
+def deposit_scale(w, total_capacity):
+    """wscale = 2^(bits - ceil(log2 max|w|)) as the device computes it from
+    the FP32 weights (the exponent e of frexp(max|w|))."""
+    m = float(np.max(np.abs(np.asarray(w, np.float32)))) if len(w) else 0.0
+    e = np.frexp(m)[1] if m > 0 and np.isfinite(m) else 0
+    return float(np.ldexp(1.0, deposit_bits(total_capacity) - int(e)))
+
+
+def fixed_point_deposit(cell, ox, oy, w, nx, n_nodes, wscale):
+    """The order-independent int64 deposit of chargeToGrid
+    (particles.pyx:336-351) in the units of wscale: per particle the charge
+    qd = rint(w * wscale) is split into the CIC corner parts
+    rint(qd * (1-fx)(1-fy)), rint(qd * fx(1-fy)), rint(qd * (1-fx)fy) and the
+    remainder (so the four sum to qd exactly), all in round-to-nearest f64,
+    added to nodes cell, cell+1, cell+nx, cell+nx+1.  Particles whose cell
+    has a corner off the grid are skipped."""
+    cell = np.asarray(cell, np.int64)
+    gx = np.asarray(ox, np.float32).astype(np.float64)
+    gy = np.asarray(oy, np.float32).astype(np.float64)
+    qd = np.rint(np.asarray(w, np.float32).astype(np.float64) * wscale)
+    ok = (cell >= 0) & (cell < n_nodes - nx - 1)
+    cell, gx, gy, qd = cell[ok], gx[ok], gy[ok], qd[ok]
+    hx, hy = 1.0 - gx, 1.0 - gy
+    v0 = np.rint(qd * (hx * hy))
+    v1 = np.rint(qd * (gx * hy))
+    v2 = np.rint(qd * (hx * gy))
+    v3 = qd - v0 - v1 - v2
+    rho = np.zeros(n_nodes, np.int64)
+    for off, v in ((0, v0), (1, v1), (nx, v2), (nx + 1, v3)):
+        np.add.at(rho, cell + off, v.astype(np.int64))
+    return rho

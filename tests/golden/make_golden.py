@@ -309,6 +309,40 @@ if __name__ == "__main__" and "--management" in sys.argv:
     management_golden()
 
 
+def management_moments(pd):
+    """count, sum w, sum w v (3 components), sum w |v|^2 of (N, 6) rows."""
+    w = pd[:, 5]
+    v = pd[:, 2:5]
+    return np.array([pd.shape[0], w.sum(), *(w[:, None] * v).sum(0), (w * (v * v).sum(1)).sum()])
+
+
+def management_ensemble_golden(n_seeds=16):
+    """The moments of the reference's localRandom output (both merge schemes,
+    down to 3000 and up to 4600 from the 4000 rows of management.npz) over
+    n_seeds seeds of its random stream."""
+    grid, particles, particleBoundary, poissonSolver, randomGen = _import_reference()
+    import particleManagement
+    pd = np.load(os.path.join(HERE, "management.npz"))["pd"]
+    g = grid.Grid(64, 64, 0.04, 0.04, 1)
+    out = np.zeros((2, 2, n_seeds, 6))
+    for scheme in (0, 1):
+        for t, target in enumerate((3000, 4600)):
+            for k in range(n_seeds):
+                P = particles.Particles("electrons", "variableWeight")
+                P.setParticleData(pd.copy())
+                bd = particleBoundary.AbsorbElliptical(g, P)
+                randomGen.seed(1000 + 31 * scheme + 7 * t + k)
+                particleManagement.localRandom(g, P, bd, target, mergeScheme=scheme)
+                out[scheme, t, k] = management_moments(np.asarray(P.getParticleData()))
+    path = os.path.join(HERE, "management_ensemble.npz")
+    np.savez_compressed(path, moments=out, before=management_moments(pd), targets=np.array([3000, 4600]))
+    print("wrote", path, os.path.getsize(path))
+
+
+if __name__ == "__main__" and "--management-ensemble" in sys.argv:
+    management_ensemble_golden()
+
+
 def reference_buildup(seed, n_steps, **kw):
     """oracle/ref_buildup.py: the reference's own loop on the c1 chamber."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))

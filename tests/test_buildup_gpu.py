@@ -132,3 +132,41 @@ def test_absorbed_rows_beyond_capacity_are_reported(gpu):
     ok.run(1)
     assert ok.status()["n_rows_dropped"] == 0
     assert ok.status()["n_absorbed"] == 20000
+
+
+def test_checkpoint_resume_is_exact(gpu, tmp_path):
+    """A run saved after 120 steps and resumed into a new Buildup continues
+    bit for bit like the run that never stopped (LU solve, roulette every 50
+    steps); the reference-format outputs hold (N, 6) float64 rows and the
+    uint0 count history (example01_basic.py:76-78), and a restart from those
+    rows alone (setParticleData) reproduces the store to FP32 rounding."""
+    from openecloud_b200.buildup import Buildup
+    kw = dict(seed=21, n_steps_table=301)
+    a = Buildup(**kw)
+    a.run(300)
+    b = Buildup(**kw)
+    b.run(120)
+    b.save(str(tmp_path))
+    c = Buildup(**kw)
+    c.load(str(tmp_path))
+    c.run(180)
+    ha, hc = a.history(), c.history()
+    assert np.array_equal(ha[0], hc[0]) and np.array_equal(ha[1], hc[1])
+    assert np.array_equal(a.P.getParticleData(), c.P.getParticleData())
+    rows = np.load(tmp_path / "particleData.npy")
+    assert rows.dtype == np.float64 and np.array_equal(rows, b.P.getParticleData())
+    pc = np.load(tmp_path / "physicalParticleCount.npy")
+    mc = np.load(tmp_path / "macroParticleCount.npy")
+    assert pc.dtype == np.uintp and pc.shape == (120,) and mc.shape == (120,)
+    assert np.array_equal(mc, b.history()[0][:120].astype(np.uintp))
+    r = Buildup(**kw)
+    r.loadParticleData(str(tmp_path))
+    again = r.P.getParticleData()
+    assert again.shape == rows.shape
+    g = r.grid
+    assert np.max(np.abs(again[:, 0] - rows[:, 0])) <= 1e-6 * g.getDx()
+    assert np.max(np.abs(again[:, 2:] - rows[:, 2:])) <= 1e-6 * np.max(np.abs(rows[:, 2:]))
+    wrong = Buildup(seed=22, n_steps_table=301)
+    from openecloud_b200.checkpoint import CheckpointError
+    with pytest.raises(CheckpointError):
+        wrong.load(str(tmp_path))

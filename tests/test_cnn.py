@@ -18,8 +18,7 @@ import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-sys.path.insert(0, os.path.join(ROOT, "oracle"))
-import cnn_oracle  # noqa: E402
+from oracle import cnn_oracle  # noqa: E402
 
 
 def test_oracle_gradient_finite_differences():

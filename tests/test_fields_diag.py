@@ -82,3 +82,49 @@ def test_buildup_with_multipole_field(gpu):
     nf, wf = free.history()
     assert np.all(np.isfinite(wq)) and nq[-1] > 0
     assert not np.array_equal(wq, wf)
+
+
+@pytest.mark.gpu
+def test_rhs_with_beam_matches_reference_charge(gpu):
+    """oec_rhs_with_beam (the per-step Poisson right-hand side of the device
+    loop: electron deposit + beam imprint, example01_basic.py:81) against the
+    electron charge of the FP64 oracle plus the reference's own
+    beam.getCharge(step * dt) (beam.py:68-78 train, :129-136 endless) at
+    steps inside and between bunches."""
+    import torch
+    from conftest import golden
+    from oracle import oracle as O
+    from openecloud_b200 import _lib
+    from openecloud_b200 import device as D
+    from openecloud_b200.beam import LHCBeam, LHCBeamEndless
+    from openecloud_b200.grid import Grid
+    from openecloud_b200.particles import Particles
+    z = golden("beam.npz")
+    g = Grid(64, 48, 0.04, 0.03, 1)
+    og = O.GridGeom(64, 48, 0.04, 0.03)
+    rng = np.random.default_rng(4)
+    n = 50000
+    r = np.sqrt(rng.uniform(0, 1, n)) * 0.98
+    a = rng.uniform(0, 2 * np.pi, n)
+    pd = np.zeros((n, 6))
+    pd[:, 0], pd[:, 1] = r * np.cos(a) * 0.02, r * np.sin(a) * 0.015
+    pd[:, 5] = rng.uniform(0.5, 1.5, n) * 1e5
+    P = Particles("electrons", "variableWeight")
+    P.setParticleData(pd)
+    P.chargeToGrid(g)
+    q_e = O.charge_to_grid(P.getParticleData(), og, P.particleCharge)
+    steps = [int(round(t / 1e-11)) for t in z["times"][:6]]
+    G = g.getNpExt()
+    for beam, key in ((LHCBeamEndless(g, 1e-11, nParticles=1.1e11), "endless_charge"),
+                      (LHCBeam(g, 1e-11, nParticles=1.15e11), "train_charge")):
+        table = D.to_device(beam.scalarTable(max(steps) + 1), torch.float64)
+        profile = D.to_device(beam.getTransversalProfile(), torch.float64)
+        for k, st in enumerate(steps):
+            step_dev = D.to_device(np.array([st]), torch.int32)
+            rho = D.zeros(G, torch.float64)
+            _lib.call("oec_rhs_with_beam", g.c_grid(), P._rho_fix.data_ptr(), P._wscale.data_ptr(),
+                      P.particleCharge, profile.data_ptr(), table.data_ptr(), step_dev.data_ptr(), table.shape[0],
+                      rho.data_ptr(), D.stream())
+            expect = q_e + z[key][k]
+            err = np.max(np.abs(D.to_numpy(rho) - expect))
+            assert err <= 1e-12 * np.max(np.abs(q_e)) + 1e-13 * np.max(np.abs(z[key][k])), (key, st, err)

@@ -29,7 +29,10 @@ def test_library_exports_all_declared_symbols():
 
 
 def test_python_signatures_cover_header():
-    import openecloud_b200  # noqa: F401  (imports every binding module)
+    import importlib
+    import openecloud_b200
     from openecloud_b200 import _lib
+    for m in openecloud_b200.__all__:  # every binding module registers its entry points
+        importlib.import_module("openecloud_b200." + m)
     missing = [n for n in declared_symbols() if n not in _lib.SIGNATURES and n not in _lib.OTHER_DECLARED]
     assert not missing, missing

@@ -93,6 +93,50 @@ def test_local_random_statistics(gpu, scheme, tag, target):
         assert abs(ekin(after) / ekin(before) - 1) < 0.05
 
 
+def _moments(pd):
+    w = pd[:, 5]
+    v = pd[:, 2:5]
+    return np.array([pd.shape[0], w.sum(), *(w[:, None] * v).sum(0), (w * (v * v).sum(1)).sum()])
+
+
+@pytest.mark.parametrize("scheme", [0, 1])
+@pytest.mark.parametrize("t,target", [(0, 3000), (1, 4600)])
+def test_local_random_ensemble_moments(gpu, scheme, t, target):
+    """16 seeds of the device merge against 16 seeds of the reference's
+    kd-tree merge (particleManagement.pyx:74-238) on the same 4000 rows: the
+    ensemble means of the count, the total weight, the momentum (sum w v) and
+    the energy (sum w |v|^2) agree within 4 combined standard errors (plus a
+    floor of 0.2 % of the value before the merge, and 1.5 % of the count).
+    Scheme 0 keeps one of the two velocities with probability proportional
+    to its weight, so momentum and energy are conserved in expectation
+    whatever the pairing; scheme 1 rescales the kept velocity by the
+    reference's factor, whose mean depends on how alike the paired
+    velocities are."""
+    from openecloud_b200.particleManagement import localRandom
+    z = golden("management.npz")
+    ref = golden("management_ensemble.npz")
+    before = ref["before"]
+    mine = []
+    for k in range(16):
+        g, P, bd = _setup(z["pd"])
+        localRandom(g, P, bd, target, mergeScheme=scheme, seed=500 + k)
+        mine.append(_moments(P.getParticleData()))
+    mine = np.array(mine) / before
+    theirs = ref["moments"][scheme, t] / before
+    names = ["count", "weight", "px", "py", "pz", "energy"]
+    for i, name in enumerate(names):
+        a, b = mine[:, i], theirs[:, i]
+        se = np.sqrt(a.var(ddof=1) / len(a) + b.var(ddof=1) / len(b))
+        floor = 0.015 if name == "count" else 0.002
+        if name.startswith("p"):  # momentum components: relative to the total momentum magnitude
+            floor = 0.002 * np.linalg.norm(before[2:5]) / abs(before[2 + i - 2])
+        print(f"scheme {scheme} target {target} {name}: device {a.mean():.5f} +- {a.std():.5f}, "
+              f"reference {b.mean():.5f} +- {b.std():.5f}")
+        assert abs(a.mean() - b.mean()) <= 4 * se + floor, name
+    if scheme == 0:
+        assert np.all(np.abs(mine[:, 1] - 1) < 1e-5)  # every merge and split conserves the weight
+
+
 def _search_sorted_ref(a, value):
     # particleManagement.pyx:244-262 as written
     n = a.shape[0]

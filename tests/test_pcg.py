@@ -84,8 +84,7 @@ def test_mg_coarse_level_is_directional_galerkin_product(args):
     import scipy.sparse as spsp
     from openecloud_b200.grid import Grid
     from openecloud_b200.poissonSolver import assemble, mg_coarsen, mg_factors
-    sys_path_oracle()
-    from mg_oracle import parent
+    from oracle.mg_oracle import parent
     g = Grid(*args)
     a, meps, _, ins = assemble(g)
     nx, ny = g.getNxExt(), g.getNyExt()
@@ -136,14 +135,6 @@ def test_mg_hierarchy_layout():
         assert smem(block) <= MG_BLOCK_SMEM and len(sizes) - block <= 8 and top(block) <= max(MG_BLOCK_TOP, 100)
         assert block == 0 or smem(block - 1) > MG_BLOCK_SMEM or len(sizes) - block + 1 > 8 or \
             top(block - 1) > MG_BLOCK_TOP
-
-
-def sys_path_oracle():
-    import os
-    import sys
-    d = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle")
-    if d not in sys.path:
-        sys.path.insert(0, d)
 
 
 def _supports_polygon():
@@ -234,8 +225,7 @@ def test_mg_vcycle_matches_oracle(gpu, name):
     import torch
     from openecloud_b200 import device as D
     from openecloud_b200.poissonSolver import PoissonSolver, _declare
-    sys_path_oracle()
-    from mg_oracle import vcycle
+    from oracle.mg_oracle import vcycle
     z = golden(f"grid_{name}.npz")
     ps = PoissonSolver(_grid(z), method="pcg", precond="mg")
     mg = ps._mg_setup()
