@@ -224,6 +224,103 @@ def bench_config(n, nx, ny, world):
             "l2": "inputs 470 MB per step > 126 MB L2 (no flush needed)"}
 
 
+def cpu_reference_c3(n_particles=2_000_000, solves=3):
+    """The compiled reference on the production shapes, on one host core:
+    SuperLU setup and back-substitution + E on the 512x512 and 1024x1024
+    ellipses (45 x 18 mm half-axes), and one particle step of 2e6 electrons
+    on the 1024x1024 ellipse at B_y = 8.33 T (weights, deposit, gather, Boris
+    push, wall test); a production passage (5000 steps) is estimated as
+    5000 x (solve + particle step).  None without oracle/_ref."""
+    mods = _ref_modules()
+    if mods is None:
+        return None
+    rgrid, rparticles, rboundary = mods
+    import poissonSolver as rps
+    out = {"cores": 1, "kind": "reference"}
+    for nodes in (512, 1024):
+        g = rgrid.Grid(nodes, nodes, 0.09, 0.036, 1)
+        t0 = time.perf_counter()
+        ps = rps.PoissonSolver(g)
+        setup = time.perf_counter() - t0
+        q = np.zeros(g.getNpExt())
+        ins = np.asarray(g.getInsidePoints()) != 0
+        q[ins] = np.random.default_rng(1).uniform(0, 1e-12, int(ins.sum()))
+        ps.solve(q)
+        t0 = time.perf_counter()
+        for _ in range(solves):
+            ps.solve(q)
+        out[f"lu_solve_ms_{nodes}"] = (time.perf_counter() - t0) / solves * 1e3
+        out[f"lu_setup_s_{nodes}"] = setup
+    rng = np.random.default_rng(3)
+    r = np.sqrt(rng.uniform(0, 1, n_particles)) * 0.99
+    a = rng.uniform(0, 2 * np.pi, n_particles)
+    pd = np.zeros((n_particles, 6))
+    pd[:, 0], pd[:, 1] = r * np.cos(a) * 0.045, r * np.sin(a) * 0.018
+    pd[:, 2:5] = rng.normal(0.0, np.sqrt(5.0 * QE / ME), (n_particles, 3))
+    pd[:, 5] = 1e3
+    P = rparticles.Particles("electrons", "variableWeight")
+    P.setParticleData(pd)
+    P.setBConst(np.array([0.0, 8.33, 0.0]))
+    bd = rboundary.AbsorbElliptical(g, P)
+    E = np.zeros(2 * g.getNpExt())
+
+    def step():
+        P.calcGridWeights(g)
+        P.chargeToGrid(g)
+        P.eFieldToParticles(g, E)
+        P.borisPush(5e-12, 1)
+        bd.indexInside()
+    step()
+    P.setParticleData(pd.copy())
+    t0 = time.perf_counter()
+    step()
+    out["particle_step_ms_2e6"] = (time.perf_counter() - t0) * 1e3
+    out["s_per_passage_estimate"] = 5000 * (out["lu_solve_ms_1024"] + out["particle_step_ms_2e6"]) * 1e-3
+    out["sample"] = (f"{solves} solves per grid after one untimed; one particle step of {n_particles} electrons; "
+                     "passage = 5000 x (1024^2 solve + particle step)")
+    return out
+
+
+def _ref_scan_worker(args):
+    """One run of the batched scan on the compiled reference (its own loop,
+    oracle/ref_buildup.py): seconds of `steps` steps after the setup."""
+    cfg, steps = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_buildup
+    t = {}
+    ref_buildup.reference_buildup(int(cfg["seed"]), steps, nx=cfg["nx"], ny=cfg["ny"], lx=cfg["lx"], ly=cfg["ly"],
+                                  boundType=cfg["boundType"], n_init=cfg["n_init"], target=cfg["target"], timing=t)
+    return t["seconds"]
+
+
+def cpu_reference_scan(n_runs=64, steps=50):
+    """The batched scan on the host cores, process-parallel: K = nproc
+    single-threaded processes of the compiled reference's loop, each on one
+    run of the scan (the first K runs of the 64), `steps` steps each; the
+    throughput is K * steps run-steps over the slowest process's time.  The
+    reference's loop has no dipole field or SEY scan (c1's emitter and beam
+    on each run's grid and chamber)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    try:
+        import ref_buildup
+    except Exception:
+        return None
+    if not ref_buildup.available():
+        return None
+    import multiprocessing as mp
+    from openecloud_b200.batch import scan_configs
+    k = os.cpu_count() or 1
+    cfgs = scan_configs(n_runs)[:k]
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(k) as pool:
+        secs = pool.map(_ref_scan_worker, [(c, steps) for c in cfgs])
+    wall = time.perf_counter() - t0
+    return {"run_steps_per_s": k * steps / max(secs), "processes": k, "cores": k, "kind": "reference",
+            "steps_per_run": steps, "slowest_run_s": max(secs), "wall_s_with_setup": wall,
+            "grids": [f"{c['nx']}^2" for c in cfgs],
+            "sample": f"{k} single-threaded processes (process-parallel), one scan run each, {steps} steps"}
+
+
 PASSAGE = ("c1 buildup: 128x128 circular chamber R=20 mm, 1e4 initial electrons at rest, endless train "
            "1.1e11 p/bunch, sigma_r 2 mm, sigma_t 0.25 ns, 25 ns spacing, copper SEY deltaMax 1.6 (Emax 300 eV), "
            "roulette cap 1e5 every 50 steps, dt=1e-11 s; one bunch passage = 2500 steps")
@@ -353,10 +450,11 @@ def production_passage(steps=100, warm=10):
     ones, with the LU and the multigrid-preconditioned iterative Poisson
     solve (one factorisation shared), scaled to a 5000-step passage; plus the
     solve comparison on the same 1024x1024 elliptical grid."""
+    import torch
     from openecloud_b200.buildup import Buildup
     kw = dict(nx=1024, ny=1024, lx=0.09, ly=0.036, boundType=1, n_init=2_200_000, w_init=1e3, dt=5e-12,
               beam_particles=1.15e11, radius_sigma=1e-3, sey_max=1.8, type_b_field=1, b_const=(0., 8.33, 0.),
-              target=2_000_000, management="local", management_every=10, n_steps_table=steps + warm + 1, seed=2000)
+              target=2_000_000, management="local", management_every=10, n_steps_table=steps + warm + 25, seed=2000)
     t0 = time.perf_counter()
     lu = Buildup(**kw)
     setup = time.perf_counter() - t0
@@ -368,8 +466,17 @@ def production_passage(steps=100, warm=10):
     out["s_per_passage_lu"] = t_lu / steps * 5000
     out["final_macro_particles_lu"] = int(lu.history()[0][-1])
     out["management_events_lu"] = lu.n_managed
+    def iterations(b, n=20):
+        """Mean PCG iterations per solve over n more steps (one replay each)."""
+        its = []
+        for _ in range(n):
+            b.run(1)
+            its.append(b.ps.lastStats.iterations)
+        return float(np.mean(its))
+
+    lu.ps.resetHistory()
     m = Buildup(poisson=lu.ps, **kw)
-    m.ps.method, m.ps.precond = "pcg", "mg"
+    m.ps.method, m.ps.precond, m.ps.warmStart = "pcg", "mg", "extrapolate"
     fb0 = m.ps.nFallbacks
     m.run(warm)
     t_mg = m.run(steps)
@@ -377,6 +484,34 @@ def production_passage(steps=100, warm=10):
     out["pcg_mg_fallbacks"] = m.ps.nFallbacks - fb0
     out["final_macro_particles_pcg_mg"] = int(m.history()[0][-1])
     out["management_events_pcg_mg"] = m.n_managed
+    out["pcg_mg_iterations_per_solve"] = iterations(m)
+    from openecloud_b200.train_c5 import WEIGHTS
+    if os.path.exists(WEIGHTS):
+        # learned correction of the extrapolated warm start (the network
+        # trained on pairs of this production run, openecloud_b200.train_c5)
+        from openecloud_b200.cnn import PoissonCNN
+        lu.ps.resetHistory()
+        c = Buildup(poisson=lu.ps, **kw)
+        c.ps.method, c.ps.precond, c.ps.warmStart = "pcg", "mg", "extrapolate+cnn"
+        c.ps.cnn = PoissonCNN.for_solver(c.ps, weights=np.load(WEIGHTS).astype(np.float64), training=False)
+        fb0 = c.ps.nFallbacks
+        c.run(warm)
+        t_c = c.run(steps)
+        out["s_per_passage_pcg_mg_learned"] = t_c / steps * 5000
+        out["pcg_mg_learned_fallbacks"] = c.ps.nFallbacks - fb0
+        out["pcg_mg_learned_iterations_per_solve"] = iterations(c)
+        out["final_macro_particles_pcg_mg_learned"] = int(c.history()[0][-1])
+        x = torch.randn(c.ps.n_nodes, device="cuda", dtype=torch.float32)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c.ps.cnn.forward(x)
+        e0.record()
+        for _ in range(10):
+            c.ps.cnn.forward(x)
+        e1.record()
+        e1.synchronize()
+        out["network_forward_ms"] = e0.elapsed_time(e1) / 10
+        lu.ps.cnn = None
+        lu.ps.warmStart = "extrapolate"
     out["timing"] = (f"device time (CUDA events) of {steps} steps after {warm} untimed ones (the management "
                      "events and graph captures of those steps included) x 5000/steps")
     return out
@@ -726,6 +861,17 @@ def run_ours(args, rank, world, local_rank):
              f"{production['poisson_solve']['lu_ms']:.2f} ms LU, {production['poisson_solve']['mg_cold_ms']:.2f} ms "
              f"MG-PCG cold, {production['poisson_solve']['mg_warm_ms']:.2f} ms warm")
 
+    cpu_c3 = cpu_scan = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.no_production:
+        cpu_c3 = cpu_reference_c3()
+        if cpu_c3 is not None:
+            _log(f"reference c3 shapes: LU 512^2 {cpu_c3['lu_solve_ms_512']:.0f} ms, 1024^2 "
+                 f"{cpu_c3['lu_solve_ms_1024']:.0f} ms, particle step 2e6 {cpu_c3['particle_step_ms_2e6']:.0f} ms")
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.no_batch:
+        cpu_scan = cpu_reference_scan()
+        if cpu_scan is not None:
+            _log(f"reference scan, process-parallel: {cpu_scan['run_steps_per_s']:.1f} run-steps/s on "
+                 f"{cpu_scan['processes']} processes")
     components = None
     if rank == 0 and world == 1 and not args.no_components:
         components = component_rooflines(peak)
@@ -762,6 +908,10 @@ def run_ours(args, rank, world, local_rank):
             line["production_passage"] = production
         if batch is not None:
             line["batched_scan"] = batch
+            if cpu_scan is not None:
+                batch["cpu_reference"] = cpu_scan
+        if production is not None and cpu_c3 is not None:
+            production["cpu_reference"] = cpu_c3
         if components is not None:
             line["component_rooflines"] = components
         print(json.dumps(line), flush=True)

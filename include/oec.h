@@ -615,6 +615,17 @@ int oec_cnn_forward(const oec_cnn_t *c, const float *x_dev, float *z_dev, void *
 int64_t oec_cnn_warm_start_work_bytes(int32_t nx, int32_t ny);
 int oec_cnn_warm_start(const oec_cnn_t *c, double scale32, const double *q_dev, double *phi_dev, void *work_dev,
                        void *stream);
+/* Learned correction of the extrapolated warm start: with d = q - 2 q1 + q2,
+ * the second difference in time of the charge (q1, q2: the two previous
+ * charges, kept in q_hist_dev [2*nx*ny] and advanced here; *count_dev, the
+ * number of earlier charges saturating at 2, starts at 0), phi += |b| N(b/|b|)
+ * with b = scale32 * d on the inside nodes.  Since A (phi_n - 2 phi_n-1 +
+ * phi_n-2) = d, this adds the network's estimate of what the linear
+ * extrapolation 2 phi_n-1 - phi_n-2 misses.  Nothing is added while fewer
+ * than two earlier charges exist.  work_dev: oec_cnn_correct_work_bytes. */
+int64_t oec_cnn_correct_work_bytes(int32_t nx, int32_t ny);
+int oec_cnn_correct(const oec_cnn_t *c, double scale32, const double *q_dev, double *q_hist_dev, int32_t *count_dev,
+                    double *phi_dev, void *work_dev, void *stream);
 /* bf16 parameters from f32 ones. */
 int oec_cnn_set_weights(const oec_cnn_t *c, const float *w32_dev, void *stream);
 /* One training step on one input x: z = N(x); the loss is either the

@@ -18,12 +18,16 @@ some run has changed.
 
 No reference counterpart: the reference runs one simulation per process.
 """
+import concurrent.futures
+import os
+
 import numpy as np
 import torch
 
 from .autotune import Autotuner
 from .buildup import Buildup
 from .grid import Grid
+from .lu_setup import factor
 from .poissonSolver import PoissonSolver
 
 GRID_KEYS = (("nx", 128), ("ny", 128), ("lx", 0.04), ("ly", 0.04), ("boundType", 1))
@@ -54,11 +58,18 @@ class BatchedBuildup:
         self.management_every = every.pop()
         self.shared = {}
         self.runs = []
+        # the host setup of every distinct grid (geometry, assembly, SuperLU
+        # factorisation: seconds each on the larger grids) in parallel
+        # threads -- scipy's splu releases the GIL -- before the device setups
+        keys = list(dict.fromkeys(tuple(cfg.get(k, d) for k, d in GRID_KEYS) for cfg in runs))
+        grids = {key: Grid(*key) for key in keys}
+        with concurrent.futures.ThreadPoolExecutor(max_workers=min(len(keys), os.cpu_count() or 1)) as ex:
+            facts = dict(zip(keys, ex.map(lambda k: factor(grids[k]), keys)))
         for cfg in runs:
             key = tuple(cfg.get(k, d) for k, d in GRID_KEYS)
             if key not in self.shared:
-                g = Grid(*key)
-                ps = PoissonSolver(g)
+                g = grids[key]
+                ps = PoissonSolver(g, factors=facts.pop(key))
                 if poisson is None:
                     self.tuner.poisson(ps)
                 elif poisson == "mg":

@@ -29,7 +29,7 @@ class Cnn_t(ctypes.Structure):
 
 _lib.OTHER_DECLARED.update({"oec_cnn_num_params", "oec_cnn_param_layout", "oec_cnn_act_bytes", "oec_cnn_forward",
                             "oec_cnn_set_weights", "oec_cnn_train_step", "oec_cnn_warm_start_work_bytes",
-                            "oec_cnn_warm_start"})
+                            "oec_cnn_warm_start", "oec_cnn_correct_work_bytes", "oec_cnn_correct"})
 
 SPECS = [(1, 16), (16, 32), (32, 64), (64, 64), (64, 32), (32, 16), (16, 16)]  # (in, out) of e0 e1 e2 e3 d2 d1 d0
 
@@ -52,6 +52,10 @@ def _declare():
         L.oec_cnn_warm_start_work_bytes.argtypes = [ctypes.c_int32, ctypes.c_int32]
         L.oec_cnn_warm_start.restype = ctypes.c_int
         L.oec_cnn_warm_start.argtypes = [ctypes.POINTER(Cnn_t), ctypes.c_double, P, P, P, P]
+        L.oec_cnn_correct_work_bytes.restype = ctypes.c_int64
+        L.oec_cnn_correct_work_bytes.argtypes = [ctypes.c_int32, ctypes.c_int32]
+        L.oec_cnn_correct.restype = ctypes.c_int
+        L.oec_cnn_correct.argtypes = [ctypes.POINTER(Cnn_t), ctypes.c_double, P, P, P, P, P, P]
         L.oec_cnn_train_step.restype = ctypes.c_int
         L.oec_cnn_train_step.argtypes = [ctypes.POINTER(Cnn_t), P, P, P, P, P, P, P, P, P, ctypes.c_float,
                                          ctypes.c_int32, ctypes.c_int32, P, P]
@@ -133,6 +137,19 @@ class PoissonCNN:
             self._ws_work = D.empty(int(L.oec_cnn_warm_start_work_bytes(self.nx, self.ny)), torch.uint8)
         self._check(L.oec_cnn_warm_start(ctypes.byref(self.c), float(scale32), q.data_ptr(), phi.data_ptr(),
                                          self._ws_work.data_ptr(), D.stream()), "warm_start")
+        return phi
+
+    def correct(self, scale32, q, q_hist, count, phi):
+        """phi += the network's estimate of A^-1 (q - 2 q1 + q2), the part of
+        phi that the linear extrapolation in time misses (q_hist: device f64
+        [2 * nx * ny] holding q1, q2; count: device int32, earlier charges
+        seen, saturating at 2; both advanced here)."""
+        L = _declare()
+        if getattr(self, "_corr_work", None) is None:
+            self._corr_work = D.empty(int(L.oec_cnn_correct_work_bytes(self.nx, self.ny)), torch.uint8)
+        self._check(L.oec_cnn_correct(ctypes.byref(self.c), float(scale32), q.data_ptr(), q_hist.data_ptr(),
+                                      count.data_ptr(), phi.data_ptr(), self._corr_work.data_ptr(), D.stream()),
+                    "correct")
         return phi
 
     def _op_arg(self, loss):

@@ -512,6 +512,37 @@ __global__ void k_ws_out(int n, const float *__restrict__ z, const uint8_t *__re
         phi[p] = inside[p] ? f * (double)z[p] : 0.0;
 }
 
+// d = q - 2 q1 + q2 (the second difference in time of the charge, 0 while
+// fewer than two earlier charges exist: *count < 2), then q2 <- q1, q1 <- q;
+// the sum of |s d|^2 over the inside nodes goes to sum.
+__global__ void k_corr_diff(int n, const double *__restrict__ q, double *__restrict__ q1, double *__restrict__ q2,
+                            const int32_t *count, const uint8_t *__restrict__ inside, double s, double *__restrict__ d,
+                            double *sum) {
+    const bool have = *count >= 2;
+    double a = 0.0;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const double qn = q[p], a1 = q1[p];
+        const double v = (have && inside[p]) ? qn - 2.0 * a1 + q2[p] : 0.0;
+        d[p] = v;
+        q2[p] = a1;
+        q1[p] = qn;
+        a += (s * v) * (s * v);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(kFullMask, a, off);
+    if ((threadIdx.x & 31) == 0 && a != 0.0) atomicAdd(sum, a);
+}
+
+__global__ void k_corr_count(int32_t *count) { *count = min(*count + 1, 2); }
+
+// phi += |s d| z on the inside nodes.
+__global__ void k_corr_add(int n, const float *__restrict__ z, const uint8_t *__restrict__ inside, const double *sum,
+                           double *__restrict__ phi) {
+    const double f = sqrt(sum[0]);
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+        if (inside[p]) phi[p] += f * (double)z[p];
+}
+
 // Adam on the f32 master weights; writes the bf16 copy.
 __global__ void k_adam(int n, float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m,
                        float *__restrict__ v, bf16 *__restrict__ w16, float lr, float b1, float b2, float eps,
@@ -800,6 +831,35 @@ extern "C" int oec_cnn_train_step(const oec_cnn_t *c, const oec_stencil_t *op, c
 extern "C" int oec_cnn_set_weights(const oec_cnn_t *c, const float *w32_dev, void *stream) {
     if (!c || !c->w16 || !w32_dev) return OEC_ERR_INVALID;
     k_to_bf16<<<grid_for(kNParams), 256, 0, as_stream(stream)>>>(kNParams, w32_dev, reinterpret_cast<bf16 *>(c->w16));
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+extern "C" int64_t oec_cnn_correct_work_bytes(int32_t nx, int32_t ny) {
+    if (nx < 3 || ny < 3) return -1;
+    return (int64_t)(al(sizeof(double) * (size_t)nx * ny) + 2 * al(sizeof(float) * (size_t)nx * ny) + 256);
+}
+
+extern "C" int oec_cnn_correct(const oec_cnn_t *c, double scale32, const double *q_dev, double *q_hist_dev,
+                               int32_t *count_dev, double *phi_dev, void *work_dev, void *stream) {
+    if (!valid_cnn(c) || !q_dev || !q_hist_dev || !count_dev || !phi_dev || !work_dev || !(scale32 > 0.0))
+        return OEC_ERR_INVALID;
+    cudaStream_t s = as_stream(stream);
+    const size_t n0 = (size_t)c->nx * c->ny;
+    char *w = static_cast<char *>(work_dev);
+    double *d = reinterpret_cast<double *>(w);
+    float *x = reinterpret_cast<float *>(w + al(sizeof(double) * n0));
+    float *z = reinterpret_cast<float *>(w + al(sizeof(double) * n0) + al(sizeof(float) * n0));
+    double *sum = reinterpret_cast<double *>(w + al(sizeof(double) * n0) + 2 * al(sizeof(float) * n0));
+    OEC_CUDA_TRY(cudaMemsetAsync(sum, 0, sizeof(double), s));
+    k_corr_diff<<<grid_for(n0), 256, 0, s>>>((int)n0, q_dev, q_hist_dev, q_hist_dev + n0, count_dev, c->inside,
+                                             scale32, d, sum);
+    k_corr_count<<<1, 1, 0, s>>>(count_dev);
+    k_ws_scale<<<grid_for(n0), 256, 0, s>>>((int)n0, d, c->inside, scale32, sum, x);
+    OEC_LAUNCH_CHECK();
+    int rc = oec_cnn_forward(c, x, z, stream);
+    if (rc) return rc;
+    k_corr_add<<<grid_for(n0), 256, 0, s>>>((int)n0, z, c->inside, sum, phi_dev);
     OEC_LAUNCH_CHECK();
     return OEC_OK;
 }

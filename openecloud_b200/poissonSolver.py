@@ -29,7 +29,7 @@ import torch
 from . import _lib
 from . import device as D
 from .constants import epsilon_0
-from .lu_setup import (LU_t, _level_lists, _levels, _np_ptr, assemble, choose_tail,  # noqa: F401
+from .lu_setup import (LU_t, _level_lists, _levels, _np_ptr, assemble, choose_tail, factor,  # noqa: F401
                        level_lanes, lu_host_arrays, lu_struct)
 
 
@@ -208,15 +208,16 @@ class PoissonSolver:
     """Reference: poissonSolver.pyx:33-67 (setup) and :83-98 (solve, getters)."""
 
     def __init__(self, gridObj, tail=None, method="lu", precond="jacobi", pcgTol=1e-8, pcgMaxIter=4000,
-                 warmStart="extrapolate"):
+                 warmStart="extrapolate", factors=None):
+        """factors: the result of lu_setup.factor(gridObj) when the host
+        setup (assembly and SuperLU factorisation) was done beforehand, e.g.
+        for several grids in parallel threads."""
         nx = gridObj.getNxExt()
         npn = gridObj.getNpExt()
         self.gridObj = gridObj
-        a, meps, st, self.insidePointsInd = assemble(gridObj)
+        a, meps, st, self.insidePointsInd, self.ludecom, self.phiToEAtGridPoints = \
+            factors if factors is not None else factor(gridObj)
         self.systemMatrix = a
-        self.ludecom = spspl.splu(a, permc_spec='MMD_AT_PLUS_A', diag_pivot_thresh=0.1)
-        self.phiToEAtGridPoints = gridObj.getEdgeToNode().dot(
-            spsp.diags(gridObj.getDsi(), 0, (2 * npn, 2 * npn)).dot(st.transpose()))
         self.n_nodes = npn
         self._device_setup(tail)
         self._stencil_setup(meps, nx, npn)
@@ -231,6 +232,8 @@ class PoissonSolver:
         self.warmStart = warmStart  # 'previous' (last phi), 'extrapolate' (2 phi_n-1 - phi_n-2), 'zero' or 'cnn'
         self._phi_prev = None    # phi of the solve before the last ('extrapolate')
         self._ws_hist = None     # device count of the solutions seen, saturating at 2 ('extrapolate')
+        self._q_hist = None      # the two previous charges ('extrapolate+cnn')
+        self._q_count = None     # device count of the charges seen, saturating at 2
         self.nSolves = 0
         # statistics of the last iterative solve and the count of LU
         # fallbacks stay on the device (no host round trip per solve)
@@ -339,6 +342,7 @@ class PoissonSolver:
         s._stats_dev = torch.zeros_like(self._stats_dev)
         s._fb_count = torch.zeros_like(self._fb_count)
         s._phi_prev = s._ws_hist = None
+        s._q_hist = s._q_count = None
         s._pcg_used = False
         s.nSolves = 0
         s.cnn = None
@@ -405,6 +409,13 @@ class PoissonSolver:
         """Iterative solves that missed pcgTol and were redone by LU."""
         return int(D.to_numpy(self._fb_count)[0])
 
+    def resetHistory(self):
+        """Forgets the earlier solutions and charges the warm starts use
+        (when one solver object is handed from one run to the next)."""
+        self._phi_prev = self._ws_hist = None
+        self._q_hist = self._q_count = None
+        self.phi.zero_()
+
     def prepare(self):
         """Builds what the configured iterative solve needs (the multigrid
         hierarchy) ahead of a CUDA graph capture that records the solve."""
@@ -412,7 +423,12 @@ class PoissonSolver:
             if torch.cuda.is_current_stream_capturing():
                 raise RuntimeError("PoissonSolver.prepare() must run before the graph capture")
             self._mg_setup()
-        if self.method == "pcg" and self.warmStart == "extrapolate" and self._phi_prev is None:
+        if self.method == "pcg" and self.warmStart == "extrapolate+cnn" and self._q_hist is None:
+            if torch.cuda.is_current_stream_capturing():
+                raise RuntimeError("PoissonSolver.prepare() must run before the graph capture")
+            self._q_hist = D.zeros(2 * self.n_nodes, torch.float64)
+            self._q_count = D.zeros(1, torch.int32)
+        if self.method == "pcg" and self.warmStart in ("extrapolate", "extrapolate+cnn") and self._phi_prev is None:
             if torch.cuda.is_current_stream_capturing():
                 raise RuntimeError("PoissonSolver.prepare() must run before the graph capture")
             self._phi_prev = self.phi.clone()
@@ -433,18 +449,22 @@ class PoissonSolver:
             ctx = self.cnn.c_handle()
         if self.warmStart == "zero":
             self.phi.zero_()
-        elif self.warmStart == "extrapolate":
+        elif self.warmStart in ("extrapolate", "extrapolate+cnn"):
             self.prepare()
             rc = _declare().oec_warm_start_extrapolate(self.phi.data_ptr(), self._phi_prev.data_ptr(), self.n_nodes,
                                                        self._ws_hist.data_ptr(), D.stream())
             if rc:
                 raise _lib.OecError("oec_warm_start_extrapolate", rc)
+            if self.warmStart == "extrapolate+cnn":
+                if self.cnn is None:
+                    raise ValueError("warmStart='extrapolate+cnn' needs a trained network in PoissonSolver.cnn")
+                self.cnn.correct(self._stencil.scale32, q, self._q_hist, self._q_count, self.phi)
         elif self.warmStart == "cnn":
             if self.cnn is None:
                 raise ValueError("warmStart='cnn' needs a trained network in PoissonSolver.cnn")
             self.cnn.warm_start(self._stencil.scale32, q, self.phi)
         elif self.warmStart != "previous":
-            raise ValueError("warmStart must be 'previous', 'extrapolate', 'zero' or 'cnn'")
+            raise ValueError("warmStart must be 'previous', 'extrapolate', 'extrapolate+cnn', 'zero' or 'cnn'")
         rc = _declare().oec_pcg_solve_async(ctypes.byref(self._stencil), q.data_ptr(), self.phi.data_ptr(),
                                             self.pcgTol, self.pcgMaxIter, pc, ctx, self._pcg_work.data_ptr(),
                                             self._stats_dev.data_ptr(), ctypes.byref(self._lu_t),
