@@ -715,6 +715,12 @@ int oec_multipole_field(int32_t nx, int32_t ny, const double *xmesh_dev, const d
  * m / (2 e) * sums[0] / sums[1]. */
 int oec_average_energy_sums(const oec_particles_t *p, double *sums_dev, void *stream);
 
+/* Index checks of the bounds-checked build (liboec_checked.so, built with
+ * -DOEC_BOUNDS_CHECK): the number of out-of-range grid node and particle
+ * indices that its kernels met and skipped since load (or the last reset);
+ * -1 from the normal build, which does not check. */
+int oec_bound_violations(int64_t *out, int32_t reset);
+
 /* ------------------------------------- context and owned handles (session.cu)
  *
  * The layer above for hosts that bring no GPU framework of their own: a

@@ -7,7 +7,9 @@ import ctypes
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "liboec.so")
+# OEC_BOUNDS_CHECK=1 selects the bounds-checked build (liboec_checked.so:
+# out-of-range indices are counted by oec_bound_violations and skipped)
+LIB_PATH = os.path.join(_HERE, "liboec_checked.so" if os.environ.get("OEC_BOUNDS_CHECK") == "1" else "liboec.so")
 
 OEC_OK = 0
 ERRORS = {1: "invalid argument", 2: "CUDA runtime error", 3: "capacity exceeded",
@@ -89,6 +91,7 @@ SIGNATURES = {
     "oec_rhs_with_beam": [_PG, _P, _P, _D, _P, _P, _P, _I32, _P, _P],
     "oec_history": [_PP, _P, _I32, _P, _P, _P, _P],
     "oec_step_advance": [_P, _P],
+    "oec_bound_violations": [_P, _I32],
 }
 _INT64_RETURNING = {"oec_sort_work_bytes": [_I64]}
 

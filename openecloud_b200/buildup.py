@@ -69,7 +69,7 @@ class Buildup:
                  material="copper", sey_max=1.6, e_hat0=300.0, type_b_field=0, b_const=(0., 0., 0.),
                  target=100000, management="global", management_every=50, capacity=None, seed=0,
                  n_steps_table=2500, sort_every=0, boundFunc=None, poisson=None, grid=None, b_multipoles=None,
-                 b_skew=(), emitter="furman", abs_cap=None):
+                 b_skew=(), emitter="furman", abs_cap=None, metrics_log=None):
         if grid is not None and (grid.nx, grid.ny, grid.lx, grid.ly, grid.boundType) != (nx, ny, lx, ly, boundType):
             raise ValueError("grid: another grid than nx, ny, lx, ly, boundType describe")
         self.grid = grid if grid is not None else Grid(nx, ny, lx, ly, boundType, boundFunc=boundFunc)
@@ -144,6 +144,7 @@ class Buildup:
                            "target": self.target, "management": management,
                            "management_every": self.management_every, "beam": beam,
                            "beam_particles": float(beam_particles)}
+        self.metrics_log = metrics_log  # path: one JSON line per management interval
         self.graph = None
         self._rows_dropped = 0
         self.n_managed = 0       # management events (roulette / merge) so far
@@ -192,6 +193,22 @@ class Buildup:
                   self.hist_n.data_ptr(), self.scratch.data_ptr(), s)
         del L
 
+    def _log_metrics(self, step):
+        """Appends one JSON line to metrics_log: the state at the start of
+        `step` (macro count, sum of weights), the anomaly counters and the
+        last iterative solve's statistics."""
+        import json
+        n = int(self.hist_n[step].item()) if step < self._table_len else None
+        w = float(self.hist_w[step].item()) if step < self._table_len else None
+        rec = {"step": step, "macro_particles": n, "sum_weights": w, "managed": self.n_managed,
+               "status": {k: v for k, v in self.P.status().items() if v}}
+        st = self.ps.lastStats
+        if st is not None:
+            rec["solve"] = {"iterations": st.iterations, "refinements": st.refinements, "converged": st.converged,
+                            "rel_residual": st.rel_residual, "fallbacks": self.ps.nFallbacks}
+        with open(self.metrics_log, "a") as f:
+            f.write(json.dumps(rec) + "\n")
+
     def _check_rows(self):
         """Raises if a step absorbed more particles than the absorbed-row
         buffer holds: those particles were removed without a wall row and
@@ -234,18 +251,22 @@ class Buildup:
             if self.sort_every and step % self.sort_every == 0 and step > 0:
                 self.P.sortByColumn(6)
             if step % self.management_every == 0:
-                self._manage(step)
+                with torch.cuda.nvtx.range(f"management {step}"):
+                    self._manage(step)
             # steps until the next management / sort point
             nxt = n_steps - k
             for every in (self.management_every, self.sort_every):
                 if every:
                     nxt = min(nxt, every - (step % every))
-            if use_graph:
-                self._replay(nxt)
-            else:
-                for _ in range(nxt):
-                    self._launch_step()
+            with torch.cuda.nvtx.range(f"buildup steps {step}..{step + nxt - 1}"):
+                if use_graph:
+                    self._replay(nxt)
+                else:
+                    for _ in range(nxt):
+                        self._launch_step()
             k += nxt
+            if self.metrics_log:
+                self._log_metrics(step + nxt)
         t1.record(s)
         t1.synchronize()
         self.steps_done += n_steps
@@ -266,6 +287,13 @@ class Buildup:
         """Records one time step into a CUDA graph (on a capture stream of its
         own; torch.cuda.graph's garbage collection per capture would cost
         more than the step)."""
+        torch.cuda.nvtx.range_push("capture step graph")
+        try:
+            self._capture_step()
+        finally:
+            torch.cuda.nvtx.range_pop()
+
+    def _capture_step(self):
         self.ps.prepare()
         if self._cap_stream is None:
             self._cap_stream = torch.cuda.Stream()

@@ -133,6 +133,7 @@ __global__ void k_gather_rows(oec_particles_t p, const int32_t *__restrict__ ind
     int na = *n_abs < cap ? *n_abs : cap;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += gridDim.x * blockDim.x) {
         int k = index[i];
+        if (!OEC_IN_BOUNDS(k, *p.count)) continue;
         int ix, iy;
         split_cell(p.cell[k], nx, inv_nx, ix, iy);
         double *r = rows + 6 * (int64_t)i;
@@ -336,7 +337,7 @@ __global__ void k_place_added(AddArgs a) {
         }
         const double *r = a.add_rows + 6 * (int64_t)k;
         store_row(a.p, dst, r, a.nx, a.ny, a.dxi, a.dyi, a.lxh, a.lyh);
-        if (a.rho) {
+        if (a.rho && OEC_IN_BOUNDS(a.p.cell[dst] + a.nx + 1, a.nx * a.ny)) {
             int c = a.p.cell[dst];
             double q = (double)llrint((double)a.p.w[dst] * *a.wscale);
             double gx = (double)a.p.ox[dst], gy = (double)a.p.oy[dst];
@@ -390,7 +391,7 @@ __global__ void __launch_bounds__(1024) k_fill_holes(AddArgs a, const uint32_t *
         const int before = block_excl_scan(absorbed, nullptr, sh);  // its barriers publish holes_before
         if (!absorbed) {
             const int k = S + (p - Nnew) - (holes_before + before);
-            if (k < A) copy_particle(a.p, a.holes[k], p);
+            if (k < A && OEC_IN_BOUNDS(a.holes[k], Nnew)) copy_particle(a.p, a.holes[k], p);
         }
         __syncthreads();  // holes_before is rewritten by the next chunk
     }
@@ -417,6 +418,9 @@ __global__ void k_mask_from_keep(const uint16_t *__restrict__ keep, int n, uint3
 }
 
 }  // namespace
+
+OEC_BOUND_QUERY(bound_violations_boundary)
+
 }  // namespace oec
 
 using namespace oec;

@@ -576,6 +576,7 @@ struct Buffers {  // activation workspace (bf16 unless noted)
     bf16 *gd0, *gu0, *gd1, *gu1, *gd2, *gu2, *ge3, *gp3, *ge2, *gp2, *ge1, *gp1, *ge0;
     float *gz, *res;
     double *sums;
+    int *err;  // set by a tensor-core convolution whose bounded wait gave up
 };
 
 size_t al(size_t b) { return (b + 255) & ~size_t(255); }
@@ -601,6 +602,7 @@ size_t carve_buffers(void *base, int nx, int ny, bool training, Buffers *b) {
         return p;
     };
     Buffers t{};
+    t.err = (int *)take(256);
     t.x16 = (bf16 *)take(sz(0, 1));
     t.e0 = (bf16 *)take(sz(0, 16));
     t.p1 = (bf16 *)take(sz(1, 16));
@@ -640,14 +642,17 @@ size_t carve_buffers(void *base, int nx, int ny, bool training, Buffers *b) {
 int grid_for(size_t n, int per_sm = 8) { return persistent_grid((int64_t)((n + 255) / 256), per_sm); }
 
 template <int CI, int CO>
-int conv3(const Level &L, const bf16 *in, const bf16 *w, bf16 *out, cudaStream_t s) {
+int conv3(const Level &L, const bf16 *in, const bf16 *w, bf16 *out, int *err, cudaStream_t s) {
+    (void)err;
     constexpr int smem = conv_smem_bytes<CI, CO>();
-    static bool attr = false;
-    if (!attr) {
-        if (cudaFuncSetAttribute(k_conv3_mma<CI, CO>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
-            return OEC_ERR_CUDA;
-        attr = true;
-    }
+    static std::atomic<int> attr[kMaxDevices];
+    if (per_device_cached(attr, [] {
+            return cudaFuncSetAttribute(k_conv3_mma<CI, CO>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) ==
+                           cudaSuccess
+                       ? 1
+                       : 0;
+        }) != 1)
+        return OEC_ERR_CUDA;
     const int tiles = L.h * ((L.w + kTX - 1) / kTX);
     k_conv3_mma<CI, CO><<<persistent_grid(tiles, 2), 128, smem, s>>>(L.h, L.w, in, w, out);
     OEC_LAUNCH_CHECK();
@@ -688,18 +693,18 @@ int forward(const oec_cnn_t *c, const float *x, Buffers &b, cudaStream_t s) {
     k_conv3_in1<<<grid_for(n0), 256, 0, s>>>(L[0].h, L[0].w, x, c->inside, w + conv_offset(0), b.e0, b.x16);
     OEC_LAUNCH_CHECK();
     pool<16>(L[0], L[1], b.e0, b.p1, s);
-    int rc = conv3<16, 32>(L[1], b.p1, w + conv_offset(1), b.e1, s);
+    int rc = conv3<16, 32>(L[1], b.p1, w + conv_offset(1), b.e1, b.err, s);
     if (rc) return rc;
     pool<32>(L[1], L[2], b.e1, b.p2, s);
-    if ((rc = conv3<32, 64>(L[2], b.p2, w + conv_offset(2), b.e2, s))) return rc;
+    if ((rc = conv3<32, 64>(L[2], b.p2, w + conv_offset(2), b.e2, b.err, s))) return rc;
     pool<64>(L[2], L[3], b.e2, b.p3, s);
-    if ((rc = conv3<64, 64>(L[3], b.p3, w + conv_offset(3), b.e3, s))) return rc;
+    if ((rc = conv3<64, 64>(L[3], b.p3, w + conv_offset(3), b.e3, b.err, s))) return rc;
     up_add<64>(L[2], L[3], 1.f, b.e3, b.e2, b.u2, s);
-    if ((rc = conv3<64, 32>(L[2], b.u2, w + conv_offset(4), b.d2, s))) return rc;
+    if ((rc = conv3<64, 32>(L[2], b.u2, w + conv_offset(4), b.d2, b.err, s))) return rc;
     up_add<32>(L[1], L[2], 1.f, b.d2, b.e1, b.u1, s);
-    if ((rc = conv3<32, 16>(L[1], b.u1, w + conv_offset(5), b.d1, s))) return rc;
+    if ((rc = conv3<32, 16>(L[1], b.u1, w + conv_offset(5), b.d1, b.err, s))) return rc;
     up_add<16>(L[0], L[1], 1.f, b.d1, b.e0, b.u0, s);
-    if ((rc = conv3<16, 16>(L[0], b.u0, w + conv_offset(6), b.d0, s))) return rc;
+    if ((rc = conv3<16, 16>(L[0], b.u0, w + conv_offset(6), b.d0, b.err, s))) return rc;
     OEC_LAUNCH_CHECK();
     return OEC_OK;
 }
@@ -792,29 +797,29 @@ extern "C" int oec_cnn_train_step(const oec_cnn_t *c, const oec_stencil_t *op, c
                                                 grad_dev + kOutOffset);
     // d0 = conv(u0)
     conv3_dw(L[0], 16, 16, b.u0, b.gd0, grad_dev + conv_offset(6), s);
-    if ((rc = conv3<16, 16>(L[0], b.gd0, wt + conv_offset(6), b.gu0, s))) return rc;
+    if ((rc = conv3<16, 16>(L[0], b.gd0, wt + conv_offset(6), b.gu0, b.err, s))) return rc;
     // u0 = up(d1) + e0
     down_sum<16>(L[0], L[1], b.gu0, b.gd1, s);
     // d1 = conv(u1)
     conv3_dw(L[1], 32, 16, b.u1, b.gd1, grad_dev + conv_offset(5), s);
-    if ((rc = conv3<16, 32>(L[1], b.gd1, wt + conv_offset(5), b.gu1, s))) return rc;
+    if ((rc = conv3<16, 32>(L[1], b.gd1, wt + conv_offset(5), b.gu1, b.err, s))) return rc;
     // u1 = up(d2) + e1
     down_sum<32>(L[1], L[2], b.gu1, b.gd2, s);
     // d2 = conv(u2)
     conv3_dw(L[2], 64, 32, b.u2, b.gd2, grad_dev + conv_offset(4), s);
-    if ((rc = conv3<32, 64>(L[2], b.gd2, wt + conv_offset(4), b.gu2, s))) return rc;
+    if ((rc = conv3<32, 64>(L[2], b.gd2, wt + conv_offset(4), b.gu2, b.err, s))) return rc;
     // u2 = up(e3) + e2
     down_sum<64>(L[2], L[3], b.gu2, b.ge3, s);
     // e3 = conv(p3)
     conv3_dw(L[3], 64, 64, b.p3, b.ge3, grad_dev + conv_offset(3), s);
-    if ((rc = conv3<64, 64>(L[3], b.ge3, wt + conv_offset(3), b.gp3, s))) return rc;
+    if ((rc = conv3<64, 64>(L[3], b.ge3, wt + conv_offset(3), b.gp3, b.err, s))) return rc;
     // p3 = pool(e2); e2 also feeds u2
     up_add<64>(L[2], L[3], 0.25f, b.gp3, b.gu2, b.ge2, s);
     conv3_dw(L[2], 32, 64, b.p2, b.ge2, grad_dev + conv_offset(2), s);
-    if ((rc = conv3<64, 32>(L[2], b.ge2, wt + conv_offset(2), b.gp2, s))) return rc;
+    if ((rc = conv3<64, 32>(L[2], b.ge2, wt + conv_offset(2), b.gp2, b.err, s))) return rc;
     up_add<32>(L[1], L[2], 0.25f, b.gp2, b.gu1, b.ge1, s);
     conv3_dw(L[1], 16, 32, b.p1, b.ge1, grad_dev + conv_offset(1), s);
-    if ((rc = conv3<32, 16>(L[1], b.ge1, wt + conv_offset(1), b.gp1, s))) return rc;
+    if ((rc = conv3<32, 16>(L[1], b.ge1, wt + conv_offset(1), b.gp1, b.err, s))) return rc;
     up_add<16>(L[0], L[1], 0.25f, b.gp1, b.gu0, b.ge0, s);
     conv3_dw(L[0], 1, 16, b.x16, b.ge0, grad_dev + conv_offset(0), s);
     OEC_LAUNCH_CHECK();

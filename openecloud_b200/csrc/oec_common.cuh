@@ -29,6 +29,45 @@ namespace oec {
 
 constexpr unsigned kFullMask = 0xffffffffu;
 
+// Index checks of the bounds-checked build (-DOEC_BOUNDS_CHECK, built as
+// liboec_checked.so by `python -m openecloud_b200.build --bounds-check`):
+// OEC_IN_BOUNDS(i, n) is true when 0 <= i < n; otherwise it adds one to the
+// library's violation counter (read with oec_bound_violations) and is false,
+// so the guarded access is skipped instead of faulting.  In the normal build
+// it is the constant true and costs nothing.
+// Each translation unit counts its own violations (device variables are not
+// shared between units of this non-relocatable build);
+// bound_violations_{particles,boundary} read and reset them on the host.
+#ifdef OEC_BOUNDS_CHECK
+namespace {
+__device__ unsigned long long g_bound_violations = 0;
+}
+__device__ __forceinline__ bool in_bounds_checked(long long i, long long n) {
+    if (i >= 0 && i < n) return true;
+    atomicAdd(&g_bound_violations, 1ULL);
+    return false;
+}
+#define OEC_IN_BOUNDS(i, n) (::oec::in_bounds_checked((long long)(i), (long long)(n)))
+#define OEC_BOUND_QUERY(name)                                                                 \
+    int name(unsigned long long *out, bool reset) {                                           \
+        OEC_CUDA_TRY(cudaMemcpyFromSymbol(out, g_bound_violations, sizeof(*out)));            \
+        if (reset) {                                                                          \
+            const unsigned long long z = 0;                                                   \
+            OEC_CUDA_TRY(cudaMemcpyToSymbol(g_bound_violations, &z, sizeof(z)));              \
+        }                                                                                     \
+        return OEC_OK;                                                                        \
+    }
+#else
+#define OEC_IN_BOUNDS(i, n) true
+#define OEC_BOUND_QUERY(name)                               \
+    int name(unsigned long long *out, bool) {              \
+        *out = 0;                                          \
+        return OEC_OK;                                     \
+    }
+#endif
+int bound_violations_particles(unsigned long long *out, bool reset);
+int bound_violations_boundary(unsigned long long *out, bool reset);
+
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
 // Devices a process may drive; per-device caches below are indexed by the

@@ -332,7 +332,8 @@ __device__ __forceinline__ unsigned sum4(const uint4 &a) { return a.x + a.y + a.
 // Send the window's nonzero nodes to the grid and clear it (all threads of
 // the CTA, after a barrier that follows the last add).  Only entries that a
 // valid cell wrote are nonzero, so every node sent is on the grid.
-__device__ __forceinline__ void window_flush(const NodeWindow &nw, unsigned long long *rho, int nx) {
+__device__ __forceinline__ void window_flush(const NodeWindow &nw, unsigned long long *rho, int nx, int nodes) {
+    (void)nodes;
     static_assert(kWinCopies == 4, "flush reads the copies of a plane as one uint4");
     const uint4 z = make_uint4(0u, 0u, 0u, 0u);
     for (int e = threadIdx.x; e < kWinNodes; e += blockDim.x) {
@@ -342,7 +343,8 @@ __device__ __forceinline__ void window_flush(const NodeWindow &nw, unsigned long
             w[0] = z;
             w[1] = z;
             const long long x = (long long)lo + (long long)(int)mid * (1LL << 21);
-            if (x != 0) atomicAdd(rho + (nw.oy + e / kWinCols) * nx + nw.ox + e % kWinCols, (unsigned long long)x);
+            const int node = (nw.oy + e / kWinCols) * nx + nw.ox + e % kWinCols;
+            if (x != 0 && OEC_IN_BOUNDS(node, nodes)) atomicAdd(rho + node, (unsigned long long)x);
         }
     }
 }
@@ -522,7 +524,7 @@ __device__ __forceinline__ void process_group(const FusedArgs &a, int q, int n, 
                 }
                 out = !in;
                 // --- charge of the survivor at its new position
-                if (DEP && !out) {
+                if (DEP && !out && OEC_IN_BOUNDS(cc[j], a.ncell)) {
                     double v[4];
                     corner_charges(ww[j], dox, doy, wscale, v);
                     acc.add(cc[j], v, nw, a.rho, a.nx, a.nx_magic);
@@ -602,7 +604,7 @@ __global__ void __launch_bounds__(kThreads, fused_min_blocks(TB, KIND)) k_push_g
             w4 = reinterpret_cast<const float4 *>(a.w)[q];
             if (threadIdx.x == 0) first_cell[parity] = c4.x;
             __syncthreads();
-            if (have_prev) window_flush(prev, a.rho, a.nx);
+            if (have_prev) window_flush(prev, a.rho, a.nx, a.ncell + a.nx + 1);
             nw.v = win + parity * kWinWords;
             window_anchor(nw, first_cell[parity], a.ncell, a.nx, a.nx_magic);
         }
@@ -617,7 +619,7 @@ __global__ void __launch_bounds__(kThreads, fused_min_blocks(TB, KIND)) k_push_g
     }
     if (DEP) {
         __syncthreads();
-        if (have_prev) window_flush(prev, a.rho, a.nx);
+        if (have_prev) window_flush(prev, a.rho, a.nx, a.ncell + a.nx + 1);
     }
     publish_tally<KIND>(a, t);
 }
@@ -662,7 +664,7 @@ __global__ void __launch_bounds__(kThreads)
         }
         acc.deposit(nw, rho, nx, nx_magic);
         __syncthreads();
-        window_flush(nw, rho, nx);
+        window_flush(nw, rho, nx, ncell + nx + 1);
     }
 }
 
@@ -767,7 +769,25 @@ __global__ void __launch_bounds__(kThreads) k_index_inside(FusedArgs a) {
 
 using namespace oec;
 
+namespace oec {
+OEC_BOUND_QUERY(bound_violations_particles)
+}  // namespace oec
+
 // =================================================================== C ABI
+
+extern "C" int oec_bound_violations(int64_t *out, int32_t reset) {
+    if (!out) return OEC_ERR_INVALID;
+#ifdef OEC_BOUNDS_CHECK
+    unsigned long long a = 0, b = 0;
+    OEC_TRY(bound_violations_particles(&a, reset != 0));
+    OEC_TRY(bound_violations_boundary(&b, reset != 0));
+    *out = (int64_t)(a + b);
+#else
+    (void)reset;
+    *out = -1;  // the normal build does not count
+#endif
+    return OEC_OK;
+}
 
 static bool aligned16(const void *ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 15u) == 0; }
 

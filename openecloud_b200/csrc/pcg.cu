@@ -710,10 +710,16 @@ int mg_cycle(const oec_mg_t *mg, const float *r, float *z, const float *q, Acc *
     P.om = mg->omega;
     P.scale = mg->scale;
     const size_t smem = mg_block_smem(mg);
-    static size_t attr_set = 0;  // largest dynamic shared-memory size enabled so far
-    if (smem > 48 * 1024 && smem > attr_set) {
-        OEC_CUDA_TRY(cudaFuncSetAttribute(k_mg_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = smem;
+    if (smem > 48 * 1024) {
+        // the largest dynamic shared-memory size enabled so far, per device
+        static std::atomic<size_t> attr_set[kMaxDevices];
+        int dev = 0;
+        OEC_CUDA_TRY(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= kMaxDevices) return OEC_ERR_INVALID;
+        if (smem > attr_set[dev].load()) {
+            OEC_CUDA_TRY(cudaFuncSetAttribute(k_mg_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMgMaxBlockSmem));
+            attr_set[dev].store(kMgMaxBlockSmem);
+        }
     }
     k_mg_block<<<1, kBlockThreads, smem, s>>>(P, B == 0 ? r : lv[B].b, B == 0 ? z : lv[B].y);
     for (int k = B - 1; k >= 0; --k) {

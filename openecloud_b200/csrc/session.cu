@@ -25,6 +25,8 @@
 #include <mutex>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "oec_common.cuh"
 
 struct oec_ctx {
@@ -412,9 +414,17 @@ extern "C" int oec_run_steps(oec_run_t *r, int32_t n_steps, int32_t use_graph) {
     const int every = r->d.management_every;
     int k = 0;
     while (k < n_steps) {
-        if (r->steps_done > 0 && r->steps_done % every == 0) OEC_TRY(manage(r));
+        if (r->steps_done > 0 && r->steps_done % every == 0) {
+            nvtxRangePushA("oec_run management");
+            const int rc = manage(r);
+            nvtxRangePop();
+            OEC_TRY(rc);
+        }
         const int nxt = std::min<int64_t>(n_steps - k, every - r->steps_done % every);
-        OEC_TRY(replay(r, nxt, use_graph != 0));
+        nvtxRangePushA("oec_run steps");
+        const int rc = replay(r, nxt, use_graph != 0);
+        nvtxRangePop();
+        OEC_TRY(rc);
         k += nxt;
         r->steps_done += nxt;
     }

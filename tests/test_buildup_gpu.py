@@ -170,3 +170,60 @@ def test_checkpoint_resume_is_exact(gpu, tmp_path):
     from openecloud_b200.checkpoint import CheckpointError
     with pytest.raises(CheckpointError):
         wrong.load(str(tmp_path))
+
+
+def test_metrics_log_one_line_per_interval(gpu, tmp_path):
+    """Buildup(metrics_log=path) appends one JSON line per management
+    interval with the state at the start of the next step, consistent with
+    history()."""
+    import json
+    from openecloud_b200.buildup import Buildup
+    path = tmp_path / "metrics.jsonl"
+    b = Buildup(seed=9, n_steps_table=121, metrics_log=str(path))
+    b.run(120)
+    lines = [json.loads(x) for x in path.read_text().splitlines()]
+    assert [r["step"] for r in lines] == [50, 100, 120]
+    n, w = b.history()
+    for r in lines:
+        assert r["macro_particles"] == int(n[r["step"]]) and r["sum_weights"] == float(w[r["step"]])
+
+
+BOUNDS_CHILD = r"""
+import sys, ctypes, numpy as np
+sys.path.insert(0, {root!r})
+from openecloud_b200 import _lib
+assert _lib.LIB_PATH.endswith("liboec_checked.so")
+from openecloud_b200.buildup import Buildup
+b = Buildup(seed=12, n_steps_table=121)
+b.run(120)
+v = ctypes.c_int64(0)
+_lib.call("oec_bound_violations", ctypes.byref(v), 0)
+n, w = b.history()
+np.savez({out!r}, n=n, w=w, violations=v.value)
+"""
+
+
+def test_bounds_checked_build_reports_no_violation(gpu, tmp_path):
+    """The bounds-checked build (OEC_BOUNDS_CHECK=1 loads liboec_checked.so)
+    runs 120 buildup steps with no out-of-range index and the same history
+    as the normal build; the normal build reports -1 (not counting)."""
+    import ctypes
+    import os
+    import subprocess
+    import sys
+    from conftest import ROOT
+    from openecloud_b200 import _lib
+    from openecloud_b200.buildup import Buildup
+    code = BOUNDS_CHILD.format(root=ROOT, out=str(tmp_path / "b.npz"))
+    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600,
+                       env=dict(os.environ, OEC_BOUNDS_CHECK="1"))
+    assert p.returncode == 0, p.stderr[-3000:]
+    got = np.load(tmp_path / "b.npz")
+    assert int(got["violations"]) == 0
+    b = Buildup(seed=12, n_steps_table=121)
+    b.run(120)
+    n, w = b.history()
+    assert np.array_equal(got["n"], n) and np.array_equal(got["w"], w)
+    v = ctypes.c_int64(0)
+    _lib.call("oec_bound_violations", ctypes.byref(v), 0)
+    assert v.value == -1
