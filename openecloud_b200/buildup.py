@@ -223,10 +223,12 @@ class Buildup:
         self._check_rows()
         n = self.P.getMacroParticleCount()
         if step > 0 and step % self.management_every == 0 and (n > 1.05 * self.target or n < 0.95 * self.target):
+            # draws keyed by the run's seed, the step and the run's own count
+            # of management events: reproducible whatever else the process ran
             if self.management == "global":
-                globalRandom(self.grid, self.P, self.target, seed=self.seed + step)
+                globalRandom(self.grid, self.P, self.target, seed=self.seed + step, call=self.n_managed + 1)
             elif self.management == "local":
-                localRandom(self.grid, self.P, self.bd, self.target, seed=self.seed + step)
+                localRandom(self.grid, self.P, self.bd, self.target, seed=self.seed + step, call=self.n_managed + 1)
             else:
                 return False
             self._prepare_deposit()

@@ -35,8 +35,10 @@ def _mask_clear(P):
               D.stream())
 
 
-def globalRandom(gridObj, particlesObj, targetMacroParticleCount, seed=0):
-    """Reference: particleManagement.pyx:35-67."""
+def globalRandom(gridObj, particlesObj, targetMacroParticleCount, seed=0, call=None):
+    """Reference: particleManagement.pyx:35-67.  The draws are keyed by
+    (seed, call); `call` defaults to a process-wide counter (a run that must
+    be reproducible on its own passes its own count of management events)."""
     P = particlesObj
     P._bind(gridObj)
     n = P.getMacroParticleCount()
@@ -44,7 +46,7 @@ def globalRandom(gridObj, particlesObj, targetMacroParticleCount, seed=0):
     diff = n - target
     factor = float(n) / float(target)
     s = D.stream()
-    call = _next_call()
+    call = _next_call() if call is None else int(call)
     if diff > 0:
         _lib.call("oec_scale_weights", P.c_particles(), factor, s)
         fails = D.zeros(1, torch.int32)
@@ -62,8 +64,10 @@ def globalRandom(gridObj, particlesObj, targetMacroParticleCount, seed=0):
 
 
 def localRandom(gridObj, particlesObj, particleBoundaryObj, targetMacroParticleCount, phaseSpaceWeights=None,
-                thresholdFactor=2., lambdavFactor=1., factorDisLimit=1., mergeScheme=0, seed=0, oversample=4):
-    """Reference: particleManagement.pyx:74-238 (see the module docstring)."""
+                thresholdFactor=2., lambdavFactor=1., factorDisLimit=1., mergeScheme=0, seed=0, oversample=4,
+                call=None):
+    """Reference: particleManagement.pyx:74-238 (see the module docstring);
+    `call` as in globalRandom."""
     P = particlesObj
     P._bind(gridObj)
     n = P.getMacroParticleCount()
@@ -109,7 +113,7 @@ def localRandom(gridObj, particlesObj, particleBoundaryObj, targetMacroParticleC
         work = D.empty(int(_lib.lib().oec_sort_work_bytes(P._cap)), torch.uint8)
         counters = D.zeros(2, torch.int32)
         _lib.call("oec_cell_merge", gridObj.c_grid(), P.c_particles(), n_cand, to_merge, lam, factorDisLimit * ds,
-                  int(mergeScheme), int(seed), _next_call(), 3.0 * vt, P._mask.data_ptr(), counters.data_ptr(),
+                  int(mergeScheme), int(seed), _next_call() if call is None else int(call), 3.0 * vt, P._mask.data_ptr(), counters.data_ptr(),
                   work.data_ptr(), s)
         localRandom.last_counters = counters.cpu().numpy()
     P.addAndRemoveParticles(rows[:to_split], None)

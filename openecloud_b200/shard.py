@@ -110,9 +110,9 @@ class ShardedBuildup(Buildup):
         do = step > 0 and step % self.management_every == 0 and \
             (n > 1.05 * self.target or n < 0.95 * self.target) and self.management in ("global", "local")
         if do and self.management == "global":
-            globalRandom(self.grid, self.P, self.target, seed=self.seed + step)
+            globalRandom(self.grid, self.P, self.target, seed=self.seed + step, call=self.n_managed + 1)
         elif do:
-            localRandom(self.grid, self.P, self.bd, self.target, seed=self.seed + step)
+            localRandom(self.grid, self.P, self.bd, self.target, seed=self.seed + step, call=self.n_managed + 1)
         flag = torch.tensor([1 if do else 0], dtype=torch.int32, device=D.device())
         dist.all_reduce(flag, op=dist.ReduceOp.MAX, group=self.group)
         if int(flag.item()):

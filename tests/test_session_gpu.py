@@ -6,9 +6,13 @@ A child process sets the c1 run up with numpy and scipy only
 graph, the LU solve and globalRandom owned by the library) and checks that
 torch was never loaded; this process runs the same configuration through the
 reference-API driver (Buildup) from the same initial rows.  The two launch
-the same kernels in the same order, so the histories and the particles agree
-bit for bit until the first management event (the roulette keys differ
-between the two drivers), and the counts after it."""
+the same kernels in the same order with the same keys (emission: run seed,
+particle slot, step; roulette: run seed + step, the run's count of
+management events); they differ only in how the dense inverses of the LU
+tail blocks are rounded (host LAPACK here, the device there), so the
+histories agree exactly before the first management event and the particle
+state to FP32 rounding; afterwards the counts and weights stay within a
+fraction of a percent."""
 import os
 import subprocess
 import sys
@@ -63,12 +67,17 @@ def test_run_handle_without_torch_matches_buildup(gpu, tmp_path):
     b.P.setParticleData(rows)
     b._prepare_deposit()
     b.run(40)
-    assert np.array_equal(got["rows40"], b.P.getParticleData())
+    mine = b.P.getParticleData()
+    rows40 = got["rows40"]
+    assert rows40.shape == mine.shape
+    scale = np.max(np.abs(mine), axis=0)
+    assert np.all(np.max(np.abs(rows40 - mine), axis=0) <= 1e-6 * scale)
     b.run(110)
     n, w = b.history()
-    assert np.array_equal(got["counts"][1:41], n[1:41]) and np.array_equal(got["weights"][1:41], w[1:41])
-    # the first roulette (step 50) brings both to the target exactly
-    assert got["counts"][51] == n[51] == 100000
+    assert np.array_equal(got["counts"][:41], n[:41])
+    assert np.max(np.abs(got["weights"][:41] / w[:41] - 1)) <= 1e-12
+    # the first roulette (step 50) clones up to the target of 1e5
+    assert abs(got["counts"][51] / 1e5 - 1) < 0.01 and abs(n[51] / 1e5 - 1) < 0.01
+    assert np.max(np.abs(got["counts"][51:].astype(float) / n[51:] - 1)) < 0.005
+    assert np.max(np.abs(got["weights"][51:] / w[51:] - 1)) < 0.005
     assert int(got["dropped"]) == 0
-    # the weight history after the management stays within a few percent
-    assert abs(got["weights"][-1] / w[-1] - 1) < 0.05

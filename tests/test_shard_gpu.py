@@ -80,6 +80,7 @@ def _two_rank_worker(rank, world, port, q):
     _init_pg("gloo", rank, world, port)
     try:
         b = ShardedBuildup(rank, world, seed=40, n_init=20000, n_steps_table=81)
+        wscale0 = float(D.to_numpy(b.P._wscale)[0])
         n0 = b.P.getMacroParticleCount()
         soa = {k: D.to_numpy(v[:n0]) for k, v in b.P.soa().items()}
         rho0 = b.P._rho_fix.clone()
@@ -93,7 +94,7 @@ def _two_rank_worker(rank, world, port, q):
         dist.all_gather_object(phis, phi)
         hist = b.history()
         if rank == 0:
-            q.put(dict(parts=parts, rho0=D.to_numpy(rho0), wscale=float(D.to_numpy(b.P._wscale)[0]),
+            q.put(dict(parts=parts, rho0=D.to_numpy(rho0), wscale=wscale0,
                        nx=b.grid.getNxExt(), G=b.grid.getNpExt(), phis=phis, hist_n=hist[0], n0=n0))
     finally:
         dist.destroy_process_group()
