@@ -27,7 +27,7 @@ import torch
 
 from . import device as D
 
-MG_BLOCK_TOPS = (320, 1280, 4608)
+MG_BLOCK_TOPS = (320, 1280, 4608, 9000)
 
 
 def _time(fn, reps):

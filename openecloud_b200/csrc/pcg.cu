@@ -360,6 +360,7 @@ constexpr int kTX = 32, kTY = 16;       // fine tile
 constexpr int kBlockThreads = 1024;
 constexpr int kMgMaxBlockLevels = 8;
 constexpr int kMgFloatsPerNode = 7;     // ex, ey, leak, dinv, b, x, y
+constexpr int kMgFloatsPerNodeLean = 3; // b, x, y (the operator read from global memory)
 constexpr int kMgMaxCoarse = 1024;
 constexpr size_t kMgMaxBlockSmem = 226 * 1024;  // dynamic, beside the level table
 
@@ -538,8 +539,11 @@ __device__ __forceinline__ void sm_sweep(const SmLevel &L, float om, const float
     }
 }
 
+// coef_smem: the levels' operator is copied to shared memory (7 floats per
+// node); otherwise it is read from its global arrays (3 floats per node in
+// shared memory: b, x, y), which lets larger levels into this kernel.
 __global__ void __launch_bounds__(kBlockThreads) k_mg_block(MgBlock P, const float *__restrict__ b_in,
-                                                            float *__restrict__ y_out) {
+                                                            float *__restrict__ y_out, int coef_smem) {
     extern __shared__ float sm[];
     __shared__ SmLevel Ls[kMgMaxBlockLevels];
     if (threadIdx.x == 0) {
@@ -549,7 +553,19 @@ __global__ void __launch_bounds__(kBlockThreads) k_mg_block(MgBlock P, const flo
             L.nx = P.nx[l];
             L.ny = P.ny[l];
             L.n = L.nx * L.ny;
-            float **a[] = {&L.ex, &L.ey, &L.lk, &L.dv, &L.b, &L.x, &L.y};
+            if (coef_smem) {
+                float **a[] = {&L.ex, &L.ey, &L.lk, &L.dv};
+                for (float **q : a) {
+                    *q = p;
+                    p += L.n;
+                }
+            } else {
+                L.ex = const_cast<float *>(P.ex[l]);
+                L.ey = const_cast<float *>(P.ey[l]);
+                L.lk = const_cast<float *>(P.leak[l]);
+                L.dv = const_cast<float *>(P.dinv[l]);
+            }
+            float **a[] = {&L.b, &L.x, &L.y};
             for (float **q : a) {
                 *q = p;
                 p += L.n;
@@ -560,10 +576,12 @@ __global__ void __launch_bounds__(kBlockThreads) k_mg_block(MgBlock P, const flo
     for (int l = 0; l < P.nb; ++l) {
         const SmLevel &L = Ls[l];
         for (int i = threadIdx.x; i < L.n; i += kBlockThreads) {
-            L.ex[i] = P.ex[l][i];
-            L.ey[i] = P.ey[l][i];
-            L.lk[i] = P.leak[l][i];
-            L.dv[i] = P.dinv[l][i];
+            if (coef_smem) {
+                L.ex[i] = P.ex[l][i];
+                L.ey[i] = P.ey[l][i];
+                L.lk[i] = P.leak[l][i];
+                L.dv[i] = P.dinv[l][i];
+            }
             L.b[i] = l == 0 ? b_in[i] : 0.f;
             L.x[i] = 0.f;
             L.y[i] = 0.f;
@@ -646,10 +664,21 @@ int mg_shift(const oec_mg_level_t &l, const oec_mg_level_t &c) {
 
 MgT mg_t(const oec_mg_level_t &l, bool with_leak) { return MgT{l.nx, l.ny, l.ex, l.ey, with_leak ? l.leak : nullptr, l.dinv}; }
 
-size_t mg_block_smem(const oec_mg_t *mg) {
+size_t mg_block_nodes(const oec_mg_t *mg) {
     size_t n = 0;
     for (int k = mg->block_level; k < mg->nlevels; ++k) n += (size_t)mg->levels[k].nx * mg->levels[k].ny;
-    return n * kMgFloatsPerNode * sizeof(float);
+    return n;
+}
+
+// Whether the one-CTA levels keep their operator (edge weights, leak,
+// inverse diagonal) in shared memory too, or read it from global memory
+// (L1/L2) so that larger levels fit.
+bool mg_block_coef_smem(const oec_mg_t *mg) {
+    return mg_block_nodes(mg) * kMgFloatsPerNode * sizeof(float) <= kMgMaxBlockSmem;
+}
+
+size_t mg_block_smem(const oec_mg_t *mg) {
+    return mg_block_nodes(mg) * (mg_block_coef_smem(mg) ? kMgFloatsPerNode : kMgFloatsPerNodeLean) * sizeof(float);
 }
 
 bool valid_mg(const oec_mg_t *mg) {
@@ -721,7 +750,8 @@ int mg_cycle(const oec_mg_t *mg, const float *r, float *z, const float *q, Acc *
             attr_set[dev].store(kMgMaxBlockSmem);
         }
     }
-    k_mg_block<<<1, kBlockThreads, smem, s>>>(P, B == 0 ? r : lv[B].b, B == 0 ? z : lv[B].y);
+    k_mg_block<<<1, kBlockThreads, smem, s>>>(P, B == 0 ? r : lv[B].b, B == 0 ? z : lv[B].y,
+                                              mg_block_coef_smem(mg) ? 1 : 0);
     for (int k = B - 1; k >= 0; --k) {
         const oec_mg_level_t &l = lv[k], &c = lv[k + 1];
         const dim3 grid((l.nx + kTX - 1) / kTX, (l.ny + kTY - 1) / kTY);

@@ -62,7 +62,7 @@ class Mg_t(ctypes.Structure):
 
 
 MG_BLOCK_SMEM = 226 * 1024   # dynamic shared memory of the one-CTA coarse solve
-MG_FLOATS_PER_NODE = 7
+MG_FLOATS_PER_NODE = 3       # b, x, y in shared memory (the operator moves there too when all 7 fit)
 MG_BLOCK_TOP = 1280          # largest level given to the one-CTA solve (one SM's issue rate bounds it)
 
 

@@ -119,9 +119,9 @@ def test_mg_coarse_level_is_directional_galerkin_product(args):
 def test_mg_hierarchy_layout():
     """Level sizes halve (rounded up) down to at most 100 nodes; the block
     level is the first of at most MG_BLOCK_TOP nodes from which the coarser
-    levels fit the one-CTA shared-memory solve (7 floats per node, 226 KB),
-    at most 8 levels."""
-    from openecloud_b200.poissonSolver import mg_hierarchy, MG_BLOCK_SMEM, MG_BLOCK_TOP
+    levels fit the one-CTA shared-memory solve (3 floats per node at least,
+    226 KB), at most 8 levels."""
+    from openecloud_b200.poissonSolver import mg_hierarchy, MG_BLOCK_SMEM, MG_BLOCK_TOP, MG_FLOATS_PER_NODE
     for nx, ny in ((1026, 1026), (130, 130), (66, 66), (26, 22), (515, 130)):
         yy, xx = np.mgrid[0:ny, 0:nx]
         inside = ((xx - nx / 2) / (nx / 2 - 1.5)) ** 2 + ((yy - ny / 2) / (ny / 2 - 1.5)) ** 2 < 1
@@ -130,7 +130,7 @@ def test_mg_hierarchy_layout():
         for (a, b), (c, d) in zip(sizes, sizes[1:]):  # isotropic weights: both directions halve
             assert (c, d) == ((a + 1) // 2, (b + 1) // 2)
         assert sizes[-1][0] * sizes[-1][1] <= 100 and (len(sizes) == 1 or sizes[-2][0] * sizes[-2][1] > 100)
-        smem = lambda k: 28 * sum(a * b for a, b in sizes[k:])  # noqa: E731
+        smem = lambda k: 4 * MG_FLOATS_PER_NODE * sum(a * b for a, b in sizes[k:])  # noqa: E731
         top = lambda k: sizes[k][0] * sizes[k][1]  # noqa: E731
         assert smem(block) <= MG_BLOCK_SMEM and len(sizes) - block <= 8 and top(block) <= max(MG_BLOCK_TOP, 100)
         assert block == 0 or smem(block - 1) > MG_BLOCK_SMEM or len(sizes) - block + 1 > 8 or \
@@ -345,3 +345,33 @@ def test_pcg_synchronous_entry_point(gpu):
     assert st.converged == 1 and a.converged == 1 and st.rel_residual <= 1e-8
     assert abs(st.iterations - a.iterations) <= 2 and st.refinements == a.refinements
     assert np.abs(D.to_numpy(phi) - phi_async).max() <= 1e-7 * np.abs(phi_async).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("top", [1280, 9000])
+def test_mg_vcycle_large_block_matches_tiled(gpu, top):
+    """On the 512x512 ellipse (45 x 18 mm), a V-cycle whose one-CTA part
+    starts at a larger level (129 x 65 nodes and coarser: the operator read
+    from global memory, 3 floats per node in shared memory) equals the
+    float64 restatement, as the default split does."""
+    import ctypes
+    import torch
+    from openecloud_b200 import device as D
+    from openecloud_b200.grid import Grid
+    from openecloud_b200.poissonSolver import PoissonSolver, _declare
+    from oracle.mg_oracle import vcycle
+    ps = PoissonSolver(Grid(512, 512, 0.09, 0.036, 1), method="pcg", precond="mg")
+    mg = ps._mg_setup(block_top=top)
+    host = mg["host"]
+    sizes = [h[4] * h[5] for h in host]
+    block = mg["c"].block_level
+    assert sizes[block] <= top and (top < 9000 or sizes[block] > 4608)
+    dinv = [D.to_numpy(k["dinv"]).astype(np.float64) for k in mg["keep"]]
+    ins = host[0][3]
+    r = np.where(ins, np.random.default_rng(6).normal(size=ins.size), 0.0).astype(np.float32)
+    rd = D.to_device(r, torch.float32)
+    zd = D.zeros(r.size, torch.float32)
+    assert _declare().oec_mg_apply(ctypes.byref(mg["c"]), rd.data_ptr(), zd.data_ptr(), D.stream()) == 0
+    got = D.to_numpy(zd).astype(np.float64)
+    want = vcycle(host, r.astype(np.float64), omega=mg["c"].omega, scale=mg["c"].scale, dinv=dinv)
+    assert np.max(np.abs(got - want)) <= 2e-4 * np.max(np.abs(want))
