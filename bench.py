@@ -454,7 +454,8 @@ def production_passage(steps=100, warm=10):
     from openecloud_b200.buildup import Buildup
     kw = dict(nx=1024, ny=1024, lx=0.09, ly=0.036, boundType=1, n_init=2_200_000, w_init=1e3, dt=5e-12,
               beam_particles=1.15e11, radius_sigma=1e-3, sey_max=1.8, type_b_field=1, b_const=(0., 8.33, 0.),
-              target=2_000_000, management="local", management_every=10, n_steps_table=steps + warm + 25, seed=2000)
+              target=2_000_000, management="local", management_every=10, n_steps_table=steps + warm + 25, seed=2000,
+              abs_cap=4_400_000)
     t0 = time.perf_counter()
     lu = Buildup(**kw)
     setup = time.perf_counter() - t0

@@ -155,13 +155,14 @@ int oec_boris_push(const oec_grid_t *grid, oec_particles_t *p, const double *e_a
 /* Fixed-point deposit scale: charge of a particle of weight w is stored as
  * llrint(w * wscale) integer units, wscale = 2^(bits - ceil(log2(wmax))).
  * Computes wscale on the device from the particles' max |w|; bits =
- * min(50, 62 - ceil(log2(capacity))), so capacity * 2^bits <= 2^62 and no
- * node can leave the int64 range whatever the particle distribution. */
+ * min(50, 63 - ceil(log2(capacity))): every particle's charge stays below
+ * 2^bits units, so capacity * 2^bits <= 2^63 and no node can leave the int64
+ * range whatever the particle distribution. */
 int oec_deposit_scale(const oec_particles_t *p, double *wscale_dev, void *stream);
 
 /* The same scale for one shard of a particle store split over several
  * stores (one per GPU) whose int64 deposits are summed afterwards: bits =
- * min(50, 62 - ceil(log2(total_capacity))) with total_capacity the sum of
+ * min(50, 63 - ceil(log2(total_capacity))) with total_capacity the sum of
  * the shards' capacities (>= p->capacity), so the summed grid stays inside
  * int64.  The shards then take the smallest of their scales (the largest
  * weight), which keeps every shard's charges exact.  Replaces the charge

@@ -989,12 +989,14 @@ extern "C" int oec_boris_push(const oec_grid_t *grid, oec_particles_t *p, const 
 }
 
 static int deposit_bits(int64_t capacity) {
-    // A node sums at most `capacity` particles of at most 2^bits units:
-    // capacity * 2^bits <= 2^62 keeps every node inside int64.  At most 50
-    // bits so that the f64 corner products stay exact to well below a unit.
+    // A node sums at most `capacity` particles, each below 2^bits units (w
+    // is an FP32 below 2^e, so w * 2^(bits - e) stays at least 2^(bits - 24)
+    // below 2^bits and its rounding cannot reach 2^bits): with capacity <=
+    // 2^(63 - bits) every node stays strictly inside int64.  At most 50 bits
+    // so that the f64 corner products stay exact to well below a unit.
     int lc = 0;
     while ((int64_t(1) << lc) < capacity) ++lc;
-    int bits = 62 - lc;
+    int bits = 63 - lc;
     return bits > 50 ? 50 : bits;
 }
 

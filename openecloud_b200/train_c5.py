@@ -39,7 +39,9 @@ def production_kwargs(seed=2000, steps=5001, **over):
     """The production buildup of the benchmark (sampled passages)."""
     kw = dict(nx=1024, ny=1024, lx=0.09, ly=0.036, boundType=1, n_init=2_200_000, w_init=1e3, dt=5e-12,
               beam_particles=1.15e11, radius_sigma=1e-3, sey_max=1.8, type_b_field=1, b_const=(0., 8.33, 0.),
-              target=2_000_000, management="local", management_every=10, n_steps_table=steps, seed=seed)
+              target=2_000_000, management="local", management_every=10, n_steps_table=steps, seed=seed,
+              abs_cap=4_400_000)  # the electrons released at rest cross the chamber together: bursts of > 1e6
+                                  # absorbed in one step (half the store's capacity of rows)
     kw.update(over)
     return kw
 

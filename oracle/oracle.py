@@ -375,12 +375,13 @@ def local_random(pd, target, g, kind=1, seed=None, threshold=2., lambda_factor=1
 
 # ------------------------------------------------- fixed-point deposit
 def deposit_bits(total_capacity):
-    """Fixed-point bits of a particle's charge: capacity * 2^bits <= 2^62
-    keeps any node inside int64; at most 50."""
+    """Fixed-point bits of a particle's charge: each particle's charge stays
+    below 2^bits units, so capacity * 2^bits <= 2^63 keeps any node inside
+    int64; at most 50."""
     lc = 0
     while (1 << lc) < total_capacity:
         lc += 1
-    return min(50, 62 - lc)
+    return min(50, 63 - lc)
 
 
 def deposit_scale(w, total_capacity):
