@@ -118,15 +118,16 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
 
 // Shared-memory layout of the convolution (bytes from the dynamic base,
 // which is 1024-byte aligned by the kernel): weights [9][CI/8][CO] rows of
-// 16 bytes, the halo [3][CI/8][kHalo] rows, the mbarrier and the tensor
-// memory address.
+// 16 bytes, two halo buffers [3][CI/8][kHalo] rows (tile k stages into one
+// while the tensor cores read the other), the two mbarriers and the tensor
+// memory address.  Tensor memory holds two accumulators of CO columns.
 template <int CI, int CO>
 struct ConvSmem {
     static constexpr int kW = 9 * (CI / 8) * CO * 16;
     static constexpr int kA = 3 * (CI / 8) * kHalo * 16;
-    static constexpr int kBar = kW + kA;
-    static constexpr int kBytes = kBar + 16 + 1024;  // + barrier, tmem address, alignment slack
-    static constexpr int kCols = CO <= 32 ? 32 : 64;  // tensor-memory columns (a power of two >= 32)
+    static constexpr int kBar = kW + 2 * kA;
+    static constexpr int kBytes = kBar + 32 + 1024;  // + barriers, tmem address, alignment slack
+    static constexpr int kCols = 2 * CO <= 32 ? 32 : (2 * CO <= 64 ? 64 : 128);
 };
 
 __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
@@ -135,7 +136,10 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
 }
 
 // out[y][x][co] = sum_{ty,tx,ci} in[y+ty-1][x+tx-1][ci] * w[co][(ty*3+tx)*CI + ci]
-// (zero outside the image), bf16 in and out, f32 accumulation.
+// (zero outside the image), bf16 in and out, f32 accumulation.  Each CTA
+// walks its tiles (blockIdx.x, + gridDim.x, ...) as a two-stage pipeline:
+// it stages tile k's halo and issues its MMAs into accumulator k % 2, then
+// writes tile k-1 out of the other accumulator while the tensor cores work.
 template <int CI, int CO>
 __global__ void __launch_bounds__(kThreads, 1)
     k_conv3(int H, int W, const __nv_bfloat16 *__restrict__ in, const __nv_bfloat16 *__restrict__ wgt,
@@ -147,8 +151,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                                                             ~uintptr_t(1023));
     unsigned char *sW = base;
     unsigned char *sA = base + L::kW;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(base + L::kBar);
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(base + L::kBar + 8);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(base + L::kBar);  // bar[0], bar[1]
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(base + L::kBar + 16);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     constexpr int C8 = CI / 8;
 
@@ -158,7 +162,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         *reinterpret_cast<uint4 *>(sW + (size_t)i * 16) =
             *reinterpret_cast<const uint4 *>(wgt + (size_t)co * 9 * CI + tap * CI + c8 * 8);
     }
-    if (tid == 0) mbar_init(bar, 1);
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        mbar_init(bar + 1, 1);
+    }
     if (warp == 0) tmem_alloc(tslot, L::kCols);
     fence_async_smem();
     fence_before_sync();
@@ -169,69 +176,99 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t sW0 = smem_u32(sW), sA0 = smem_u32(sA);
     const int tiles_x = (W + kM - 1) / kM;
     const int ntiles = H * tiles_x;
-    uint32_t phase = 0;
+    const int mine = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    uint32_t phase0 = 0u, phase1 = 0u;  // parity of the next completion of bar[0], bar[1]
     bool ok = true;
-    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+
+    // halo rows y-1..y+1, pixels x0-1..x0+kM of tile `tile` into buffer b: row (r, c8, px)
+    auto stage = [&](int tile, int b) {
         const int y = tile / tiles_x, x0 = (tile % tiles_x) * kM;
-        // halo rows y-1..y+1, pixels x0-1..x0+kM: row (r, c8, px)
+        unsigned char *dst = sA + b * L::kA;
         for (int i = tid; i < 3 * C8 * kHalo; i += kThreads) {
             const int px = i % kHalo, c8 = (i / kHalo) % C8, r = i / (kHalo * C8);
             const int yy = y + r - 1, xx = x0 + px - 1;
             uint4 v = make_uint4(0u, 0u, 0u, 0u);
             if (yy >= 0 && yy < H && xx >= 0 && xx < W)
                 v = *reinterpret_cast<const uint4 *>(in + ((size_t)yy * W + xx) * CI + c8 * 8);
-            *reinterpret_cast<uint4 *>(sA + (size_t)i * 16) = v;
+            *reinterpret_cast<uint4 *>(dst + (size_t)i * 16) = v;
         }
-        fence_async_smem();
-        __syncthreads();
-        fence_after_sync();
+    };
+    // MMAs of the tile staged in buffer b into accumulator b, committed to bar[b]
+    auto issue = [&](int b) {
         if (tid == 0) {
+            const uint32_t a0 = sA0 + (uint32_t)(b * L::kA);
+            const uint32_t d = tmem + (uint32_t)(b * CO);
 #pragma unroll 1
             for (int tap = 0; tap < 9; ++tap) {
                 const int ty = tap / 3, tx = tap % 3;
 #pragma unroll
                 for (int kc = 0; kc < CI / 16; ++kc) {
-                    const uint32_t a = sA0 + (uint32_t)(((ty * C8 + 2 * kc) * kHalo + tx) * 16);
-                    const uint32_t b = sW0 + (uint32_t)((tap * C8 + 2 * kc) * CO * 16);
-                    mma_bf16(tmem, smem_desc(a, kHalo * 16, 128), smem_desc(b, CO * 16, 128), idesc,
-                             (tap | kc) != 0);
+                    const uint32_t a = a0 + (uint32_t)(((ty * C8 + 2 * kc) * kHalo + tx) * 16);
+                    const uint32_t bw = sW0 + (uint32_t)((tap * C8 + 2 * kc) * CO * 16);
+                    mma_bf16(d, smem_desc(a, kHalo * 16, 128), smem_desc(bw, CO * 16, 128), idesc, (tap | kc) != 0);
                 }
             }
-            commit(bar);
+            commit(bar + b);
         }
         __syncwarp();
-        if (mbar_wait(bar, phase)) {
-            phase ^= 1;
+    };
+    // waits for accumulator b and writes the tile out
+    auto epilogue = [&](int tile, int b) {
+        if (mbar_wait(bar + b, b ? phase1 : phase0)) {
+            if (b) phase1 ^= 1u;
+            else phase0 ^= 1u;
         } else {
             atomicExch(err, 1);
             ok = false;
+            return;
         }
         fence_after_sync();
-        if (ok) {
-            const int x = x0 + warp * 32 + lane;
+        const int y = tile / tiles_x, x = (tile % tiles_x) * kM + warp * 32 + lane;
 #pragma unroll
-            for (int c0 = 0; c0 < CO; c0 += 16) {
-                float v[16];
-                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-                if (x < W) {
-                    uint4 *dst = reinterpret_cast<uint4 *>(out + ((size_t)y * W + x) * CO + c0);
-                    dst[0] = make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
-                    dst[1] = make_uint4(pack2(v[8], v[9]), pack2(v[10], v[11]), pack2(v[12], v[13]),
-                                        pack2(v[14], v[15]));
-                }
+        for (int c0 = 0; c0 < CO; c0 += 16) {
+            float v[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(b * CO + c0), v);
+            if (x < W) {
+                uint4 *dst = reinterpret_cast<uint4 *>(out + ((size_t)y * W + x) * CO + c0);
+                dst[0] = make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
+                dst[1] = make_uint4(pack2(v[8], v[9]), pack2(v[10], v[11]), pack2(v[12], v[13]),
+                                    pack2(v[14], v[15]));
             }
         }
-        fence_before_sync();
-        // every warp has read the accumulators and every thread is done
-        // with the halo: the next tile may overwrite both
-        ok = __syncthreads_and(ok);
+    };
+
+    if (mine > 0) {
+        stage(blockIdx.x, 0);
+        fence_async_smem();
+        __syncthreads();
+        fence_after_sync();
+        issue(0);
     }
+    for (int k = 1; k < mine; ++k) {  // the same trip count in every thread
+        const int b = k & 1;
+        // buffer and accumulator b last served tile k-2, whose MMAs this
+        // thread saw complete and whose accumulator every warp has read
+        stage(blockIdx.x + k * gridDim.x, b);
+        fence_async_smem();
+        fence_before_sync();
+        ok = __syncthreads_and(ok);
+        fence_after_sync();
+        if (!ok) break;
+        issue(b);
+        epilogue(blockIdx.x + (k - 1) * gridDim.x, b ^ 1);
+        fence_before_sync();
+    }
+    if (mine > 0 && ok) epilogue(blockIdx.x + (mine - 1) * gridDim.x, (mine - 1) & 1);
+    fence_before_sync();
+    ok = __syncthreads_and(ok);
     if (!ok) {
-        // the committed MMAs of the last tile get a bounded time to end
-        // before their tensor memory is freed
-        mbar_wait(bar, phase);
+        // committed MMAs get a bounded time to end before their tensor
+        // memory is freed
+        mbar_wait(bar, phase0);
+        mbar_wait(bar + 1, phase1);
     }
     __syncthreads();
+    fence_after_sync();
     if (warp == 0) tmem_free(tmem, L::kCols);
 }
 
