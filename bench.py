@@ -49,7 +49,7 @@ METRIC = "particle-steps/s"
 # (ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none -k regex:k_push_gather -s 3 -c 1):
 # the particle part scaled by 2 to 2^24 electrons, the grid part (E table and
 # deposit grid, 12.7 MB) added once.
-NCU_TRAFFIC_PER_LAUNCH = {1 << 24: 771791520}
+NCU_TRAFFIC_PER_LAUNCH = {1 << 24: 768996672}
 
 
 # ------------------------------------------------------------- workload
@@ -880,7 +880,7 @@ def run_ours(args, rank, world, local_rank):
             _log(f"{c['kernel']}: {c['ms']:.3f} ms, {c['achieved_gbs']:.0f} GB/s ({c['frac']:.2f} of peak)")
     batch = None
     if rank == 0 and world == 1 and not args.no_batch:
-        batch = batched_scan()
+        batch = batched_scan(steps=args.scan_steps)
         _log(f"batched scan: {batch['runs']} runs, {batch['ms_per_batch_step']:.1f} ms per batch step at width "
              f"{batch['branch_width']} ({batch['run_steps_per_s']:.0f} run-steps/s), setup {batch['setup_s']:.0f} s")
 
@@ -935,6 +935,8 @@ def main():
     ap.add_argument("--no-production", action="store_true",
                     help="skip the 1024x1024 production passage sample and solve comparison")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-run batched scan")
+    ap.add_argument("--scan-steps", type=int, default=100,
+                    help="batch steps of the scan before its 50 steady ones (2450: a whole 2500-step passage)")
     ap.add_argument("--no-components", action="store_true",
                     help="skip the achieved bandwidth of the deposit, boundary, emission and merge kernels")
     args = ap.parse_args()
