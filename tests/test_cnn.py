@@ -151,3 +151,47 @@ def test_training_and_warm_start(gpu):
     print(f"Jacobi-PCG to 1e-8 (iterations, rel. error of the start vs LU): zero start {zero}, "
           f"untrained-network start {untrained}, trained-network start {trained}")
     assert trained[1] < 0.7 * zero[1] and trained[1] < 0.7 * untrained[1]
+
+
+@pytest.mark.gpu
+def test_learned_correction_on_the_production_chamber(gpu):
+    """The network trained on 2e4 pairs of a production run
+    (openecloud_b200/train_c5.py, weights in openecloud_b200/weights) as the
+    correction of the extrapolated warm start, on another production run
+    (1024x1024 ellipse 45 x 18 mm, 2.2e6 electrons, 8.33 T, merging every 10
+    steps; seed 2000): over 40 steps after 20 warm-up ones, the multigrid-PCG
+    solve at 1e-8 starts from a smaller residual and needs fewer iterations
+    than from the extrapolation alone, with no LU fallback.  This is what the
+    trained network gains over the method without it; per step it costs one
+    forward pass (0.4 ms at 1026^2), more than the iterations it saves (the
+    passage times are in the benchmark)."""
+    import os
+    from openecloud_b200.buildup import Buildup
+    from openecloud_b200.cnn import PoissonCNN
+    from openecloud_b200.train_c5 import WEIGHTS, production_kwargs
+    assert os.path.exists(WEIGHTS)
+    w = np.load(WEIGHTS).astype(np.float64)
+    kw = production_kwargs(seed=2000, steps=70)
+    stats = {}
+    ps = None
+    for ws in ("extrapolate", "extrapolate+cnn"):
+        b = Buildup(poisson=ps, **kw)
+        ps = b.ps
+        ps.resetHistory()
+        ps.method, ps.precond, ps.warmStart = "pcg", "mg", ws
+        ps.cnn = PoissonCNN.for_solver(ps, weights=w, training=False) if ws != "extrapolate" else None
+        fb0 = ps.nFallbacks
+        b.run(20)
+        r0, it = [], []
+        for _ in range(40):
+            b.run(1)
+            st = ps.lastStats
+            assert st.converged == 1 and st.rel_residual <= 1e-8
+            r0.append(st.rel_residual0)
+            it.append(st.iterations)
+        assert ps.nFallbacks == fb0
+        stats[ws] = (float(np.mean(r0)), float(np.mean(it)))
+    print(f"production chamber, MG-PCG to 1e-8 (mean initial residual, iterations): extrapolation "
+          f"{stats['extrapolate']}, with the learned correction {stats['extrapolate+cnn']}")
+    assert stats["extrapolate+cnn"][0] < stats["extrapolate"][0]
+    assert stats["extrapolate+cnn"][1] <= stats["extrapolate"][1]
