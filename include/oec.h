@@ -528,6 +528,12 @@ typedef struct oec_mg {
     const float *coarse_inv;         /* [ncoarse*ncoarse] row-major inverse of its operator */
     float omega;                     /* damped-Jacobi weight */
     float scale;                     /* coarse-correction scale */
+    int32_t cluster_top;             /* > 0: the levels from the first one of at most cluster_top nodes
+                                        (no lower than block_level) to the bottom are solved by one
+                                        thread-block cluster of 8 or 16 CTAs (their bands of b, x, y in
+                                        distributed shared memory) instead of the one-CTA kernel;
+                                        0: one CTA.  The one-CTA path is also taken when the cluster
+                                        levels do not fit 226 KB of shared memory per CTA. */
 } oec_mg_t;
 
 /* z = M r, one V-cycle (r, z f32 [nx*ny] of level 0; z is 0 outside).
@@ -598,7 +604,13 @@ typedef struct oec_cnn {
     const uint8_t *inside;  /* [nx*ny] */
     void *w16;              /* bf16 parameters, oec_cnn_num_params() of them */
     void *act;              /* workspace of oec_cnn_act_bytes(nx, ny, training) bytes */
+    int32_t conv_kernel;    /* 3x3 convolutions with 16..64 input channels: OEC_CNN_CONV_MMA_SYNC
+                               (warp-level mma.sync m16n8k16) or OEC_CNN_CONV_TCGEN05 (tcgen05.mma
+                               issued by one thread, f32 accumulators in tensor memory) */
 } oec_cnn_t;
+
+#define OEC_CNN_CONV_MMA_SYNC 0
+#define OEC_CNN_CONV_TCGEN05 1
 
 int32_t oec_cnn_num_params(void);
 /* offsets[9]: start of each layer's weights in the flat parameter vector
@@ -609,6 +621,10 @@ int oec_cnn_param_layout(int32_t *offsets, int32_t *shapes);
 int64_t oec_cnn_act_bytes(int32_t nx, int32_t ny, int32_t training);
 /* z = N(x) (f32 [nx*ny] in and out, device). */
 int oec_cnn_forward(const oec_cnn_t *c, const float *x_dev, float *z_dev, void *stream);
+/* Bounded tensor-memory waits of the tcgen05 convolutions that gave up since
+ * the last forward pass or training step began (0 on a healthy device; the
+ * results of that pass are then invalid).  Synchronises the stream. */
+int oec_cnn_status(const oec_cnn_t *c, int32_t *wait_timeouts_host, void *stream);
 /* Warm start of the iterative solve: phi0 = |b| N(b / |b|) with
  * b = scale32 * q on the inside nodes (the network approximates the inverse
  * of the scaled operator); phi0 = 0 outside.  work_dev:

@@ -24,12 +24,17 @@ from . import device as D
 
 class Cnn_t(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("inside", ctypes.c_void_p),
-                ("w16", ctypes.c_void_p), ("act", ctypes.c_void_p)]
+                ("w16", ctypes.c_void_p), ("act", ctypes.c_void_p), ("conv_kernel", ctypes.c_int32)]
+
+
+CONV_KERNELS = {"mma.sync": 0, "tcgen05": 1}  # OEC_CNN_CONV_MMA_SYNC, OEC_CNN_CONV_TCGEN05
+CONV_KERNEL = "mma.sync"  # default kernel of the 3x3 convolutions
 
 
 _lib.OTHER_DECLARED.update({"oec_cnn_num_params", "oec_cnn_param_layout", "oec_cnn_act_bytes", "oec_cnn_forward",
                             "oec_cnn_set_weights", "oec_cnn_train_step", "oec_cnn_warm_start_work_bytes",
-                            "oec_cnn_warm_start", "oec_cnn_correct_work_bytes", "oec_cnn_correct"})
+                            "oec_cnn_warm_start", "oec_cnn_correct_work_bytes", "oec_cnn_correct",
+                            "oec_cnn_status"})
 
 SPECS = [(1, 16), (16, 32), (32, 64), (64, 64), (64, 32), (32, 16), (16, 16)]  # (in, out) of e0 e1 e2 e3 d2 d1 d0
 
@@ -46,6 +51,8 @@ def _declare():
         L.oec_cnn_act_bytes.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
         L.oec_cnn_forward.restype = ctypes.c_int
         L.oec_cnn_forward.argtypes = [ctypes.POINTER(Cnn_t), P, P, P]
+        L.oec_cnn_status.restype = ctypes.c_int
+        L.oec_cnn_status.argtypes = [ctypes.POINTER(Cnn_t), P, P]
         L.oec_cnn_set_weights.restype = ctypes.c_int
         L.oec_cnn_set_weights.argtypes = [ctypes.POINTER(Cnn_t), P, P]
         L.oec_cnn_warm_start_work_bytes.restype = ctypes.c_int64
@@ -83,8 +90,12 @@ def init_weights(seed=0):
 class PoissonCNN:
     """The network on one extended grid (nx, ny) with its inside mask."""
 
-    def __init__(self, nx, ny, inside, weights=None, seed=0, training=True, op=None):
+    def __init__(self, nx, ny, inside, weights=None, seed=0, training=True, op=None, conv_kernel=None):
         L = _declare()
+        kernel = CONV_KERNEL if conv_kernel is None else conv_kernel
+        if kernel not in CONV_KERNELS:
+            raise ValueError(f"conv_kernel must be one of {sorted(CONV_KERNELS)}")
+        self.conv_kernel = kernel
         self.nx, self.ny = int(nx), int(ny)
         self.n = L.oec_cnn_num_params()
         self.inside = D.to_device(np.asarray(inside).astype(np.uint8).reshape(-1), torch.uint8)
@@ -98,7 +109,8 @@ class PoissonCNN:
         self.training = bool(training)
         self.op = op  # oec_stencil_t of the scaled operator (residual loss), or None
         self.act = D.empty(int(L.oec_cnn_act_bytes(self.nx, self.ny, 1 if training else 0)), torch.uint8)
-        self.c = Cnn_t(self.nx, self.ny, D.ptr(self.inside), D.ptr(self.w16), D.ptr(self.act))
+        self.c = Cnn_t(self.nx, self.ny, D.ptr(self.inside), D.ptr(self.w16), D.ptr(self.act),
+                       CONV_KERNELS[kernel])
         self._check(L.oec_cnn_set_weights(ctypes.byref(self.c), self.w32.data_ptr(), D.stream()), "set_weights")
         if training:
             self.grad = D.zeros(self.n, torch.float32)
@@ -122,6 +134,14 @@ class PoissonCNN:
 
     def c_handle(self):
         return ctypes.cast(ctypes.pointer(self.c), ctypes.c_void_p)
+
+    def wait_timeouts(self):
+        """Bounded tensor-memory waits of the tcgen05 convolutions that gave
+        up during the last forward pass or training step (0 on a healthy
+        device)."""
+        n = ctypes.c_int32(0)
+        self._check(_declare().oec_cnn_status(ctypes.byref(self.c), ctypes.byref(n), D.stream()), "status")
+        return int(n.value)
 
     def forward(self, x, out=None):
         """z = N(x) on the device (f32 [nx*ny])."""

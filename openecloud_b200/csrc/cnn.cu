@@ -21,9 +21,11 @@
 //
 // Storage: activations and weights in bf16 (NHWC, channels innermost),
 // accumulation in f32.  3x3 convolutions with 16..64 input channels run as
-// implicit GEMMs on the tensor cores (mma.sync m16n8k16 bf16 -> f32,
-// operands staged in shared memory and fetched with ldmatrix); the
-// single-channel input convolution and the 1x1 output use the f32 pipes.  The
+// implicit GEMMs on the tensor cores, in one of two kernels chosen by
+// oec_cnn_t.conv_kernel: tcgen05.mma with the accumulators in tensor memory
+// (umma.cuh), or the warp-level mma.sync m16n8k16 bf16 -> f32 with operands
+// fetched by ldmatrix (below); the single-channel input convolution and the
+// 1x1 output use the f32 pipes.  The
 // data gradient of a 3x3 convolution is the same kernel with the weights
 // flipped and transposed; the weight gradients (training only) are f32
 // reductions over the pixels.
@@ -32,6 +34,7 @@
 #include <stdint.h>
 
 #include "oec_common.cuh"
+#include "umma.cuh"
 
 typedef __nv_bfloat16 bf16;
 
@@ -642,8 +645,7 @@ size_t carve_buffers(void *base, int nx, int ny, bool training, Buffers *b) {
 int grid_for(size_t n, int per_sm = 8) { return persistent_grid((int64_t)((n + 255) / 256), per_sm); }
 
 template <int CI, int CO>
-int conv3(const Level &L, const bf16 *in, const bf16 *w, bf16 *out, int *err, cudaStream_t s) {
-    (void)err;
+int conv3_mma_sync(const Level &L, const bf16 *in, const bf16 *w, bf16 *out, cudaStream_t s) {
     constexpr int smem = conv_smem_bytes<CI, CO>();
     static std::atomic<int> attr[kMaxDevices];
     if (per_device_cached(attr, [] {
@@ -657,6 +659,35 @@ int conv3(const Level &L, const bf16 *in, const bf16 *w, bf16 *out, int *err, cu
     k_conv3_mma<CI, CO><<<persistent_grid(tiles, 2), 128, smem, s>>>(L.h, L.w, in, w, out);
     OEC_LAUNCH_CHECK();
     return OEC_OK;
+}
+
+template <int CI, int CO>
+int conv3_tcgen05(const Level &L, const bf16 *in, const bf16 *w, bf16 *out, int *err, cudaStream_t s) {
+    using S = umma::ConvSmem<CI, CO>;
+    // resident CTAs per SM (shared memory and tensor-memory columns bound it), per device
+    static std::atomic<int> per_sm_cache[kMaxDevices];
+    const int per_sm = per_device_cached(per_sm_cache, [] {
+        int b = 0;
+        if (cudaFuncSetAttribute(umma::k_conv3<CI, CO>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kBytes) !=
+                cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, umma::k_conv3<CI, CO>, umma::kThreads, S::kBytes) !=
+                cudaSuccess)
+            return -1;
+        return b < 512 / S::kCols ? b : 512 / S::kCols;
+    });
+    if (per_sm < 1) return OEC_ERR_CUDA;
+    const int tiles = L.h * ((L.w + umma::kM - 1) / umma::kM);
+    umma::k_conv3<CI, CO><<<persistent_grid(tiles, per_sm), umma::kThreads, S::kBytes, s>>>(L.h, L.w, in, w, out,
+                                                                                             err);
+    OEC_LAUNCH_CHECK();
+    return OEC_OK;
+}
+
+// One 3x3 convolution by the kernel the network selects.
+template <int CI, int CO>
+int conv3(int kernel, const Level &L, const bf16 *in, const bf16 *w, bf16 *out, int *err, cudaStream_t s) {
+    if (kernel == OEC_CNN_CONV_TCGEN05) return conv3_tcgen05<CI, CO>(L, in, w, out, err, s);
+    return conv3_mma_sync<CI, CO>(L, in, w, out, s);
 }
 
 template <int C>
@@ -682,7 +713,8 @@ void conv3_dw(const Level &L, int ci, int co, const bf16 *X, const bf16 *G, floa
 }
 
 bool valid_cnn(const oec_cnn_t *c) {
-    return c && c->nx >= 3 && c->ny >= 3 && c->inside && c->w16 && c->act;
+    return c && c->nx >= 3 && c->ny >= 3 && c->inside && c->w16 && c->act &&
+           (c->conv_kernel == OEC_CNN_CONV_MMA_SYNC || c->conv_kernel == OEC_CNN_CONV_TCGEN05);
 }
 
 int forward(const oec_cnn_t *c, const float *x, Buffers &b, cudaStream_t s) {
@@ -690,21 +722,22 @@ int forward(const oec_cnn_t *c, const float *x, Buffers &b, cudaStream_t s) {
     levels_of(c->nx, c->ny, L);
     const bf16 *w = reinterpret_cast<const bf16 *>(c->w16);
     const size_t n0 = (size_t)c->nx * c->ny;
+    OEC_CUDA_TRY(cudaMemsetAsync(b.err, 0, sizeof(int), s));
     k_conv3_in1<<<grid_for(n0), 256, 0, s>>>(L[0].h, L[0].w, x, c->inside, w + conv_offset(0), b.e0, b.x16);
     OEC_LAUNCH_CHECK();
     pool<16>(L[0], L[1], b.e0, b.p1, s);
-    int rc = conv3<16, 32>(L[1], b.p1, w + conv_offset(1), b.e1, b.err, s);
+    int rc = conv3<16, 32>(c->conv_kernel, L[1], b.p1, w + conv_offset(1), b.e1, b.err, s);
     if (rc) return rc;
     pool<32>(L[1], L[2], b.e1, b.p2, s);
-    if ((rc = conv3<32, 64>(L[2], b.p2, w + conv_offset(2), b.e2, b.err, s))) return rc;
+    if ((rc = conv3<32, 64>(c->conv_kernel, L[2], b.p2, w + conv_offset(2), b.e2, b.err, s))) return rc;
     pool<64>(L[2], L[3], b.e2, b.p3, s);
-    if ((rc = conv3<64, 64>(L[3], b.p3, w + conv_offset(3), b.e3, b.err, s))) return rc;
+    if ((rc = conv3<64, 64>(c->conv_kernel, L[3], b.p3, w + conv_offset(3), b.e3, b.err, s))) return rc;
     up_add<64>(L[2], L[3], 1.f, b.e3, b.e2, b.u2, s);
-    if ((rc = conv3<64, 32>(L[2], b.u2, w + conv_offset(4), b.d2, b.err, s))) return rc;
+    if ((rc = conv3<64, 32>(c->conv_kernel, L[2], b.u2, w + conv_offset(4), b.d2, b.err, s))) return rc;
     up_add<32>(L[1], L[2], 1.f, b.d2, b.e1, b.u1, s);
-    if ((rc = conv3<32, 16>(L[1], b.u1, w + conv_offset(5), b.d1, b.err, s))) return rc;
+    if ((rc = conv3<32, 16>(c->conv_kernel, L[1], b.u1, w + conv_offset(5), b.d1, b.err, s))) return rc;
     up_add<16>(L[0], L[1], 1.f, b.d1, b.e0, b.u0, s);
-    if ((rc = conv3<16, 16>(L[0], b.u0, w + conv_offset(6), b.d0, b.err, s))) return rc;
+    if ((rc = conv3<16, 16>(c->conv_kernel, L[0], b.u0, w + conv_offset(6), b.d0, b.err, s))) return rc;
     OEC_LAUNCH_CHECK();
     return OEC_OK;
 }
@@ -754,6 +787,16 @@ extern "C" int oec_cnn_forward(const oec_cnn_t *c, const float *x_dev, float *z_
     return OEC_OK;
 }
 
+extern "C" int oec_cnn_status(const oec_cnn_t *c, int32_t *wait_timeouts_host, void *stream) {
+    if (!valid_cnn(c) || !wait_timeouts_host) return OEC_ERR_INVALID;
+    cudaStream_t s = as_stream(stream);
+    Buffers b;
+    carve_buffers(c->act, c->nx, c->ny, false, &b);
+    OEC_CUDA_TRY(cudaMemcpyAsync(wait_timeouts_host, b.err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    OEC_CUDA_TRY(cudaStreamSynchronize(s));
+    return OEC_OK;
+}
+
 extern "C" int oec_cnn_train_step(const oec_cnn_t *c, const oec_stencil_t *op, const float *x_dev,
                                   const float *target_dev, float *z_dev, float *w32_dev, float *grad_dev,
                                   float *adam_m_dev, float *adam_v_dev, void *wt16_dev, float lr, int32_t step,
@@ -797,29 +840,29 @@ extern "C" int oec_cnn_train_step(const oec_cnn_t *c, const oec_stencil_t *op, c
                                                 grad_dev + kOutOffset);
     // d0 = conv(u0)
     conv3_dw(L[0], 16, 16, b.u0, b.gd0, grad_dev + conv_offset(6), s);
-    if ((rc = conv3<16, 16>(L[0], b.gd0, wt + conv_offset(6), b.gu0, b.err, s))) return rc;
+    if ((rc = conv3<16, 16>(c->conv_kernel, L[0], b.gd0, wt + conv_offset(6), b.gu0, b.err, s))) return rc;
     // u0 = up(d1) + e0
     down_sum<16>(L[0], L[1], b.gu0, b.gd1, s);
     // d1 = conv(u1)
     conv3_dw(L[1], 32, 16, b.u1, b.gd1, grad_dev + conv_offset(5), s);
-    if ((rc = conv3<16, 32>(L[1], b.gd1, wt + conv_offset(5), b.gu1, b.err, s))) return rc;
+    if ((rc = conv3<16, 32>(c->conv_kernel, L[1], b.gd1, wt + conv_offset(5), b.gu1, b.err, s))) return rc;
     // u1 = up(d2) + e1
     down_sum<32>(L[1], L[2], b.gu1, b.gd2, s);
     // d2 = conv(u2)
     conv3_dw(L[2], 64, 32, b.u2, b.gd2, grad_dev + conv_offset(4), s);
-    if ((rc = conv3<32, 64>(L[2], b.gd2, wt + conv_offset(4), b.gu2, b.err, s))) return rc;
+    if ((rc = conv3<32, 64>(c->conv_kernel, L[2], b.gd2, wt + conv_offset(4), b.gu2, b.err, s))) return rc;
     // u2 = up(e3) + e2
     down_sum<64>(L[2], L[3], b.gu2, b.ge3, s);
     // e3 = conv(p3)
     conv3_dw(L[3], 64, 64, b.p3, b.ge3, grad_dev + conv_offset(3), s);
-    if ((rc = conv3<64, 64>(L[3], b.ge3, wt + conv_offset(3), b.gp3, b.err, s))) return rc;
+    if ((rc = conv3<64, 64>(c->conv_kernel, L[3], b.ge3, wt + conv_offset(3), b.gp3, b.err, s))) return rc;
     // p3 = pool(e2); e2 also feeds u2
     up_add<64>(L[2], L[3], 0.25f, b.gp3, b.gu2, b.ge2, s);
     conv3_dw(L[2], 32, 64, b.p2, b.ge2, grad_dev + conv_offset(2), s);
-    if ((rc = conv3<64, 32>(L[2], b.ge2, wt + conv_offset(2), b.gp2, b.err, s))) return rc;
+    if ((rc = conv3<64, 32>(c->conv_kernel, L[2], b.ge2, wt + conv_offset(2), b.gp2, b.err, s))) return rc;
     up_add<32>(L[1], L[2], 0.25f, b.gp2, b.gu1, b.ge1, s);
     conv3_dw(L[1], 16, 32, b.p1, b.ge1, grad_dev + conv_offset(1), s);
-    if ((rc = conv3<32, 16>(L[1], b.ge1, wt + conv_offset(1), b.gp1, b.err, s))) return rc;
+    if ((rc = conv3<32, 16>(c->conv_kernel, L[1], b.ge1, wt + conv_offset(1), b.gp1, b.err, s))) return rc;
     up_add<16>(L[0], L[1], 0.25f, b.gp1, b.gu0, b.ge0, s);
     conv3_dw(L[0], 1, 16, b.x16, b.ge0, grad_dev + conv_offset(0), s);
     OEC_LAUNCH_CHECK();

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <utility>
 
 #include "oec.h"
 
@@ -92,6 +93,35 @@ int per_device_cached(std::atomic<int> *slots, F compute) {
 
 // Number of SMs of the current device (cached per device).
 int sm_count();
+
+// Programmatic dependent launch.  A kernel launched by launch_overlapped may
+// be scheduled while the kernel before it on the stream (or before it in a
+// captured graph) still runs; its first statement is pdl_wait(), which
+// returns once that kernel has finished and its writes are visible, and
+// pdl_launch() then lets the next kernel be scheduled early in turn.  Both
+// are no-ops in a kernel launched the ordinary way.  Setting the environment
+// variable OEC_NO_PDL=1 before the first launch turns the overlap off (for
+// timing comparisons).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+bool pdl_enabled();
+
+template <typename... P, typename... A>
+cudaError_t launch_overlapped(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              A &&...args) {
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
 
 // Persistent grid: enough CTAs to cover `work_items` CTA-sized chunks, at
 // most `per_sm` resident CTAs per SM.

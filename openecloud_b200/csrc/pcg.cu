@@ -20,6 +20,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <cooperative_groups.h>
+
 #include <map>
 #include <mutex>
 #include <string>
@@ -207,6 +209,8 @@ __global__ void __launch_bounds__(kT) k_apply32(int nx, int G, const float *__re
                                                 const float *__restrict__ ey, const uint8_t *__restrict__ in,
                                                 const float *__restrict__ p, float *__restrict__ q, Acc *acc,
                                                 const Ctl *c, cudaGraphConditionalHandle h_inner) {
+    pdl_wait();
+    pdl_launch();
     Acc *a = acc + c->slot;
     if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h_inner, 0);
     double pq = 0.0;
@@ -230,6 +234,8 @@ __global__ void __launch_bounds__(kT) k_update32(int G, const float *__restrict_
                                                  const float *__restrict__ p, const float *__restrict__ q,
                                                  float *__restrict__ d, float *__restrict__ r,
                                                  float *__restrict__ z, Acc *acc, const Ctl *c) {
+    pdl_wait();
+    pdl_launch();
     Acc *a = acc + c->slot;
     const double pq = a->pq, rzv = a->rz;
     if (!(pq > 0.0) || !isfinite(rzv)) {
@@ -263,6 +269,8 @@ __global__ void __launch_bounds__(kT) k_update32(int G, const float *__restrict_
 __global__ void __launch_bounds__(kT) k_zdots32(int G, const float *__restrict__ r, const float *__restrict__ zn,
                                                 const float *__restrict__ q, float *__restrict__ z, Acc *acc,
                                                 const Ctl *c) {
+    pdl_wait();
+    pdl_launch();
     Acc *a = acc + c->slot;
     double rzn = 0.0, zq = 0.0;
     for (int i = blockIdx.x * kT + threadIdx.x; i < G; i += gridDim.x * kT) {
@@ -286,6 +294,8 @@ __global__ void __launch_bounds__(kT) k_zdots32(int G, const float *__restrict__
 __global__ void __launch_bounds__(kT) k_direction32(int G, const float *__restrict__ z, float *__restrict__ p,
                                                     Acc *acc, Ctl *c, int max_iter, oec_pcg_stats_t *stats,
                                                     cudaGraphConditionalHandle h_inner) {
+    pdl_wait();
+    pdl_launch();
     const int slot = c->slot;
     Acc *a = acc + slot, *next = acc + (slot ^ 1);
     const double rz = a->rz;
@@ -411,6 +421,8 @@ __device__ __forceinline__ void tile_sweep(const MgT &L, float om, const float *
 template <int SX, int SY>
 __global__ void __launch_bounds__(kT) k_mg_down(MgT L, float om, const float *__restrict__ b, float *__restrict__ x,
                                                 float *__restrict__ bc, int cnx, int cny) {
+    pdl_wait();
+    pdl_launch();
     __shared__ float s1[(kTY + 4) * (kTX + 4)];
     __shared__ float s2[(kTY + 2) * (kTX + 2)];
     const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY;
@@ -462,6 +474,8 @@ __global__ void __launch_bounds__(kT) k_mg_up(MgT L, float om, float scale, cons
                                               const float *__restrict__ x, const float *__restrict__ yc, int cnx,
                                               float *__restrict__ out, const float *__restrict__ q, Acc *acc,
                                               const Ctl *ctl) {
+    pdl_wait();
+    pdl_launch();
     __shared__ float s1[(kTY + 4) * (kTX + 4)];
     __shared__ float s2[(kTY + 2) * (kTX + 2)];
     const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY;
@@ -544,6 +558,8 @@ __device__ __forceinline__ void sm_sweep(const SmLevel &L, float om, const float
 // shared memory: b, x, y), which lets larger levels into this kernel.
 __global__ void __launch_bounds__(kBlockThreads) k_mg_block(MgBlock P, const float *__restrict__ b_in,
                                                             float *__restrict__ y_out, int coef_smem) {
+    pdl_wait();
+    pdl_launch();
     extern __shared__ float sm[];
     __shared__ SmLevel Ls[kMgMaxBlockLevels];
     if (threadIdx.x == 0) {
@@ -641,10 +657,276 @@ __global__ void __launch_bounds__(kBlockThreads) k_mg_block(MgBlock P, const flo
     for (int i = threadIdx.x; i < T.n; i += kBlockThreads) y_out[i] = T.y[i];
 }
 
+// ------------------------------------------------ one-cluster coarse levels
+//
+// The levels from the cluster level down, solved by one thread-block cluster
+// of up to 16 CTAs (oec_mg_t.cluster_top): each level's rows are dealt out
+// in bands of `rows` consecutive rows per CTA, and a CTA keeps its bands of
+// b, x and y in its shared memory; the rows beyond a band (stencil
+// neighbours, aggregation children and parents) are read from the other
+// CTAs' shared memory through the cluster's distributed shared memory.  The
+// phases of the V-cycle are separated by cluster barriers instead of kernel
+// launches.  The arithmetic of every node is the one-CTA kernel's
+// (k_mg_block), in the same order.
+
+constexpr int kClusterMax = 16;
+constexpr int kClusterLevels = 12;
+constexpr int kClusterThreads = 1024;
+
+struct MgCluster {
+    int nl;       // levels, top (the cluster level) to bottom
+    int ncta;     // CTAs of the cluster
+    int m;        // inside nodes of the bottom level
+    int nx[kClusterLevels], ny[kClusterLevels];
+    int rows[kClusterLevels];  // rows of a band: ceil(ny / ncta)
+    int off[kClusterLevels];   // float offset of the level's b band; x, y follow at +span, +2 span
+    const float *ex[kClusterLevels], *ey[kClusterLevels], *leak[kClusterLevels], *dinv[kClusterLevels];
+    const int32_t *idx;
+    const float *inv;
+    float om, scale;
+    const float *b_top;  // right-hand side of the top level (global)
+    float *out;          // result of the top level (global)
+    const float *q;      // with acc: CG dots r.z and z.q of the top level
+    Acc *acc;
+    const Ctl *ctl;
+};
+
+size_t mg_cluster_floats(const MgCluster &P) {
+    size_t n = 0;
+    for (int l = 0; l < P.nl; ++l) n += 3 * (size_t)P.rows[l] * P.nx[l];
+    return n;
+}
+
+struct ClLevel {
+    int nx, ny, R, off;
+    const float *ex, *ey, *lk, *dv;
+};
+
+// Pointer to node (r, 0) of array a (0 b, 1 x, 2 y) of level L, in the CTA
+// that owns row r.
+__device__ __forceinline__ float *cl_row(float *const *base, const ClLevel &L, int a, int r) {
+    const int o = r / L.R;
+    return base[o] + L.off + a * L.R * L.nx + (r - o * L.R) * L.nx;
+}
+
+// (A v)_i at node (r, c) of level L, the rows r-1, r, r+1 of v given.
+__device__ __forceinline__ float cl_apply(const ClLevel &L, int i, int r, int c, const float *vm, const float *v0,
+                                          const float *vp) {
+    const float vi = v0[c];
+    float y = L.lk[i] * vi;
+    if (c + 1 < L.nx) y += L.ex[i] * (vi - v0[c + 1]);
+    if (c > 0) y += L.ex[i - 1] * (vi - v0[c - 1]);
+    if (r + 1 < L.ny) y += L.ey[i] * (vi - vp[c]);
+    if (r > 0) y += L.ey[i - L.nx] * (vi - vm[c]);
+    return y;
+}
+
+__device__ __forceinline__ void cl_sync() { cooperative_groups::this_cluster().sync(); }
+
+__device__ __forceinline__ double cl_block_sum(double v, double *sh) {
+    v = warp_sum(v);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (w == 0) {
+        s = l < kClusterThreads / 32 ? sh[l] : 0.0;
+        s = warp_sum(s);
+    }
+    __syncthreads();
+    return s;
+}
+
+__global__ void __launch_bounds__(kClusterThreads, 1) k_mg_cluster(MgCluster P) {
+    pdl_wait();
+    pdl_launch();
+    extern __shared__ __align__(16) float smc[];
+    __shared__ float *base[kClusterMax];
+    __shared__ ClLevel Ls[kClusterLevels];
+    __shared__ double red[kClusterThreads / 32];
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    const unsigned me = cluster.block_rank();
+    if (threadIdx.x < P.ncta) base[threadIdx.x] = cluster.map_shared_rank(smc, threadIdx.x);
+    if (threadIdx.x < P.nl) {
+        const int l = threadIdx.x;
+        Ls[l] = ClLevel{P.nx[l], P.ny[l], P.rows[l], P.off[l], P.ex[l], P.ey[l], P.leak[l], P.dinv[l]};
+    }
+    __syncthreads();
+    const float om = P.om;
+    // own band of level L: rows [r0, r1), nodes [r0*nx, r1*nx)
+    auto band = [&](const ClLevel &L, int &r0, int &r1) {
+        r0 = min((int)me * L.R, L.ny);
+        r1 = min(r0 + L.R, L.ny);
+    };
+    {  // top right-hand side into the band; bottom result cleared
+        const ClLevel &T = Ls[0];
+        int r0, r1;
+        band(T, r0, r1);
+        float *b = smc + T.off;
+        for (int e = threadIdx.x; e < (r1 - r0) * T.nx; e += kClusterThreads) b[e] = P.b_top[r0 * T.nx + e];
+        const ClLevel &B = Ls[P.nl - 1];
+        band(B, r0, r1);
+        float *y = smc + B.off + 2 * B.R * B.nx;
+        for (int e = threadIdx.x; e < (r1 - r0) * B.nx; e += kClusterThreads) y[e] = 0.f;
+    }
+    cl_sync();
+    // ---- down
+    for (int l = 0; l + 1 < P.nl; ++l) {
+        const ClLevel &L = Ls[l], &C = Ls[l + 1];
+        const int sx = C.nx != L.nx, sy = C.ny != L.ny;
+        int r0, r1;
+        band(L, r0, r1);
+        // x = y0 + w D^-1 (b - A y0), y0 = w D^-1 b (formed on the fly from b)
+        for (int e = threadIdx.x; e < (r1 - r0) * L.nx; e += kClusterThreads) {
+            const int lr = e / L.nx, c = e - lr * L.nx, r = r0 + lr, i = r * L.nx + c;
+            float *x = smc + L.off + L.R * L.nx + lr * L.nx;
+            const float d = L.dv[i];
+            if (d == 0.f) {
+                x[c] = 0.f;
+                continue;
+            }
+            const float *b0 = cl_row(base, L, 0, r);
+            const float *bm = r > 0 ? cl_row(base, L, 0, r - 1) : b0;
+            const float *bp = r + 1 < L.ny ? cl_row(base, L, 0, r + 1) : b0;
+            const float yi = om * d * b0[c];
+            float ax = L.lk[i] * yi;
+            if (c + 1 < L.nx) ax += L.ex[i] * (yi - om * L.dv[i + 1] * b0[c + 1]);
+            if (c > 0) ax += L.ex[i - 1] * (yi - om * L.dv[i - 1] * b0[c - 1]);
+            if (r + 1 < L.ny) ax += L.ey[i] * (yi - om * L.dv[i + L.nx] * bp[c]);
+            if (r > 0) ax += L.ey[i - L.nx] * (yi - om * L.dv[i - L.nx] * bm[c]);
+            x[c] = yi + om * d * (b0[c] - ax);
+        }
+        cl_sync();
+        // coarse right-hand side: sum over the inside children of b - A x
+        int R0, R1;
+        band(C, R0, R1);
+        for (int e = threadIdx.x; e < (R1 - R0) * C.nx; e += kClusterThreads) {
+            const int lr = e / C.nx, Cc = e - lr * C.nx, R = R0 + lr;
+            float s = 0.f;
+#pragma unroll
+            for (int dd = 0; dd < 4; ++dd) {
+                const int r = (R << sy) + (dd >> 1), c = (Cc << sx) + (dd & 1);
+                if ((dd >> 1) <= sy && (dd & 1) <= sx && r < L.ny && c < L.nx) {
+                    const int i = r * L.nx + c;
+                    if (L.dv[i] != 0.f) {
+                        const float *x0 = cl_row(base, L, 1, r);
+                        const float *xm = r > 0 ? cl_row(base, L, 1, r - 1) : x0;
+                        const float *xp = r + 1 < L.ny ? cl_row(base, L, 1, r + 1) : x0;
+                        s += cl_row(base, L, 0, r)[c] - cl_apply(L, i, r, c, xm, x0, xp);
+                    }
+                }
+            }
+            smc[C.off + lr * C.nx + Cc] = s;
+        }
+        cl_sync();
+    }
+    {  // bottom: y[idx[r]] = sum_c inv[r][c] b[idx[c]], one warp per row
+        const ClLevel &B = Ls[P.nl - 1];
+        const int lane = threadIdx.x & 31;
+        const int warps = P.ncta * (kClusterThreads / 32);
+        for (int r = (int)me * (kClusterThreads / 32) + (threadIdx.x >> 5); r < P.m; r += warps) {
+            const float *row = P.inv + (size_t)r * P.m;
+            float s = 0.f;
+            for (int c = lane; c < P.m; c += 32) {
+                const int j = P.idx[c], jr = j / B.nx;
+                s = fmaf(row[c], cl_row(base, B, 0, jr)[j - jr * B.nx], s);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFullMask, s, o);
+            if (lane == 0) {
+                const int j = P.idx[r], jr = j / B.nx;
+                cl_row(base, B, 2, jr)[j - jr * B.nx] = s;
+            }
+        }
+        cl_sync();
+    }
+    // ---- up
+    for (int l = P.nl - 2; l >= 0; --l) {
+        const ClLevel &L = Ls[l], &C = Ls[l + 1];
+        const int sx = C.nx != L.nx, sy = C.ny != L.ny;
+        int r0, r1;
+        band(L, r0, r1);
+        const int n = (r1 - r0) * L.nx;
+        float *bb = smc + L.off, *xx = bb + L.R * L.nx, *yy = xx + L.R * L.nx;
+        // y = x + scale * (coarse result at the parent) on the inside nodes
+        for (int e = threadIdx.x; e < n; e += kClusterThreads) {
+            const int lr = e / L.nx, c = e - lr * L.nx, r = r0 + lr, i = r * L.nx + c;
+            const int pr = r >> sy;
+            yy[e] = L.dv[i] != 0.f ? xx[e] + P.scale * cl_row(base, C, 2, pr)[c >> sx] : 0.f;
+        }
+        cl_sync();
+        // two sweeps: y -> x -> y
+        for (int sweep = 0; sweep < 2; ++sweep) {
+            const int src = sweep == 0 ? 2 : 1;
+            float *dst = sweep == 0 ? xx : yy;
+            const bool last = sweep == 1 && l == 0;
+            double rz = 0.0, zq = 0.0;
+            for (int e = threadIdx.x; e < n; e += kClusterThreads) {
+                const int lr = e / L.nx, c = e - lr * L.nx, r = r0 + lr, i = r * L.nx + c;
+                const float d = L.dv[i];
+                float v = 0.f;
+                if (d != 0.f) {
+                    const float *v0 = cl_row(base, L, src, r);
+                    const float *vm = r > 0 ? cl_row(base, L, src, r - 1) : v0;
+                    const float *vp = r + 1 < L.ny ? cl_row(base, L, src, r + 1) : v0;
+                    v = v0[c] + om * d * (bb[e] - cl_apply(L, i, r, c, vm, v0, vp));
+                }
+                if (last) {
+                    P.out[i] = v;
+                    if (P.acc) {
+                        rz += (double)bb[e] * (double)v;
+                        zq += (double)v * (double)P.q[i];
+                    }
+                } else {
+                    dst[e] = v;
+                }
+            }
+            if (last && P.acc) {
+                Acc *a = P.acc + P.ctl->slot;
+                rz = cl_block_sum(rz, red);
+                zq = cl_block_sum(zq, red);
+                if (threadIdx.x == 0) {
+                    if (rz != 0.0) atomicAdd(&a->rzn, rz);
+                    if (zq != 0.0) atomicAdd(&a->zq, zq);
+                }
+            }
+            cl_sync();
+        }
+    }
+    if (P.nl == 1) {  // the top level is the bottom: its result to out
+        const ClLevel &B = Ls[0];
+        int r0, r1;
+        band(B, r0, r1);
+        const float *y = smc + B.off + 2 * B.R * B.nx;
+        double rz = 0.0, zq = 0.0;
+        for (int e = threadIdx.x; e < (r1 - r0) * B.nx; e += kClusterThreads) {
+            const int i = r0 * B.nx + e;
+            P.out[i] = y[e];
+            if (P.acc) {
+                rz += (double)smc[B.off + e] * (double)y[e];
+                zq += (double)y[e] * (double)P.q[i];
+            }
+        }
+        if (P.acc) {
+            Acc *a = P.acc + P.ctl->slot;
+            rz = cl_block_sum(rz, red);
+            zq = cl_block_sum(zq, red);
+            if (threadIdx.x == 0) {
+                if (rz != 0.0) atomicAdd(&a->rzn, rz);
+                if (zq != 0.0) atomicAdd(&a->zq, zq);
+            }
+        }
+        cl_sync();
+    }
+}
+
 // acc[slot].rzn += r.z, acc[slot].zq += z.q (used when the block kernel
 // writes z itself).
 __global__ void __launch_bounds__(kT) k_dots32(int G, const float *__restrict__ r, const float *__restrict__ z,
                                                const float *__restrict__ q, Acc *acc, const Ctl *ctl) {
+    pdl_wait();
+    pdl_launch();
     acc += ctl->slot;
     double rzn = 0.0, zq = 0.0;
     for (int i = blockIdx.x * kT + threadIdx.x; i < G; i += gridDim.x * kT) {
@@ -704,11 +986,110 @@ bool valid_mg(const oec_mg_t *mg) {
     return mg_block_smem(mg) <= kMgMaxBlockSmem;
 }
 
+// The cluster size used for the one-cluster levels on this device: 16 CTAs
+// when a cluster of 16 with the largest shared-memory size can be resident,
+// else 8 (portable); 0 when clusters cannot run.
+int mg_cluster_ctas() {
+    static std::atomic<int> cached[kMaxDevices];
+    return per_device_cached(cached, [] {
+        constexpr int smem = (int)kMgMaxBlockSmem;
+        if (cudaFuncSetAttribute(k_mg_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+            return -1;
+        for (int n : {16, 8}) {
+            if (n > 8 && cudaFuncSetAttribute(k_mg_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                             cudaSuccess)
+                continue;
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(n);
+            cfg.blockDim = dim3(kClusterThreads);
+            cfg.dynamicSmemBytes = smem;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = n;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            int clusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&clusters, k_mg_cluster, &cfg) == cudaSuccess && clusters >= 1)
+                return n;
+        }
+        cudaGetLastError();
+        return -1;
+    });
+}
+
+// First level of the one-cluster solve: the first of at most
+// mg->cluster_top nodes, no lower than the block level.
+int mg_cluster_top_level(const oec_mg_t *mg) {
+    for (int k = 0; k < mg->block_level; ++k)
+        if ((int64_t)mg->levels[k].nx * mg->levels[k].ny <= mg->cluster_top) return k;
+    return mg->block_level;
+}
+
+// The plan of the one-cluster levels (top level to the bottom): bands and
+// shared-memory offsets.  False when the cluster path is off or does not
+// fit; the one-CTA block path is used instead.
+bool mg_cluster_plan(const oec_mg_t *mg, MgCluster &P) {
+    if (mg->cluster_top <= 0) return false;
+    const int ncta = mg_cluster_ctas();
+    if (ncta <= 0) return false;
+    const int top = mg_cluster_top_level(mg);
+    if (mg->nlevels - top > kClusterLevels) return false;
+    P = MgCluster{};
+    P.nl = mg->nlevels - top;
+    P.ncta = ncta;
+    P.m = mg->ncoarse;
+    int off = 0;
+    for (int j = 0; j < P.nl; ++j) {
+        const oec_mg_level_t &l = mg->levels[top + j];
+        P.nx[j] = l.nx;
+        P.ny[j] = l.ny;
+        P.rows[j] = (l.ny + ncta - 1) / ncta;
+        P.off[j] = off;
+        off += 3 * P.rows[j] * l.nx;
+        P.ex[j] = l.ex;
+        P.ey[j] = l.ey;
+        P.leak[j] = l.leak;
+        P.dinv[j] = l.dinv;
+    }
+    if ((size_t)off * sizeof(float) > kMgMaxBlockSmem) return false;
+    P.idx = mg->coarse_idx;
+    P.inv = mg->coarse_inv;
+    P.om = mg->omega;
+    P.scale = mg->scale;
+    return true;
+}
+
+int launch_mg_cluster(const MgCluster &P, cudaStream_t s) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(P.ncta);
+    cfg.blockDim = dim3(kClusterThreads);
+    cfg.dynamicSmemBytes = mg_cluster_floats(P) * sizeof(float);
+    cfg.stream = s;
+    cudaLaunchAttribute at[2];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = P.ncta;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[1].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl_enabled() ? 2 : 1;
+    OEC_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_mg_cluster, P));
+    return OEC_OK;
+}
+
 // One V-cycle z = M r; with acc, also the flexible-CG dot products r.z and
 // z.q into acc[ctl->slot] (q the operator image of the current direction).
+// Levels above the coarse solve run as tiled kernels over the whole GPU; the
+// coarse levels run in one cluster (mg->cluster_top) or one CTA.
 int mg_cycle(const oec_mg_t *mg, const float *r, float *z, const float *q, Acc *acc, const Ctl *ctl,
              cudaStream_t s) {
-    const int L = mg->nlevels, B = mg->block_level;
+    const int L = mg->nlevels;
+    MgCluster C;
+    const bool clustered = mg_cluster_plan(mg, C);
+    const int B = clustered ? mg_cluster_top_level(mg) : mg->block_level;
     const oec_mg_level_t *lv = mg->levels;
     for (int k = 0; k < B; ++k) {
         const oec_mg_level_t &l = lv[k], &c = lv[k + 1];
@@ -716,42 +1097,56 @@ int mg_cycle(const oec_mg_t *mg, const float *r, float *z, const float *q, Acc *
         const MgT m = mg_t(l, k > 0);
         const float *b = k == 0 ? r : l.b;
         switch (mg_shift(l, c)) {
-            case 3: k_mg_down<1, 1><<<grid, kT, 0, s>>>(m, mg->omega, b, l.x, c.b, c.nx, c.ny); break;
-            case 2: k_mg_down<0, 1><<<grid, kT, 0, s>>>(m, mg->omega, b, l.x, c.b, c.nx, c.ny); break;
-            case 1: k_mg_down<1, 0><<<grid, kT, 0, s>>>(m, mg->omega, b, l.x, c.b, c.nx, c.ny); break;
+            case 3: OEC_CUDA_TRY(launch_overlapped(k_mg_down<1, 1>, grid, dim3(kT), 0, s, m, mg->omega, b, l.x, c.b, c.nx, c.ny)); break;
+            case 2: OEC_CUDA_TRY(launch_overlapped(k_mg_down<0, 1>, grid, dim3(kT), 0, s, m, mg->omega, b, l.x, c.b, c.nx, c.ny)); break;
+            case 1: OEC_CUDA_TRY(launch_overlapped(k_mg_down<1, 0>, grid, dim3(kT), 0, s, m, mg->omega, b, l.x, c.b, c.nx, c.ny)); break;
             default: return OEC_ERR_INVALID;
         }
     }
-    MgBlock P{};
-    P.nb = L - B;
-    P.m = mg->ncoarse;
-    for (int k = B; k < L; ++k) {
-        const int j = k - B;
-        P.nx[j] = lv[k].nx;
-        P.ny[j] = lv[k].ny;
-        P.ex[j] = lv[k].ex;
-        P.ey[j] = lv[k].ey;
-        P.leak[j] = lv[k].leak;
-        P.dinv[j] = lv[k].dinv;
-    }
-    P.idx = mg->coarse_idx;
-    P.inv = mg->coarse_inv;
-    P.om = mg->omega;
-    P.scale = mg->scale;
-    const size_t smem = mg_block_smem(mg);
-    if (smem > 48 * 1024) {
-        // the largest dynamic shared-memory size enabled so far, per device
-        static std::atomic<size_t> attr_set[kMaxDevices];
-        int dev = 0;
-        OEC_CUDA_TRY(cudaGetDevice(&dev));
-        if (dev < 0 || dev >= kMaxDevices) return OEC_ERR_INVALID;
-        if (smem > attr_set[dev].load()) {
-            OEC_CUDA_TRY(cudaFuncSetAttribute(k_mg_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMgMaxBlockSmem));
-            attr_set[dev].store(kMgMaxBlockSmem);
+    if (clustered) {
+        C.b_top = B == 0 ? r : lv[B].b;
+        C.out = B == 0 ? z : lv[B].y;
+        if (B == 0 && acc) {
+            C.q = q;
+            C.acc = acc;
+            C.ctl = ctl;
         }
+        OEC_TRY(launch_mg_cluster(C, s));
+    } else {
+        MgBlock P{};
+        P.nb = L - B;
+        P.m = mg->ncoarse;
+        for (int k = B; k < L; ++k) {
+            const int j = k - B;
+            P.nx[j] = lv[k].nx;
+            P.ny[j] = lv[k].ny;
+            P.ex[j] = lv[k].ex;
+            P.ey[j] = lv[k].ey;
+            P.leak[j] = lv[k].leak;
+            P.dinv[j] = lv[k].dinv;
+        }
+        P.idx = mg->coarse_idx;
+        P.inv = mg->coarse_inv;
+        P.om = mg->omega;
+        P.scale = mg->scale;
+        const size_t smem = mg_block_smem(mg);
+        if (smem > 48 * 1024) {
+            // the largest dynamic shared-memory size enabled so far, per device
+            static std::atomic<size_t> attr_set[kMaxDevices];
+            int dev = 0;
+            OEC_CUDA_TRY(cudaGetDevice(&dev));
+            if (dev < 0 || dev >= kMaxDevices) return OEC_ERR_INVALID;
+            if (smem > attr_set[dev].load()) {
+                OEC_CUDA_TRY(cudaFuncSetAttribute(k_mg_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)kMgMaxBlockSmem));
+                attr_set[dev].store(kMgMaxBlockSmem);
+            }
+        }
+        const float *bin = B == 0 ? r : lv[B].b;
+        float *yout = B == 0 ? z : lv[B].y;
+        OEC_CUDA_TRY(launch_overlapped(k_mg_block, dim3(1), dim3(kBlockThreads), smem, s, P, bin, yout,
+                                       mg_block_coef_smem(mg) ? 1 : 0));
     }
-    k_mg_block<<<1, kBlockThreads, smem, s>>>(P, B == 0 ? r : lv[B].b, B == 0 ? z : lv[B].y,
-                                              mg_block_coef_smem(mg) ? 1 : 0);
     for (int k = B - 1; k >= 0; --k) {
         const oec_mg_level_t &l = lv[k], &c = lv[k + 1];
         const dim3 grid((l.nx + kTX - 1) / kTX, (l.ny + kTY - 1) / kTY);
@@ -762,15 +1157,16 @@ int mg_cycle(const oec_mg_t *mg, const float *r, float *z, const float *q, Acc *
         Acc *a = k == 0 ? acc : nullptr;
         const float om = mg->omega, sc = mg->scale;
         switch (mg_shift(l, c)) {
-            case 3: k_mg_up<1, 1><<<grid, kT, 0, s>>>(m, om, sc, b, l.x, c.y, c.nx, out, qq, a, ctl); break;
-            case 2: k_mg_up<0, 1><<<grid, kT, 0, s>>>(m, om, sc, b, l.x, c.y, c.nx, out, qq, a, ctl); break;
-            case 1: k_mg_up<1, 0><<<grid, kT, 0, s>>>(m, om, sc, b, l.x, c.y, c.nx, out, qq, a, ctl); break;
+            case 3: OEC_CUDA_TRY(launch_overlapped(k_mg_up<1, 1>, grid, dim3(kT), 0, s, m, om, sc, b, l.x, c.y, c.nx, out, qq, a, ctl)); break;
+            case 2: OEC_CUDA_TRY(launch_overlapped(k_mg_up<0, 1>, grid, dim3(kT), 0, s, m, om, sc, b, l.x, c.y, c.nx, out, qq, a, ctl)); break;
+            case 1: OEC_CUDA_TRY(launch_overlapped(k_mg_up<1, 0>, grid, dim3(kT), 0, s, m, om, sc, b, l.x, c.y, c.nx, out, qq, a, ctl)); break;
             default: return OEC_ERR_INVALID;
         }
     }
-    if (acc && B == 0) {
+    if (acc && B == 0 && !clustered) {
         const int G = lv[0].nx * lv[0].ny;
-        k_dots32<<<persistent_grid((G + kT - 1) / kT, 4), kT, 0, s>>>(G, r, z, q, acc, ctl);
+        OEC_CUDA_TRY(launch_overlapped(k_dots32, dim3(persistent_grid((G + kT - 1) / kT, 4)), dim3(kT), 0, s, G, r, z,
+                                       q, acc, ctl));
     }
     OEC_LAUNCH_CHECK();
     return OEC_OK;
@@ -952,15 +1348,18 @@ int build_solve(const SolveArgs &a, cudaStream_t s) {
                 OEC_TRY(c3.begin(2, b_inner));
                 k_apply32<<<grid, kT, 0, c3.s>>>(nx, G, st->ex32, st->ey32, st->inside, w.p, w.q, w.acc, w.ctl,
                                                  h_inner);
-                k_update32<<<grid, kT, 0, c3.s>>>(G, st->dinv32, pc, w.p, w.q, w.d, w.r, w.z, w.acc, w.ctl);
+                OEC_CUDA_TRY(launch_overlapped(k_update32, dim3(grid), dim3(kT), 0, c3.s, G, st->dinv32, pc, w.p, w.q,
+                                               w.d, w.r, w.z, w.acc, w.ctl));
                 OEC_LAUNCH_CHECK();
                 if (pc == OEC_PRECOND_MG) {
                     OEC_TRY(external_apply(pc, a.ctx, w.r, w.z, w.q, w.acc, w.ctl, c3.s));
                 } else if (external) {
                     OEC_TRY(external_apply(pc, a.ctx, w.r, w.zn, nullptr, nullptr, nullptr, c3.s));
-                    k_zdots32<<<grid, kT, 0, c3.s>>>(G, w.r, w.zn, w.q, w.z, w.acc, w.ctl);
+                    OEC_CUDA_TRY(launch_overlapped(k_zdots32, dim3(grid), dim3(kT), 0, c3.s, G, w.r, w.zn, w.q, w.z,
+                                                   w.acc, w.ctl));
                 }
-                k_direction32<<<grid, kT, 0, c3.s>>>(G, w.z, w.p, w.acc, w.ctl, a.max_iter, a.stats, h_inner);
+                OEC_CUDA_TRY(launch_overlapped(k_direction32, dim3(grid), dim3(kT), 0, c3.s, G, w.z, w.p, w.acc, w.ctl,
+                                               a.max_iter, a.stats, h_inner));
                 OEC_LAUNCH_CHECK();
                 OEC_TRY(c3.end());
             }

@@ -58,11 +58,12 @@ class Mg_t(ctypes.Structure):
     _P = ctypes.c_void_p
     _fields_ = [("nlevels", ctypes.c_int32), ("levels", ctypes.POINTER(MgLevel_t)), ("block_level", ctypes.c_int32),
                 ("ncoarse", ctypes.c_int32), ("coarse_idx", _P), ("coarse_inv", _P), ("omega", ctypes.c_float),
-                ("scale", ctypes.c_float)]
+                ("scale", ctypes.c_float), ("cluster_top", ctypes.c_int32)]
 
 
 MG_BLOCK_SMEM = 226 * 1024   # dynamic shared memory of the one-CTA coarse solve
 MG_FLOATS_PER_NODE = 3       # b, x, y in shared memory (the operator moves there too when all 7 fit)
+MG_CLUSTER_TOP = 0           # largest level given to the one-cluster coarse solve (0: the one-CTA solve)
 MG_BLOCK_TOP = 1280          # largest level given to the one-CTA solve (one SM's issue rate bounds it)
 
 
@@ -266,11 +267,13 @@ class PoissonSolver:
         self._stencil = st
         self._pcg_work = D.empty(int(_declare().oec_pcg_work_bytes(st.nx, st.ny)), torch.uint8)
 
-    def _mg_setup(self, omega=0.8, scale=1.0, bottom=100, block_top=None):
+    def _mg_setup(self, omega=0.8, scale=1.0, bottom=100, block_top=None, cluster_top=None):
         """Aggregation multigrid hierarchy (oec_mg_t) on the scaled f32
         operator, down to at most `bottom` nodes, whose inside block is
         inverted densely (f64 on the host, stored in f32); levels of at most
-        `block_top` nodes (default MG_BLOCK_TOP) go to the one-CTA solve.  The
+        `block_top` nodes (default MG_BLOCK_TOP) go to the one-CTA solve, or
+        with `cluster_top` > 0 (default MG_CLUSTER_TOP) the levels from the
+        first one of at most `cluster_top` nodes go to the one-cluster solve.  The
         operators are shared with sibling solvers; the work vectors are this
         solver's.  The host copy of every level (ex, ey, leak, inside, nx, ny)
         is kept under "host"."""
@@ -306,7 +309,8 @@ class PoissonSolver:
             ops.append(t)
         shared = {"ops": ops, "cidx": D.to_device(idx.astype(np.int32), torch.int32),
                   "cinv": D.to_device(np.linalg.inv(M).astype(np.float32), torch.float32),
-                  "block_level": block, "omega": omega, "scale": scale, "host": lv}
+                  "block_level": block, "omega": omega, "scale": scale, "host": lv,
+                  "cluster_top": MG_CLUSTER_TOP if cluster_top is None else int(cluster_top)}
         self._mg = self._mg_state(shared)
         return self._mg
 
@@ -321,7 +325,7 @@ class PoissonSolver:
                                    D.ptr(o["dinv"]), D.ptr(o["inside"]), D.ptr(w["b"]), D.ptr(w["x"]),
                                    D.ptr(w["y"]))
         mg = Mg_t(len(ops), levels, shared["block_level"], shared["cidx"].shape[0], D.ptr(shared["cidx"]),
-                  D.ptr(shared["cinv"]), shared["omega"], shared["scale"])
+                  D.ptr(shared["cinv"]), shared["omega"], shared["scale"], shared.get("cluster_top", 0))
         keep = [dict(o, **w) for o, w in zip(ops, work)]
         return {"c": mg, "levels": levels, "work": work, "shared": shared, "keep": keep, "nlevels": len(ops),
                 "block_level": shared["block_level"], "host": shared["host"]}

@@ -48,28 +48,55 @@ def _rel(a, b):
     return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-300))
 
 
+KERNELS = ["mma.sync", "tcgen05"]
+
+
 @pytest.mark.gpu
-def test_forward_matches_oracle(gpu):
+@pytest.mark.parametrize("kernel", KERNELS)
+@pytest.mark.parametrize("shape", [(38, 45), (130, 257), (1026, 1026)])
+def test_forward_matches_oracle(gpu, kernel, shape):
+    """Forward pass through either tensor-core convolution kernel against the
+    oracle, from a 38x45 grid to the production grid (1026^2 nodes: every
+    level of the U-Net has several 128-pixel tiles per row and ragged
+    tails)."""
     import torch
     from openecloud_b200 import device as D
     from openecloud_b200.cnn import PoissonCNN
-    inside, x, t, w = _case()
-    net = PoissonCNN(inside.shape[1], inside.shape[0], inside, weights=w, training=False)
+    inside, x, t, w = _case(*shape)
+    net = PoissonCNN(inside.shape[1], inside.shape[0], inside, weights=w, training=False, conv_kernel=kernel)
     z = D.to_numpy(net.forward(D.to_device(x.reshape(-1), torch.float32))).reshape(inside.shape)
+    assert net.wait_timeouts() == 0
     zo, _ = cnn_oracle.forward(w, x, inside, bf=True)
     assert _rel(z, zo) <= 1e-2, _rel(z, zo)  # bf16 rounding-boundary flips, 7 layers
     assert np.all(z[~inside] == 0.0)
 
 
 @pytest.mark.gpu
+def test_tensor_core_kernels_agree(gpu):
+    """The tcgen05 and mma.sync kernels compute the same sums in f32 (in
+    another order): the forward passes agree far inside the bf16 rounding of
+    the activations."""
+    import torch
+    from openecloud_b200 import device as D
+    from openecloud_b200.cnn import PoissonCNN
+    inside, x, t, w = _case(514, 514, seed=3)
+    xd = D.to_device(x.reshape(-1), torch.float32)
+    z = {k: D.to_numpy(PoissonCNN(514, 514, inside, weights=w, training=False, conv_kernel=k).forward(xd))
+         for k in KERNELS}
+    assert _rel(z["tcgen05"], z["mma.sync"]) <= 2e-2
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", KERNELS)
 @pytest.mark.parametrize("shape", [(38, 45), (70, 130)])
-def test_gradients_match_oracle(gpu, shape):
+def test_gradients_match_oracle(gpu, shape, kernel):
     import torch
     from openecloud_b200 import device as D
     from openecloud_b200.cnn import PoissonCNN
     inside, x, t, w = _case(*shape, seed=2)
-    net = PoissonCNN(shape[1], shape[0], inside, weights=w)
+    net = PoissonCNN(shape[1], shape[0], inside, weights=w, conv_kernel=kernel)
     loss, g, z = net.loss_and_grad(D.to_device(x.reshape(-1), torch.float32), D.to_device(t.reshape(-1), torch.float32))
+    assert net.wait_timeouts() == 0
     lo, go, zo = cnn_oracle.loss_and_grad(w, x, t, inside, bf=True)
     assert abs(loss - lo) <= 1e-3 * lo
     g = D.to_numpy(g).astype(np.float64)

@@ -216,11 +216,14 @@ def test_pcg_warm_start_and_fallback(gpu):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("cluster_top", [0, 4000, 1 << 30])
 @pytest.mark.parametrize("name", ["rect_24x20", "ellipse_40x24", "circle_128"])
-def test_mg_vcycle_matches_oracle(gpu, name):
+def test_mg_vcycle_matches_oracle(gpu, name, cluster_top):
     """oec_mg_apply (f32) equals the float64 restatement of the V-cycle on the
-    device's own f32 level weights (the small grids run every level in the
-    one-CTA solve, the 128 circle its finest level in the tiled kernels)."""
+    device's own f32 level weights.  cluster_top 0: the small grids run every
+    level in the one-CTA solve, the 128 circle its finest level in the tiled
+    kernels; 4000: the coarse levels in the one-cluster solve; 2^30: every
+    level in the one-cluster solve."""
     import ctypes
     import torch
     from openecloud_b200 import device as D
@@ -228,7 +231,7 @@ def test_mg_vcycle_matches_oracle(gpu, name):
     from oracle.mg_oracle import vcycle
     z = golden(f"grid_{name}.npz")
     ps = PoissonSolver(_grid(z), method="pcg", precond="mg")
-    mg = ps._mg_setup()
+    mg = ps._mg_setup(cluster_top=cluster_top)
     host = mg["host"]
     dinv = [D.to_numpy(k["dinv"]).astype(np.float64) for k in mg["keep"]]
     assert mg["nlevels"] >= 2 and host[-1][4] * host[-1][5] <= 100
@@ -247,17 +250,24 @@ def test_mg_vcycle_matches_oracle(gpu, name):
 @pytest.mark.gpu
 def test_mg_pcg_iterations(gpu):
     """One V-cycle per iteration cuts the iteration count of the 128x128
-    circle by well over 5x against Jacobi, to the same 1e-8 residual."""
+    circle by well over 5x against Jacobi, to the same 1e-8 residual; the
+    V-cycle in one CTA (cluster_top 0) and wholly in one cluster (its CG dot
+    products included) take the same iterations and solution."""
     from openecloud_b200.poissonSolver import PoissonSolver
     z = golden("grid_circle_128.npz")
     q = z["poisson_q"]
-    its = {}
-    for pc in ("jacobi", "mg"):
+    its, phis = {}, {}
+    for pc, ct in (("jacobi", None), ("mg", 0), ("mg", 1 << 30)):
         ps = PoissonSolver(_grid(z), method="pcg", precond=pc, pcgTol=1e-8, pcgMaxIter=20000)
+        if ct is not None:
+            ps._mg_setup(cluster_top=ct)
         ps.solve(q)
         assert ps.lastStats.converged == 1 and ps.nFallbacks == 0
-        its[pc] = ps.lastStats.iterations
-    assert its["mg"] * 5 < its["jacobi"], its
+        its[(pc, ct)] = ps.lastStats.iterations
+        phis[(pc, ct)] = ps.getPhi()
+    assert its[("mg", 0)] * 5 < its[("jacobi", None)], its
+    assert abs(its[("mg", 0)] - its[("mg", 1 << 30)]) <= 1, its
+    assert rel_err(phis[("mg", 0)], phis[("mg", 1 << 30)]) <= 1e-7
 
 
 @pytest.mark.gpu
@@ -348,8 +358,8 @@ def test_pcg_synchronous_entry_point(gpu):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("top", [1280, 9000])
-def test_mg_vcycle_large_block_matches_tiled(gpu, top):
+@pytest.mark.parametrize("top,cluster_top", [(1280, 0), (9000, 0), (1280, 40000), (1280, 150000)])
+def test_mg_vcycle_large_block_matches_tiled(gpu, top, cluster_top):
     """On the 512x512 ellipse (45 x 18 mm), a V-cycle whose one-CTA part
     starts at a larger level (129 x 65 nodes and coarser: the operator read
     from global memory, 3 floats per node in shared memory) equals the
@@ -361,7 +371,7 @@ def test_mg_vcycle_large_block_matches_tiled(gpu, top):
     from openecloud_b200.poissonSolver import PoissonSolver, _declare
     from oracle.mg_oracle import vcycle
     ps = PoissonSolver(Grid(512, 512, 0.09, 0.036, 1), method="pcg", precond="mg")
-    mg = ps._mg_setup(block_top=top)
+    mg = ps._mg_setup(block_top=top, cluster_top=cluster_top)
     host = mg["host"]
     sizes = [h[4] * h[5] for h in host]
     block = mg["c"].block_level
