@@ -604,13 +604,13 @@ typedef struct oec_cnn {
     const uint8_t *inside;  /* [nx*ny] */
     void *w16;              /* bf16 parameters, oec_cnn_num_params() of them */
     void *act;              /* workspace of oec_cnn_act_bytes(nx, ny, training) bytes */
-    int32_t conv_kernel;    /* 3x3 convolutions with 16..64 input channels: OEC_CNN_CONV_MMA_SYNC
-                               (warp-level mma.sync m16n8k16) or OEC_CNN_CONV_TCGEN05 (tcgen05.mma
-                               issued by one thread, f32 accumulators in tensor memory) */
+    int32_t conv_kernel;    /* 3x3 convolutions with 16..64 input channels: OEC_CNN_CONV_TCGEN05 (0,
+                               tcgen05.mma issued by one thread, f32 accumulators in tensor memory)
+                               or OEC_CNN_CONV_MMA_SYNC (warp-level mma.sync m16n8k16) */
 } oec_cnn_t;
 
-#define OEC_CNN_CONV_MMA_SYNC 0
-#define OEC_CNN_CONV_TCGEN05 1
+#define OEC_CNN_CONV_TCGEN05 0
+#define OEC_CNN_CONV_MMA_SYNC 1
 
 int32_t oec_cnn_num_params(void);
 /* offsets[9]: start of each layer's weights in the flat parameter vector

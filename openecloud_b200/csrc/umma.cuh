@@ -138,8 +138,11 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
 // out[y][x][co] = sum_{ty,tx,ci} in[y+ty-1][x+tx-1][ci] * w[co][(ty*3+tx)*CI + ci]
 // (zero outside the image), bf16 in and out, f32 accumulation.  Each CTA
 // walks its tiles (blockIdx.x, + gridDim.x, ...) as a two-stage pipeline:
-// it stages tile k's halo and issues its MMAs into accumulator k % 2, then
-// writes tile k-1 out of the other accumulator while the tensor cores work.
+// it starts the asynchronous copies of tile k's halo into buffer k % 2,
+// writes tile k-1 out of the other accumulator while they fly, then issues
+// tile k's MMAs into accumulator k % 2.  Several CTAs share an SM (as many
+// as its shared memory holds), so one CTA's copies overlap another's MMAs
+// and epilogue.
 template <int CI, int CO>
 __global__ void __launch_bounds__(kThreads, 1)
     k_conv3(int H, int W, const __nv_bfloat16 *__restrict__ in, const __nv_bfloat16 *__restrict__ wgt,
@@ -180,19 +183,24 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint32_t phase0 = 0u, phase1 = 0u;  // parity of the next completion of bar[0], bar[1]
     bool ok = true;
 
-    // halo rows y-1..y+1, pixels x0-1..x0+kM of tile `tile` into buffer b: row (r, c8, px)
+    // halo rows y-1..y+1, pixels x0-1..x0+kM of tile `tile` into buffer b: row (r, c8, px),
+    // by asynchronous 16-byte copies (zeros stored directly outside the image)
     auto stage = [&](int tile, int b) {
         const int y = tile / tiles_x, x0 = (tile % tiles_x) * kM;
         unsigned char *dst = sA + b * L::kA;
         for (int i = tid; i < 3 * C8 * kHalo; i += kThreads) {
             const int px = i % kHalo, c8 = (i / kHalo) % C8, r = i / (kHalo * C8);
             const int yy = y + r - 1, xx = x0 + px - 1;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
             if (yy >= 0 && yy < H && xx >= 0 && xx < W)
-                v = *reinterpret_cast<const uint4 *>(in + ((size_t)yy * W + xx) * CI + c8 * 8);
-            *reinterpret_cast<uint4 *>(dst + (size_t)i * 16) = v;
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst + (size_t)i * 16)),
+                             "l"(in + ((size_t)yy * W + xx) * CI + c8 * 8)
+                             : "memory");
+            else
+                *reinterpret_cast<uint4 *>(dst + (size_t)i * 16) = make_uint4(0u, 0u, 0u, 0u);
         }
+        asm volatile("cp.async.commit_group;" ::: "memory");
     };
+    auto staged = [&]() { asm volatile("cp.async.wait_group 0;" ::: "memory"); };
     // MMAs of the tile staged in buffer b into accumulator b, committed to bar[b]
     auto issue = [&](int b) {
         if (tid == 0) {
@@ -239,6 +247,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 
     if (mine > 0) {
         stage(blockIdx.x, 0);
+        staged();
         fence_async_smem();
         __syncthreads();
         fence_after_sync();
@@ -247,16 +256,17 @@ __global__ void __launch_bounds__(kThreads, 1)
     for (int k = 1; k < mine; ++k) {  // the same trip count in every thread
         const int b = k & 1;
         // buffer and accumulator b last served tile k-2, whose MMAs this
-        // thread saw complete and whose accumulator every warp has read
+        // thread saw complete and whose accumulator every warp has read;
+        // tile k's copies fly while tile k-1 is written out
         stage(blockIdx.x + k * gridDim.x, b);
+        epilogue(blockIdx.x + (k - 1) * gridDim.x, b ^ 1);
+        staged();
         fence_async_smem();
         fence_before_sync();
         ok = __syncthreads_and(ok);
         fence_after_sync();
         if (!ok) break;
         issue(b);
-        epilogue(blockIdx.x + (k - 1) * gridDim.x, b ^ 1);
-        fence_before_sync();
     }
     if (mine > 0 && ok) epilogue(blockIdx.x + (mine - 1) * gridDim.x, (mine - 1) & 1);
     fence_before_sync();

@@ -187,11 +187,14 @@ def test_learned_correction_on_the_production_chamber(gpu):
     correction of the extrapolated warm start, on another production run
     (1024x1024 ellipse 45 x 18 mm, 2.2e6 electrons, 8.33 T, merging every 10
     steps; seed 2000): over 40 steps after 20 warm-up ones, the multigrid-PCG
-    solve at 1e-8 starts from a smaller residual and needs fewer iterations
-    than from the extrapolation alone, with no LU fallback.  This is what the
-    trained network gains over the method without it; per step it costs one
-    forward pass (0.4 ms at 1026^2), more than the iterations it saves (the
-    passage times are in the benchmark)."""
+    solve at 1e-8 needs fewer iterations than from the extrapolation alone
+    (measured 15.6 against 16.3 per solve), converges every time and never
+    falls back to LU.  The corrected start has the LARGER initial residual
+    (about 7x): the bf16 noise of the network's output sits in the highest
+    spatial frequencies, which A amplifies and the first V-cycle removes,
+    while the smooth error that costs CG its iterations is smaller.  Per step
+    the correction costs one forward pass (0.3 ms at 1026^2), more than the
+    iterations it saves (the passage times are in the benchmark)."""
     import os
     from openecloud_b200.buildup import Buildup
     from openecloud_b200.cnn import PoissonCNN
@@ -217,8 +220,9 @@ def test_learned_correction_on_the_production_chamber(gpu):
             r0.append(st.rel_residual0)
             it.append(st.iterations)
         assert ps.nFallbacks == fb0
-        stats[ws] = (float(np.mean(r0)), float(np.mean(it)))
-    print(f"production chamber, MG-PCG to 1e-8 (mean initial residual, iterations): extrapolation "
+        if ps.cnn is not None:
+            assert ps.cnn.wait_timeouts() == 0
+        stats[ws] = (float(np.median(r0)), float(np.mean(it)))
+    print(f"production chamber, MG-PCG to 1e-8 (median initial residual, mean iterations): extrapolation "
           f"{stats['extrapolate']}, with the learned correction {stats['extrapolate+cnn']}")
-    assert stats["extrapolate+cnn"][0] < stats["extrapolate"][0]
-    assert stats["extrapolate+cnn"][1] <= stats["extrapolate"][1]
+    assert stats["extrapolate+cnn"][1] < stats["extrapolate"][1]
