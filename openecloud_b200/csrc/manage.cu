@@ -28,7 +28,11 @@
 namespace oec {
 namespace {
 
-constexpr int kTile = 1024;  // elements per sort tile (one CTA)
+constexpr int kSortThreads = 256;                      // threads per sort CTA (8 warps)
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kPerLane = 16;                            // keys per thread
+constexpr int kTile = kSortThreads * kPerLane;          // keys per sort tile (one CTA): 4096
+constexpr int kWarpKeys = 32 * kPerLane;                // a warp's consecutive keys in the tile
 
 __device__ __forceinline__ int blk_scan(int v, int *tot, int *sh) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -58,16 +62,29 @@ __device__ __forceinline__ int blk_scan(int v, int *tot, int *sh) {
 
 // ----------------------------------------------------------- radix sort
 
-__global__ void k_digit_hist(const uint32_t *__restrict__ keys, const int32_t *n_p, int shift, int ntiles,
-                             int *__restrict__ hist) {
-    __shared__ int h[256];
-    int n = *n_p;
-    for (int d = threadIdx.x; d < 256; d += blockDim.x) h[d] = 0;
+// Digit counts of one tile (kTile keys): per-warp counters in shared memory
+// (fewer same-address conflicts), summed per digit at the end; written
+// digit-major, hist[d * ntiles + tile].
+__global__ void __launch_bounds__(kSortThreads) k_digit_hist(const uint32_t *__restrict__ keys, const int32_t *n_p,
+                                                             int shift, int ntiles, int *__restrict__ hist) {
+    __shared__ int h[kSortWarps][256];
+    const int n = *n_p;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int d = threadIdx.x; d < kSortWarps * 256; d += kSortThreads) (&h[0][0])[d] = 0;
     __syncthreads();
-    int i = blockIdx.x * kTile + threadIdx.x;
-    if (i < n) atomicAdd(&h[(keys[i] >> shift) & 255u], 1);
+    const int64_t base = (int64_t)blockIdx.x * kTile + w * kWarpKeys + lane;
+#pragma unroll 4
+    for (int r = 0; r < kPerLane; ++r) {
+        const int64_t i = base + r * 32;
+        if (i < n) atomicAdd(&h[w][(keys[i] >> shift) & 255u], 1);
+    }
     __syncthreads();
-    for (int d = threadIdx.x; d < 256; d += blockDim.x) hist[d * ntiles + blockIdx.x] = h[d];
+    for (int d = threadIdx.x; d < 256; d += kSortThreads) {
+        int c = 0;
+#pragma unroll
+        for (int k = 0; k < kSortWarps; ++k) c += h[k][d];
+        hist[d * ntiles + blockIdx.x] = c;
+    }
 }
 
 // exclusive scan of `len` ints in one CTA (len <= 1024 * chunks)
@@ -103,51 +120,67 @@ __global__ void k_scan_add_tiles(int *a, int len, const int *partial) {
     if (i < len) a[i] += partial[blockIdx.x];
 }
 
-// Stable scatter of one tile (kTile elements, one per thread) by the digit
-// at `shift`: a thread's place among the equal digits of its warp comes
-// from a match over the warp (the lanes below it with the same digit); the
-// counts of every (digit, warp) pair, scanned digit-major, give each warp's
-// start inside its digit, so the order is (digit, warp, lane) = stable.
-__global__ void __launch_bounds__(kTile) k_scatter(const uint32_t *__restrict__ keys,
-                                                   const int32_t *__restrict__ vals, const int32_t *n_p, int shift,
-                                                   int ntiles, const int *__restrict__ offs,
-                                                   uint32_t *__restrict__ okeys, int32_t *__restrict__ ovals) {
-    constexpr int kWarps = kTile / 32;
-    __shared__ int sh[32];
-    __shared__ int cnt[256 * kWarps];  // (digit, warp), digit-major
+// Stable scatter of one tile (kTile keys) by the digit at `shift`.  Warp w
+// owns the tile's keys w*512 .. w*512+511 and walks them in 16 rounds of 32
+// consecutive keys (coalesced loads); a key's place among the equal digits
+// of its warp is the warp's running count of that digit (shared memory, one
+// counter row per warp) plus the lanes below it in the round with the same
+// digit (a warp match).  After the rounds the counts of the lower warps give
+// each warp's start inside the tile's run of a digit, and the scanned tile
+// histogram the run's start in the output, so the order is (digit, tile,
+// warp, round, lane) = stable.
+__global__ void __launch_bounds__(kSortThreads) k_scatter(const uint32_t *__restrict__ keys,
+                                                          const int32_t *__restrict__ vals, const int32_t *n_p,
+                                                          int shift, int ntiles, const int *__restrict__ offs,
+                                                          uint32_t *__restrict__ okeys, int32_t *__restrict__ ovals) {
+    __shared__ int cnt[kSortWarps][256];  // running digit counts, then each warp's start in a digit's run
     const int n = *n_p;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int i = blockIdx.x * kTile + threadIdx.x;
-    const bool valid = i < n;
-    const uint32_t k = valid ? keys[i] : 0u;
-    const int32_t v = valid ? vals[i] : 0;
-    const int d = valid ? (int)((k >> shift) & 255u) : 256;  // 256: no element
-    for (int e = threadIdx.x; e < 256 * kWarps; e += kTile) cnt[e] = 0;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    for (int e = threadIdx.x; e < kSortWarps * 256; e += kSortThreads) (&cnt[0][0])[e] = 0;
     __syncthreads();
-    const unsigned peers = __match_any_sync(kFullMask, d);
-    const int rank = __popc(peers & ((1u << lane) - 1u));
-    if (valid && rank == 0) cnt[d * kWarps + w] = __popc(peers);
-    __syncthreads();
-    // exclusive scan of the 256 * kWarps counts, kWarps per thread... 8 each
-    constexpr int kPerThread = 256 * kWarps / kTile;
-    int local[kPerThread], sum = 0;
+    const int64_t base = (int64_t)blockIdx.x * kTile + w * kWarpKeys + lane;
+    uint32_t k[kPerLane];
+    int32_t v[kPerLane];
+    int dr[kPerLane];  // digit << 16 | rank among the warp's equal digits, -1: no key
 #pragma unroll
-    for (int j = 0; j < kPerThread; ++j) {
-        local[j] = cnt[threadIdx.x * kPerThread + j];
-        sum += local[j];
+    for (int r = 0; r < kPerLane; ++r) {
+        const int64_t i = base + r * 32;
+        const bool valid = i < n;
+        k[r] = valid ? keys[i] : 0u;
+        v[r] = valid ? vals[i] : 0;
     }
-    int base = blk_scan(sum, nullptr, sh);
 #pragma unroll
-    for (int j = 0; j < kPerThread; ++j) {
-        cnt[threadIdx.x * kPerThread + j] = base;
-        base += local[j];
+    for (int r = 0; r < kPerLane; ++r) {
+        const bool valid = base + r * 32 < n;
+        const int d = valid ? (int)((k[r] >> shift) & 255u) : 256;
+        const unsigned peers = __match_any_sync(kFullMask, d);
+        int rank = 0;
+        if (valid) rank = cnt[w][d] + __popc(peers & below);
+        __syncwarp();
+        if (valid && (peers & below) == 0) cnt[w][d] += __popc(peers);
+        __syncwarp();
+        dr[r] = valid ? (d << 16 | rank) : -1;
     }
     __syncthreads();
-    if (valid) {
-        const int local_pos = cnt[d * kWarps + w] + rank;
-        const int dst = offs[d * ntiles + blockIdx.x] + (local_pos - cnt[d * kWarps]);
-        okeys[dst] = k;
-        ovals[dst] = v;
+    // each warp's start inside the tile's run of digit d: the counts of the lower warps
+    for (int d = threadIdx.x; d < 256; d += kSortThreads) {
+        int run = 0;
+#pragma unroll
+        for (int q = 0; q < kSortWarps; ++q) {
+            const int c = cnt[q][d];
+            cnt[q][d] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kPerLane; ++r) {
+        if (dr[r] < 0) continue;
+        const int d = dr[r] >> 16, rank = dr[r] & 0xffff;
+        const int dst = offs[d * ntiles + blockIdx.x] + cnt[w][d] + rank;
+        okeys[dst] = k[r];
+        ovals[dst] = v[r];
     }
 }
 
@@ -495,11 +528,11 @@ static int radix_sort(uint32_t *keys, int32_t *vals, uint32_t *k2, int32_t *v2, 
     // block totals after the histogram and its 256-byte slack
     int *partial = reinterpret_cast<int *>(reinterpret_cast<char *>(hist) + 4 * (int64_t)len + 256);
     for (int shift = 0; shift < bits; shift += 8) {
-        k_digit_hist<<<ntiles, kTile, 0, s>>>(keys, n_dev, shift, ntiles, hist);
+        k_digit_hist<<<ntiles, kSortThreads, 0, s>>>(keys, n_dev, shift, ntiles, hist);
         k_scan_tiles<<<nb, 1024, 0, s>>>(hist, len, partial);
         k_scan_serial_chunks<<<1, 1024, 0, s>>>(partial, nb);
         k_scan_add_tiles<<<nb, 1024, 0, s>>>(hist, len, partial);
-        k_scatter<<<ntiles, kTile, 0, s>>>(keys, vals, n_dev, shift, ntiles, hist, k2, v2);
+        k_scatter<<<ntiles, kSortThreads, 0, s>>>(keys, vals, n_dev, shift, ntiles, hist, k2, v2);
         uint32_t *tk = keys;
         keys = k2;
         k2 = tk;

@@ -51,6 +51,35 @@ def test_sort_by_column(gpu, col):
         assert np.all(np.diff(after[:, col]) >= 0)
 
 
+@pytest.mark.parametrize("n", [4096, 300_001])
+def test_sort_by_column_many_tiles_stable(gpu, n):
+    """The radix sort over many 4096-key tiles (and a ragged last tile):
+    sorting by cell keeps equal cells in their previous order, exactly as a
+    stable host argsort; sorting by weight orders the FP32 weights."""
+    from openecloud_b200.grid import Grid
+    from openecloud_b200.particles import Particles
+    rng = np.random.default_rng(n)
+    g = Grid(64, 48, 0.04, 0.03, 0)
+    pd = np.empty((n, 6))
+    pd[:, 0] = rng.uniform(-0.0199, 0.0199, n)
+    pd[:, 1] = rng.uniform(-0.0149, 0.0149, n)
+    pd[:, 2:5] = rng.normal(0.0, 1e6, (n, 3))
+    pd[:, 5] = rng.choice([0.5, 1.0, 1.5, 2.0], n)  # many equal weights
+    P = Particles("electrons", "variableWeight")
+    P.setParticleData(pd)
+    P._bind(g)
+    before = P.getParticleData()
+    cells_before = P.soa()["cell"][:n].cpu().numpy()
+    P.sortByColumn(6)
+    after = P.getParticleData()
+    assert np.array_equal(after, before[np.argsort(cells_before, kind="stable")])
+    w_before = P.getParticleData()[:, 5].copy()
+    rows = P.getParticleData()
+    P.sortByColumn(5)
+    after = P.getParticleData()
+    assert np.array_equal(after, rows[np.argsort(w_before.astype(np.float32), kind="stable")])
+
+
 @pytest.mark.parametrize("target", [3100, 5200, 800])
 def test_global_random(gpu, target):
     from openecloud_b200.particleManagement import globalRandom
