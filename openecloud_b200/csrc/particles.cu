@@ -315,6 +315,31 @@ struct NodeWindow {
         add_at(key, ix, iy, q, rho, nx);
     }
 
+    // x to window entry e, |x| < 2^41 known
+    __device__ __forceinline__ void add_entry_in_range(int e, long long x) {
+        unsigned *w = v + e * (kWinPlanes * kWinCopies) + (threadIdx.x & (kWinCopies - 1));
+        atomicAdd(w, (unsigned)x & 0x1fffffu);
+        atomicAdd(w + kWinCopies, (unsigned)(int)(x >> 21));
+    }
+
+    // add_at for the corner charges of a particle whose whole charge is
+    // below 2^40 in magnitude, so every corner is below 2^41 and the range
+    // test is made once per particle by the caller instead of per corner
+    // (3 % of the fused step on the 2^24-electron microbench)
+    __device__ __forceinline__ void add_at_in_range(int key, int ix, int iy, const double q[4],
+                                                    unsigned long long *rho, int nx) {
+        const int rx = ix - ox, ry = iy - oy;
+        if ((unsigned)rx < (unsigned)(kWinCols - 1) && (unsigned)ry < (unsigned)(kWinRows - 1)) {
+            const int e = ry * kWinCols + rx;
+            add_entry_in_range(e, __double2ll_rn(q[0]));
+            add_entry_in_range(e + 1, __double2ll_rn(q[1]));
+            add_entry_in_range(e + kWinCols, __double2ll_rn(q[2]));
+            add_entry_in_range(e + kWinCols + 1, __double2ll_rn(q[3]));
+        } else {
+            add_node4(rho, key, nx, q);
+        }
+    }
+
     // the same for cell key = ix + iy * nx with its column and row known
     __device__ __forceinline__ void add_at(int key, int ix, int iy, const double q[4], unsigned long long *rho,
                                            int nx) {
@@ -542,7 +567,11 @@ __device__ __forceinline__ void process_group(const FusedArgs &a, int q, int n, 
                 if (DEP && !out && OEC_IN_BOUNDS(cc[j], a.ncell)) {
                     double v[4];
                     corner_charges(ww[j], dox, doy, wscale, v);
-                    nw.add_at(cc[j], ix, iy, v, a.rho, a.nx);
+                    // |corner| <= |rint(w * wscale)| + 2 (the fourth corner takes the rounding rest)
+                    if (fabs((double)ww[j] * wscale) < 0x1p40)
+                        nw.add_at_in_range(cc[j], ix, iy, v, a.rho, a.nx);
+                    else
+                        nw.add_at(cc[j], ix, iy, v, a.rho, a.nx);
                 }
             }
         }
