@@ -126,10 +126,12 @@ class Buildup:
         self.hist_w = D.zeros(self._table_len, torch.float64)
         self.hist_n = D.zeros(self._table_len, torch.int32)
         self.scratch = D.zeros(256, torch.float64)  # oec_history's partial sums
-        # absorbed rows per step: by default bounded by a fraction of the
-        # capacity; a step that absorbs more is counted on the device
-        # (status n_rows_dropped) and run() raises
-        self.abs_cap = int(abs_cap) if abs_cap is not None else max(4096, cap // 8)
+        # absorbed rows per step: by default the store's capacity, so that no
+        # step can absorb more (a bunch can sweep the whole cloud into the
+        # wall at once); a smaller abs_cap saves memory, and a step that
+        # absorbs more than it is counted on the device (status
+        # n_rows_dropped) and run() raises
+        self.abs_cap = int(abs_cap) if abs_cap is not None else max(4096, cap)
         self.bd.ensure_buffers(self.abs_cap)
         self.em.ensure_buffers(self.bd._rows.shape[0])
         self.P._deposit_buffers(self.grid)

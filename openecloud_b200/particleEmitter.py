@@ -73,8 +73,12 @@ class FurmanEmitter:
         if self._work is None or self._cap_abs < cap_abs:
             self._cap_abs = int(cap_abs)
             self._work = D.empty(int(L.oec_furman_work_bytes(self._cap_abs)), torch.uint8)
-            self._out = D.zeros((self.m * self._cap_abs + 1, 6), torch.float64)
             self._n_out = D.zeros(1, torch.int32)
+        # output rows: secondaries beyond the store's capacity could not be
+        # added anyway (the emission and oec_add_remove count them as dropped)
+        out_rows = min(self.m * self._cap_abs, max(self.particlesObj._cap, 1)) + 1
+        if self._out is None or self._out.shape[0] < out_rows:
+            self._out = D.zeros((out_rows, 6), torch.float64)
 
     def _launch(self, cap, step, step_dev, replay):
         """One emission over the boundary's first min(n_abs, cap) rows into
@@ -176,8 +180,12 @@ class SecElecEmitter:
         if self._work is None or self._cap_abs < cap_abs:
             self._cap_abs = int(cap_abs)
             self._work = D.empty(int(L.oec_secelec_work_bytes(self._cap_abs)), torch.uint8)
-            self._out = D.zeros((self.m * self._cap_abs + 1, 6), torch.float64)
             self._n_out = D.zeros(1, torch.int32)
+        # output rows: secondaries beyond the store's capacity could not be
+        # added anyway (the emission and oec_add_remove count them as dropped)
+        out_rows = min(self.m * self._cap_abs, max(self.particlesObj._cap, 1)) + 1
+        if self._out is None or self._out.shape[0] < out_rows:
+            self._out = D.zeros((out_rows, 6), torch.float64)
 
     def _launch(self, cap, step, step_dev, replay):
         bd = self.particleBoundaryObj
