@@ -133,6 +133,8 @@ class Buildup:
         # n_rows_dropped) and run() raises
         self.abs_cap = int(abs_cap) if abs_cap is not None else max(4096, cap)
         self.bd.ensure_buffers(self.abs_cap)
+        # the store does not grow inside a run: at most `cap` secondaries can be added per step
+        self.em.out_cap = cap
         self.em.ensure_buffers(self.bd._rows.shape[0])
         self.P._deposit_buffers(self.grid)
         self.P._hole_buffers()

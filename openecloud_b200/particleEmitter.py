@@ -58,6 +58,7 @@ class FurmanEmitter:
         self._work = None
         self._out = None
         self._n_out = None
+        self.out_cap = None  # bound on the output rows (None: m per absorbed row)
         self.secondaryCount = 0
 
     def setEHat0(self, value):
@@ -74,9 +75,13 @@ class FurmanEmitter:
             self._cap_abs = int(cap_abs)
             self._work = D.empty(int(L.oec_furman_work_bytes(self._cap_abs)), torch.uint8)
             self._n_out = D.zeros(1, torch.int32)
-        # output rows: secondaries beyond the store's capacity could not be
-        # added anyway (the emission and oec_add_remove count them as dropped)
-        out_rows = min(self.m * self._cap_abs, max(self.particlesObj._cap, 1)) + 1
+        # output rows: m per absorbed row, or at most `out_cap` when the caller
+        # fixes it (a buildup whose store cannot grow: secondaries beyond its
+        # capacity could not be added, and the emission counts them dropped)
+        out_rows = self.m * self._cap_abs
+        if self.out_cap is not None:
+            out_rows = min(out_rows, max(int(self.out_cap), 1))
+        out_rows += 1
         if self._out is None or self._out.shape[0] < out_rows:
             self._out = D.zeros((out_rows, 6), torch.float64)
 
@@ -152,6 +157,7 @@ class SecElecEmitter:
         self._work = None
         self._out = None
         self._n_out = None
+        self.out_cap = None  # bound on the output rows (None: m per absorbed row)
         self.secondaryCount = 0
         self.stainlessMod(seyMax, reflec)
 
@@ -181,9 +187,13 @@ class SecElecEmitter:
             self._cap_abs = int(cap_abs)
             self._work = D.empty(int(L.oec_secelec_work_bytes(self._cap_abs)), torch.uint8)
             self._n_out = D.zeros(1, torch.int32)
-        # output rows: secondaries beyond the store's capacity could not be
-        # added anyway (the emission and oec_add_remove count them as dropped)
-        out_rows = min(self.m * self._cap_abs, max(self.particlesObj._cap, 1)) + 1
+        # output rows: m per absorbed row, or at most `out_cap` when the caller
+        # fixes it (a buildup whose store cannot grow: secondaries beyond its
+        # capacity could not be added, and the emission counts them dropped)
+        out_rows = self.m * self._cap_abs
+        if self.out_cap is not None:
+            out_rows = min(out_rows, max(int(self.out_cap), 1))
+        out_rows += 1
         if self._out is None or self._out.shape[0] < out_rows:
             self._out = D.zeros((out_rows, 6), torch.float64)
 
