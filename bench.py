@@ -49,7 +49,7 @@ METRIC = "particle-steps/s"
 # (ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none -k regex:k_push_gather -s 3 -c 1):
 # the particle part scaled by 2 to 2^24 electrons, the grid part (E table and
 # deposit grid, 12.7 MB) added once.
-NCU_TRAFFIC_PER_LAUNCH = {1 << 24: 768996672}
+NCU_TRAFFIC_PER_LAUNCH = {1 << 24: 773544608}
 
 
 # ------------------------------------------------------------- workload

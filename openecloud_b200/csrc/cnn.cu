@@ -161,37 +161,51 @@ __global__ void __launch_bounds__(128) k_conv3_mma(int H, int W, const bf16 *__r
 }
 
 // Input convolution, one channel in (f32), 16 out (bf16); inside mask on x.
-__global__ void k_conv3_in1(int H, int W, const float *__restrict__ x, const uint8_t *__restrict__ inside,
-                            const bf16 *__restrict__ wgt, bf16 *__restrict__ out, bf16 *__restrict__ x16) {
+// A CTA computes a 32 x 8 pixel tile from a 34 x 10 halo tile of the masked,
+// bf16-rounded input staged once in shared memory (each input pixel is read
+// from memory once per tile instead of once per tap).
+constexpr int kIn1TX = 32, kIn1TY = 8;
+__global__ void __launch_bounds__(kIn1TX *kIn1TY)
+    k_conv3_in1(int H, int W, const float *__restrict__ x, const uint8_t *__restrict__ inside,
+                const bf16 *__restrict__ wgt, bf16 *__restrict__ out, bf16 *__restrict__ x16) {
     __shared__ float sw[16 * 9];
-    for (int i = threadIdx.x; i < 16 * 9; i += blockDim.x) sw[i] = __bfloat162float(wgt[i]);
+    __shared__ float tile[kIn1TY + 2][kIn1TX + 2];
+    const int tid = threadIdx.x;
+    for (int i = tid; i < 16 * 9; i += blockDim.x) sw[i] = __bfloat162float(wgt[i]);
+    const int x0 = blockIdx.x * kIn1TX, y0 = blockIdx.y * kIn1TY;
+    for (int e = tid; e < (kIn1TY + 2) * (kIn1TX + 2); e += blockDim.x) {
+        const int ty = e / (kIn1TX + 2), tx = e - ty * (kIn1TX + 2);
+        const int yy = y0 + ty - 1, xs = x0 + tx - 1;
+        float v = 0.f;
+        if (yy >= 0 && yy < H && xs >= 0 && xs < W) {
+            const int q = yy * W + xs;
+            if (inside[q]) v = __bfloat162float(__float2bfloat16_rn(x[q]));
+        }
+        tile[ty][tx] = v;
+    }
     __syncthreads();
-    const int n = H * W;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-        const int y = p / W, xx = p % W;
-        float v[9];
+    const int lx = tid % kIn1TX, ly = tid / kIn1TX;
+    const int xx = x0 + lx, y = y0 + ly;
+    if (xx >= W || y >= H) return;
+    const int p = y * W + xx;
+    float v[9];
+#pragma unroll
+    for (int tap = 0; tap < 9; ++tap) v[tap] = tile[ly + tap / 3][lx + tap % 3];
+    x16[p] = __float2bfloat16_rn(inside[p] ? x[p] : 0.f);
+    uint32_t o[8];
+#pragma unroll
+    for (int c = 0; c < 16; c += 2) {
+        float s0 = 0.f, s1 = 0.f;
 #pragma unroll
         for (int tap = 0; tap < 9; ++tap) {
-            const int yy = y + tap / 3 - 1, xs = xx + tap % 3 - 1;
-            const int q = yy * W + xs;
-            v[tap] = (yy >= 0 && yy < H && xs >= 0 && xs < W && inside[q]) ? __bfloat162float(__float2bfloat16_rn(x[q])) : 0.f;
+            s0 = fmaf(v[tap], sw[c * 9 + tap], s0);
+            s1 = fmaf(v[tap], sw[(c + 1) * 9 + tap], s1);
         }
-        x16[p] = __float2bfloat16_rn(inside[p] ? x[p] : 0.f);
-        uint32_t o[8];
-#pragma unroll
-        for (int c = 0; c < 16; c += 2) {
-            float s0 = 0.f, s1 = 0.f;
-#pragma unroll
-            for (int tap = 0; tap < 9; ++tap) {
-                s0 = fmaf(v[tap], sw[c * 9 + tap], s0);
-                s1 = fmaf(v[tap], sw[(c + 1) * 9 + tap], s1);
-            }
-            o[c / 2] = pack_bf16(s0, s1);
-        }
-        uint4 *dst = reinterpret_cast<uint4 *>(out + (size_t)p * 16);
-        dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
-        dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
+        o[c / 2] = pack_bf16(s0, s1);
     }
+    uint4 *dst = reinterpret_cast<uint4 *>(out + (size_t)p * 16);
+    dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
+    dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
 }
 
 // 2x2 average of the children (out-of-range children count as zero).
@@ -730,7 +744,8 @@ int forward(const oec_cnn_t *c, const float *x, Buffers &b, cudaStream_t s) {
     const bf16 *w = reinterpret_cast<const bf16 *>(c->w16);
     const size_t n0 = (size_t)c->nx * c->ny;
     OEC_CUDA_TRY(cudaMemsetAsync(b.err, 0, sizeof(int), s));
-    k_conv3_in1<<<grid_for(n0), 256, 0, s>>>(L[0].h, L[0].w, x, c->inside, w + conv_offset(0), b.e0, b.x16);
+    k_conv3_in1<<<dim3((L[0].w + kIn1TX - 1) / kIn1TX, (L[0].h + kIn1TY - 1) / kIn1TY), kIn1TX * kIn1TY, 0, s>>>(
+        L[0].h, L[0].w, x, c->inside, w + conv_offset(0), b.e0, b.x16);
     OEC_LAUNCH_CHECK();
     pool<16>(L[0], L[1], b.e0, b.p1, s);
     int rc = conv3<16, 32>(c->conv_kernel, L[1], b.p1, w + conv_offset(1), b.e1, b.err, s);

@@ -19,6 +19,7 @@
 // be captured into a larger graph (a buildup time step).
 #include <math.h>
 #include <stdint.h>
+#include <stdlib.h>
 
 #include <cooperative_groups.h>
 
@@ -125,6 +126,7 @@ struct Ctl {
     double inv_rnorm;          // 1 / ||r|| of the current refinement
     double coef;               // scale32 * ||r||: weight of the f32 correction
     double best;               // best inner residual so far (stagnation window)
+    double pq_prev;            // p.Ap of the previous inner iteration (k_cg_step)
     int slot, it, total, refine, best_at, ticket;
     oec_pcg_stats_t stats;     // stats of the synchronous entry point
 };
@@ -338,6 +340,97 @@ __global__ void __launch_bounds__(kT) k_direction32(int G, const float *__restri
     }
     c->slot = slot ^ 1;
     if (more) cudaGraphSetConditional(h_inner, 1);
+}
+
+// The inner iteration's CG part when the preconditioner runs first in the
+// loop body (the multigrid V-cycle: z = M r with acc.rzn += r.z and
+// acc.zq += z.q of the previous direction's q): the new direction
+// p = z + beta p (beta = -(z.q)/(p.q), flexible CG; p = z in the first
+// iteration), q = A p with p.q, the step alpha = (r.z)/(p.q) into d and r
+// with |r|^2, and the convergence check of k_direction32 -- one cooperative
+// launch with grid-wide barriers between the parts instead of three launches
+// (all CTAs resident).  A non-positive or non-finite curvature leaves d and r
+// unchanged and ends the loop as a breakdown.
+__global__ void __launch_bounds__(kT) k_cg_step(int nx, int G, const float *__restrict__ ex,
+                                                const float *__restrict__ ey, const uint8_t *__restrict__ in,
+                                                const float *__restrict__ z, float *__restrict__ p,
+                                                float *__restrict__ q, float *__restrict__ d, float *__restrict__ r,
+                                                Acc *acc, Ctl *c, int max_iter, oec_pcg_stats_t *stats,
+                                                cudaGraphConditionalHandle h_inner) {
+    cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+    Acc *a = acc + c->slot;
+    const int it = c->it;
+    if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h_inner, 0);
+    float beta = 0.f;
+    if (it > 0) {
+        double b = -a->zq / c->pq_prev;
+        beta = isfinite(b) ? (float)b : 0.f;
+    }
+    const int stride = gridDim.x * kT;
+    for (int i = blockIdx.x * kT + threadIdx.x; i < G; i += stride) p[i] = it > 0 ? fmaf(beta, p[i], z[i]) : z[i];
+    grid.sync();
+    double pq = 0.0;
+    for (int i = blockIdx.x * kT + threadIdx.x; i < G; i += stride) {
+        float v = 0.0f;
+        if (in[i]) {
+            v = apply_at(i, nx, ex, ey, p);
+            pq += (double)p[i] * (double)v;
+        }
+        q[i] = v;
+    }
+    cta_add(pq, &a->pq);
+    grid.sync();
+    const double pqs = a->pq, rz = a->rzn;
+    double rr = 0.0;
+    if (pqs > 0.0 && isfinite(rz)) {
+        const float alpha = (float)(rz / pqs);
+        for (int i = blockIdx.x * kT + threadIdx.x; i < G; i += stride) {
+            d[i] = fmaf(alpha, p[i], d[i]);
+            const float ri = fmaf(-alpha, q[i], r[i]);
+            r[i] = ri;
+            rr += (double)ri * (double)ri;
+        }
+        cta_add(rr, &a->rr);
+    } else if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a->rr = __longlong_as_double(0x7ff8000000000000LL);
+    }
+    grid.sync();
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const double rrs = a->rr;
+    const int it1 = it + 1, total = c->total + 1;
+    c->it = it1;
+    c->total = total;
+    stats->iterations = total;
+    bool more = total < max_iter;
+    if (!isfinite(rrs)) {
+        stats->breakdown = 1;
+        more = false;
+    } else {
+        const double rel_in = sqrt(rrs);
+        if (rel_in <= c->inner_tol) {
+            more = false;
+        } else if (rel_in < 0.9 * c->best) {
+            c->best = rel_in;
+            c->best_at = it1;
+        } else if (it1 - c->best_at >= 1024) {
+            more = false;
+        }
+    }
+    // the next V-cycle accumulates its dot products from zero
+    c->pq_prev = pqs;
+    a->pq = a->rr = a->rzn = a->zq = 0.0;
+    if (more) cudaGraphSetConditional(h_inner, 1);
+}
+
+// Start of the inner loop of k_cg_step: d = 0, q = 0, arms the loop (r was
+// scaled by k_scale32).
+__global__ void __launch_bounds__(kT) k_init_cg(int G, float *__restrict__ d, float *__restrict__ q,
+                                                cudaGraphConditionalHandle h_inner) {
+    for (int i = blockIdx.x * kT + threadIdx.x; i < G; i += gridDim.x * kT) {
+        d[i] = 0.0f;
+        q[i] = 0.0f;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h_inner, 1);
 }
 
 // phi += coef d on the inside nodes.
@@ -1307,12 +1400,42 @@ int capture_graph(cudaStream_t s, cudaGraph_t *g) {
 }
 
 // Records the whole solve into the capture of s.
+// Grids up to this many nodes take the cooperative k_cg_step: its grid
+// barriers cost less than three launches only while the passes are short
+// (measured cold solves, 15 / 23 iterations: 128^2 circle 0.826 -> 0.778 ms,
+// 1024^2 ellipse 2.83 -> 3.24 ms).
+constexpr int kCgStepMaxNodes = 1 << 17;
+
+// Grid of the cooperative k_cg_step for G nodes on this device: at most two
+// resident CTAs per SM, so that the whole grid fits beside other work (0:
+// a grid above kCgStepMaxNodes, cooperative launches unavailable, or
+// OEC_CG_STEP=0 in the environment; the iteration then runs as three
+// kernels).
+int cg_step_grid(int G) {
+    if (G > kCgStepMaxNodes) return 0;
+    static std::atomic<int> cached[kMaxDevices];
+    const int per_sm = per_device_cached(cached, [] {
+        const char *e = getenv("OEC_CG_STEP");
+        if (e && e[0] == '0') return 0;
+        int dev = 0, coop = 0, b = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cg_step, kT, 0) != cudaSuccess)
+            b = 0;
+        cudaGetLastError();
+        return b < 2 ? b : 2;
+    });
+    if (per_sm <= 0) return 0;
+    return persistent_grid((G + kT - 1) / kT, per_sm);
+}
+
 int build_solve(const SolveArgs &a, cudaStream_t s) {
     const oec_stencil_t *st = a.st;
     const int nx = st->nx, G = st->nx * st->ny;
     const int grid = persistent_grid((G + kT - 1) / kT, 4);
     const int pc = a.precond;
     const bool external = pc == OEC_PRECOND_CNN || pc == OEC_PRECOND_MG;
+    const int coop_grid = pc == OEC_PRECOND_MG ? cg_step_grid(G) : 0;
     Work w = carve(a.work, G);
     OEC_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(Ctl), s));
     OEC_CUDA_TRY(cudaMemsetAsync(a.stats, 0, sizeof(oec_pcg_stats_t), s));
@@ -1334,34 +1457,52 @@ int build_solve(const SolveArgs &a, cudaStream_t s) {
             BodyCapture c2;
             OEC_TRY(c2.begin(1, b_work));
             OEC_CUDA_TRY(cudaGraphConditionalHandleCreate(&h_inner, b_work, 0, 0));
-            if (external) {
+            if (coop_grid > 0) {
+                // multigrid: V-cycle first in the loop body, then the CG step
                 k_scale32<<<grid, kT, 0, c2.s>>>(G, w.r64, w.ctl, w.r);
+                k_init_cg<<<grid, kT, 0, c2.s>>>(G, w.d, w.q, h_inner);
                 OEC_LAUNCH_CHECK();
-                OEC_TRY(external_apply(pc, a.ctx, w.r, w.z, nullptr, nullptr, nullptr, c2.s));
-            }
-            k_init32<<<grid, kT, 0, c2.s>>>(G, w.r64, w.ctl, st->dinv32, pc, external ? 1 : 0, w.r, w.z, w.p, w.d,
-                                            w.acc, h_inner);
-            OEC_LAUNCH_CHECK();
-            OEC_TRY(add_conditional(c2.s, h_inner, cudaGraphCondTypeWhile, &b_inner));
-            {
+                OEC_TRY(add_conditional(c2.s, h_inner, cudaGraphCondTypeWhile, &b_inner));
                 BodyCapture c3;
                 OEC_TRY(c3.begin(2, b_inner));
-                k_apply32<<<grid, kT, 0, c3.s>>>(nx, G, st->ex32, st->ey32, st->inside, w.p, w.q, w.acc, w.ctl,
-                                                 h_inner);
-                OEC_CUDA_TRY(launch_overlapped(k_update32, dim3(grid), dim3(kT), 0, c3.s, G, st->dinv32, pc, w.p, w.q,
-                                               w.d, w.r, w.z, w.acc, w.ctl));
-                OEC_LAUNCH_CHECK();
-                if (pc == OEC_PRECOND_MG) {
-                    OEC_TRY(external_apply(pc, a.ctx, w.r, w.z, w.q, w.acc, w.ctl, c3.s));
-                } else if (external) {
-                    OEC_TRY(external_apply(pc, a.ctx, w.r, w.zn, nullptr, nullptr, nullptr, c3.s));
-                    OEC_CUDA_TRY(launch_overlapped(k_zdots32, dim3(grid), dim3(kT), 0, c3.s, G, w.r, w.zn, w.q, w.z,
-                                                   w.acc, w.ctl));
-                }
-                OEC_CUDA_TRY(launch_overlapped(k_direction32, dim3(grid), dim3(kT), 0, c3.s, G, w.z, w.p, w.acc, w.ctl,
-                                               a.max_iter, a.stats, h_inner));
-                OEC_LAUNCH_CHECK();
+                OEC_TRY(external_apply(pc, a.ctx, w.r, w.z, w.q, w.acc, w.ctl, c3.s));
+                int max_iter = a.max_iter;
+                void *args[] = {(void *)&nx, (void *)&G, (void *)&st->ex32, (void *)&st->ey32, (void *)&st->inside,
+                                (void *)&w.z, (void *)&w.p, (void *)&w.q, (void *)&w.d, (void *)&w.r,
+                                (void *)&w.acc, (void *)&w.ctl, (void *)&max_iter, (void *)&a.stats,
+                                (void *)&h_inner};
+                OEC_CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_cg_step, dim3(coop_grid), dim3(kT), args, 0, c3.s));
                 OEC_TRY(c3.end());
+            } else {
+                if (external) {
+                    k_scale32<<<grid, kT, 0, c2.s>>>(G, w.r64, w.ctl, w.r);
+                    OEC_LAUNCH_CHECK();
+                    OEC_TRY(external_apply(pc, a.ctx, w.r, w.z, nullptr, nullptr, nullptr, c2.s));
+                }
+                k_init32<<<grid, kT, 0, c2.s>>>(G, w.r64, w.ctl, st->dinv32, pc, external ? 1 : 0, w.r, w.z, w.p, w.d,
+                                                w.acc, h_inner);
+                OEC_LAUNCH_CHECK();
+                OEC_TRY(add_conditional(c2.s, h_inner, cudaGraphCondTypeWhile, &b_inner));
+                {
+                    BodyCapture c3;
+                    OEC_TRY(c3.begin(2, b_inner));
+                    k_apply32<<<grid, kT, 0, c3.s>>>(nx, G, st->ex32, st->ey32, st->inside, w.p, w.q, w.acc, w.ctl,
+                                                     h_inner);
+                    OEC_CUDA_TRY(launch_overlapped(k_update32, dim3(grid), dim3(kT), 0, c3.s, G, st->dinv32, pc, w.p, w.q,
+                                                   w.d, w.r, w.z, w.acc, w.ctl));
+                    OEC_LAUNCH_CHECK();
+                    if (pc == OEC_PRECOND_MG) {
+                        OEC_TRY(external_apply(pc, a.ctx, w.r, w.z, w.q, w.acc, w.ctl, c3.s));
+                    } else if (external) {
+                        OEC_TRY(external_apply(pc, a.ctx, w.r, w.zn, nullptr, nullptr, nullptr, c3.s));
+                        OEC_CUDA_TRY(launch_overlapped(k_zdots32, dim3(grid), dim3(kT), 0, c3.s, G, w.r, w.zn, w.q, w.z,
+                                                       w.acc, w.ctl));
+                    }
+                    OEC_CUDA_TRY(launch_overlapped(k_direction32, dim3(grid), dim3(kT), 0, c3.s, G, w.z, w.p, w.acc, w.ctl,
+                                                   a.max_iter, a.stats, h_inner));
+                    OEC_LAUNCH_CHECK();
+                    OEC_TRY(c3.end());
+                }
             }
             k_accumulate64<<<grid, kT, 0, c2.s>>>(G, w.ctl, w.d, st->inside, a.phi);
             OEC_LAUNCH_CHECK();

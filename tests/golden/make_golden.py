@@ -370,6 +370,28 @@ if __name__ == "__main__" and "--buildup" in sys.argv:
     buildup_golden()
 
 
+def _buildup20_seed(s):
+    c, w = reference_buildup(200 + s, 20 * 2500)
+    return c[::250], w[::250]
+
+
+def buildup20_golden(n_seeds=8):
+    """The c1 configuration over its full 20 bunch passages (50,000 steps),
+    8 seeds of the reference's random stream (one process each), sampled
+    every 250 steps."""
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(n_seeds) as pool:
+        res = pool.map(_buildup20_seed, range(n_seeds))
+    out = {"count": np.array([r[0] for r in res]), "weight": np.array([r[1] for r in res]), "every": np.array(250)}
+    path = os.path.join(HERE, "buildup_c1_20.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "final line density", out["weight"][:, -1])
+
+
+if __name__ == "__main__" and "--buildup20" in sys.argv:
+    buildup20_golden()
+
+
 def beam_golden():
     grid, particles, particleBoundary, poissonSolver, randomGen = _import_reference()
     from beam import LHCBeam, LHCBeamEndless

@@ -3,9 +3,10 @@
 Configuration: 128x128 circular chamber R = 20 mm, 1e4 initial electrons,
 endless bunch train (sigma_r 2 mm, sigma_t 0.25 ns, 1.1e11 protons, 25 ns),
 copper SEY with delta_max 1.6 and E_max 300 eV, roulette cap 1e5 every 50
-steps, dt = 1e-11 s, one bunch passage (2500 steps).  The golden file holds
-the reference's line density for 8 seeds; the ensemble mean of 8 device runs
-must stay within twice the reference's seed-to-seed spread (floor 0.2%).
+steps, dt = 1e-11 s, one bunch passage (2500 steps) and the configuration's
+full 20 passages (50,000 steps).  The golden files hold the reference's line
+density for 8 seeds each; the ensemble mean of 8 device runs must stay within
+twice the reference's seed-to-seed spread (floor 0.2%).
 """
 import numpy as np
 import pytest
@@ -36,6 +37,39 @@ def test_buildup_line_density_within_reference_spread(gpu):
     assert not bad.any(), (np.nonzero(bad)[0][:10], m_gpu[bad][:5], m_ref[bad][:5])
     # the cloud builds up over the passage as in the reference
     assert m_gpu[-1] / m_gpu[0] > 1.2
+
+
+def test_buildup_twenty_passages_within_reference_spread(gpu):
+    """The c1 configuration over its full 20 bunch passages (50,000 steps)
+    against 8 seeds of the reference (tests/golden/buildup_c1_20.npz, made
+    by make_golden.py --buildup20), sampled every 250 steps: the ensemble
+    mean of 8 device runs stays within twice the reference's seed-to-seed
+    spread at every sample (floor 0.2 %), and the saturated line density
+    (mean over the last five passages) within twice the spread of that
+    mean across the reference's seeds."""
+    from openecloud_b200.buildup import Buildup
+    z = golden("buildup_c1_20.npz")
+    every = int(z["every"])
+    ref = z["weight"]
+    n_steps = (ref.shape[1] - 1) * every
+    runs = []
+    for s in range(8):
+        b = Buildup(seed=3000 + s, n_steps_table=n_steps + 1)
+        b.run(n_steps)
+        n, w = b.history()
+        st = b.status()
+        assert st["n_capacity_drop"] == 0 and st["n_nonfinite"] == 0
+        runs.append(w[::every])
+    gpu_w = np.array(runs)
+    m_ref, s_ref = ref.mean(0), ref.std(0, ddof=1)
+    m_gpu = gpu_w.mean(0)
+    bad = np.abs(m_gpu - m_ref) > 2 * np.maximum(s_ref, 0.002 * m_ref)
+    assert not bad.any(), (np.nonzero(bad)[0][:10], m_gpu[bad][:5], m_ref[bad][:5])
+    tail = ref.shape[1] - 1 - 5 * 2500 // every
+    sat_ref, sat_gpu = ref[:, tail:].mean(1), gpu_w[:, tail:].mean(1)
+    print(f"saturated line density: device {sat_gpu.mean():.4e} +- {sat_gpu.std(ddof=1):.2e}, "
+          f"reference {sat_ref.mean():.4e} +- {sat_ref.std(ddof=1):.2e}")
+    assert abs(sat_gpu.mean() - sat_ref.mean()) <= 2 * max(sat_ref.std(ddof=1), 0.002 * sat_ref.mean())
 
 
 def test_buildup_step_graph_with_multigrid_pcg(gpu):
