@@ -600,19 +600,27 @@ def component_rooflines(peak, n=1 << 24, n_merge=2_000_000):
     n_sec = int(D.to_numpy(em._n_out)[0])
     out.append(line("Furman emission (oec_furman_emit)", (48 + 16) * n_abs + 48 * n_sec, ms,
                     f"row and normal per absorbed particle, row per secondary ({n_sec})"))
-    moved = min(n_abs, n_sec) + abs(n_sec - n_abs)
+    # the placement rule the refill takes (decided on the device the same
+    # way) and the kept particles it moves through the scratch store
+    holes = D.to_numpy(bd._index[:min(n_abs, bd._index.shape[0])])
+    if n_sec < n_abs:
+        rule, moved = "in place, fewer rows than holes", n - int(holes[n_sec]) - (n_abs - n_sec)
+    elif n - n_abs + n_sec > int(P._array_len.item()):
+        rule, moved = "new array", n - n_abs
+    else:
+        rule, moved = "in place, rows fill the holes", 0
     # the refill changes the store, so it is timed once; a small store's
     # refill loads its kernels first
     W = Particles("electrons", "variableWeight")
     W.setParticleData(pd[:4096])
     W._bind(g)
     W.addAndRemoveParticles(pd[:16], (np.arange(4096) % 3 != 0).astype(np.uint16))
-    ms = timed(lambda: _lib.call("oec_add_remove", cg, cp, P._mask.data_ptr(), bd._index.data_ptr(),
+    ms = timed(lambda: _lib.call("oec_add_remove", cg, cp, P.c_scratch(), P._mask.data_ptr(), bd._index.data_ptr(),
                                  bd._n_abs.data_ptr(), bd._index.shape[0], em._out.data_ptr(), em._n_out.data_ptr(),
-                                 em._out.shape[0], rho, wsc, P._scan_scratch.data_ptr(), st, sh), reps=1, warm=0)
-    out.append(line("refill and compaction (oec_add_remove)", n / 8 + (48 + 28 + 16) * n_sec + 56 * moved, ms,
-                    "absorbed bits; per secondary a row read, 7 fields written, its deposit; per tail move "
-                    "28 B read + 28 B written"))
+                                 em._out.shape[0], P._array_len.data_ptr(), rho, wsc, st, sh), reps=1, warm=0)
+    out.append(line("refill and compaction (oec_add_remove)", n / 8 + (48 + 28 + 16) * n_sec + 112 * moved, ms,
+                    f"{rule}: absorbed bits; per secondary a row read, 7 fields written, its deposit; per moved "
+                    f"particle ({moved}) 28 B read and 28 B written twice (through the scratch store)"))
     # (d) cell-binned merge of a 2e6-electron store over 10 % toward a 1.8e6 target
     pm, _, _ = workload(n_merge, seed=9)
     pm[:, 5] = np.random.default_rng(9).uniform(0.2, 2.0, n_merge) * 1e3

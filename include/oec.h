@@ -55,7 +55,9 @@ typedef struct oec_status {
     int32_t n_rows_dropped;    /* absorbed particles beyond the absorbed-row capacity of
                                   oec_wall_interaction: removed without a wall row, so
                                   they emit no secondaries (the caller must grow the rows) */
-    int32_t reserved[4];
+    int32_t n_emit_skipped;    /* absorbed rows with a non-finite position, energy or wall
+                                  normal: they emit no secondaries */
+    int32_t reserved[3];
 } oec_status_t;
 
 /* ------------------------------------------------------------ types */
@@ -239,22 +241,38 @@ int oec_save_absorbed(const oec_grid_t *grid, const oec_particles_t *p, const in
  * (particleBoundary.pyx:99-221 rect, :252-297 ellipse, :373-481 cut-cell):
  * moves each row back onto the wall, writes (n_abs, 2) inward normals;
  * dt is the last push step (used by the cut-cell back step).  Rows whose
- * cut-cell intersection is not found are counted in status->n_not_found. */
+ * intersection is not found are counted in status->n_not_found: for the
+ * rectangle a zero velocity across the crossed side (the point is clamped
+ * onto the wall), for the ellipse a back step that misses the wall (the
+ * point is projected radially onto it); the reference's formulas give NaN
+ * there. */
 int oec_wall_interaction(const oec_grid_t *grid, const oec_boundary_t *boundary, double dt, double *rows_dev,
                          const int32_t *n_abs_dev, int32_t cap, double *normals_dev, oec_status_t *status_dev,
                          void *stream);
 
 /* addAndRemoveParticles (particles.pyx:94-121): remove the absorbed
- * particles (holes = ascending absorbed indices) and insert the added rows:
- * added row k fills hole k, extra rows are appended after the old count,
- * and remaining holes are filled by the kept particles of the tail region
- * in order.  Optionally deposits the added rows into rho_fix (same scale as
- * oec_push_gather).  scratch_dev: >= 1 int32.  The count is updated on the
- * device; rows beyond the capacity are dropped and counted. */
-int oec_add_remove(const oec_grid_t *grid, oec_particles_t *p, const uint32_t *absorbed_mask_dev,
-                   const int32_t *holes_dev, const int32_t *n_holes_dev, int32_t holes_cap,
-                   const double *add_rows_dev, const int32_t *n_add_dev, int32_t add_cap, int64_t *rho_fix_dev,
-                   const double *wscale_dev, int32_t *scratch_dev, oec_status_t *status_dev, void *stream);
+ * particles (holes = ascending absorbed indices) and insert the added rows,
+ * leaving every particle in the slot the reference's array gives it:
+ *  - no added rows (_removeParticles, :254-269): each hole below the new
+ *    count, in ascending order, takes the last kept particle of the tail;
+ *  - new count above *array_len_dev (_addAndRemoveParticlesNewArray,
+ *    :109-116, :201-219): the kept particles in order, then the added rows;
+ *    *array_len_dev becomes int(1.1 * new count);
+ *  - otherwise (_addAndRemoveParticles, :222-252): added row k fills hole k;
+ *    extra rows are appended after the old count, or, with fewer rows than
+ *    holes, the kept particles after the last filled hole shift down in
+ *    order.
+ * array_len_dev: the row count of the reference's particle array (set to
+ * the count wherever the reference calls setParticleData), or NULL to never
+ * take the new-array rule.  tmp: a scratch store of at least p's capacity
+ * (count pointer unused).  Optionally deposits the added rows into rho_fix
+ * (same scale as oec_push_gather).  The count is updated on the device;
+ * rows beyond the capacity are dropped and counted. */
+int oec_add_remove(const oec_grid_t *grid, oec_particles_t *p, oec_particles_t *tmp,
+                   const uint32_t *absorbed_mask_dev, const int32_t *holes_dev, const int32_t *n_holes_dev,
+                   int32_t holes_cap, const double *add_rows_dev, const int32_t *n_add_dev, int32_t add_cap,
+                   int32_t *array_len_dev, int64_t *rho_fix_dev, const double *wscale_dev, oec_status_t *status_dev,
+                   void *stream);
 
 /* keepParticles u16 array (1 = keep) -> absorbed bitmask (1 = remove). */
 int oec_mask_from_keep(const uint16_t *keep_dev, int64_t n, uint32_t *mask_dev, int64_t mask_words, void *stream);

@@ -43,7 +43,7 @@ class Boundary_t(ctypes.Structure):
 
 STATUS_FIELDS = ["n_absorbed", "n_secondaries", "n_nonfinite", "n_clipped", "n_not_found",
                  "n_capacity_drop", "deposit_overflow", "n_wait_timeout", "warn_derm", "warn_tsprime",
-                 "n_out_of_grid", "n_rows_dropped"]
+                 "n_out_of_grid", "n_rows_dropped", "n_emit_skipped"]
 STATUS_WORDS = 16
 
 _P = ctypes.c_void_p
@@ -77,7 +77,7 @@ SIGNATURES = {
     "oec_absorbed_index": [_PP, _P, _P, _I32, _P, _P, _P, _P],
     "oec_save_absorbed": [_PG, _PP, _P, _P, _I32, _P, _P],
     "oec_wall_interaction": [_PG, _PB, _D, _P, _P, _I32, _P, _P, _P],
-    "oec_add_remove": [_PG, _PP, _P, _P, _P, _I32, _P, _P, _I32, _P, _P, _P, _P, _P],
+    "oec_add_remove": [_PG, _PP, _PP, _P, _P, _P, _I32, _P, _P, _I32, _P, _P, _P, _P, _P],
     "oec_mask_from_keep": [_P, _I64, _P, _I64, _P],
     "oec_homo_load": [_PG, _PB, _PP, _I64, _D, _D, _I32, ctypes.c_uint64, _P, _P],
     "oec_sort_particles": [_PP, _PP, _I32, _P, _P],

@@ -138,6 +138,7 @@ class Buildup:
         self.em.ensure_buffers(self.bd._rows.shape[0])
         self.P._deposit_buffers(self.grid)
         self.P._hole_buffers()
+        self.P.c_scratch()  # allocated before any capture
         self._prepare_deposit()
         _lib.call("oec_history", self.P.c_particles(), self.step_dev.data_ptr(), self._table_len,
                   self.hist_w.data_ptr(), self.hist_n.data_ptr(), self.scratch.data_ptr(), D.stream())
@@ -187,9 +188,10 @@ class Buildup:
         _lib.call("oec_wall_interaction", cg, cb, self.dt, bd._rows.data_ptr(), bd._n_abs.data_ptr(), cap,
                   bd._normals.data_ptr(), P._status.data_ptr(), s)
         em._launch(cap, 0, self.step_dev, None)
-        _lib.call("oec_add_remove", cg, cp, P._mask.data_ptr(), bd._index.data_ptr(), bd._n_abs.data_ptr(),
-                  bd._index.shape[0], em._out.data_ptr(), em._n_out.data_ptr(), em._out.shape[0],
-                  P._rho_fix.data_ptr(), P._wscale.data_ptr(), P._scan_scratch.data_ptr(), P._status.data_ptr(), s)
+        _lib.call("oec_add_remove", cg, cp, P.c_scratch(), P._mask.data_ptr(), bd._index.data_ptr(),
+                  bd._n_abs.data_ptr(), bd._index.shape[0], em._out.data_ptr(), em._n_out.data_ptr(),
+                  em._out.shape[0], P._array_len.data_ptr(), P._rho_fix.data_ptr(), P._wscale.data_ptr(),
+                  P._status.data_ptr(), s)
         _lib.call("oec_step_advance", self.step_dev.data_ptr(), s)
         # state at the start of the next step, before its management
         # (example01_basic.py:56-57 records it there)
@@ -284,9 +286,10 @@ class Buildup:
         reallocation by management or sorting changes them) and the solver
         settings."""
         P, bd, em, ps = self.P, self.bd, self.em, self.ps
-        bufs = (P._mask, P._rho_fix, P._wscale, P._status, P._scan_scratch, bd._index, bd._rows, bd._normals,
+        bufs = (P._mask, P._rho_fix, P._wscale, P._status, P._array_len, bd._index, bd._rows, bd._normals,
                 bd._n_abs, bd._scratch, em._work, em._out, em._n_out, self.btab)
-        return (bytes(P.c_particles()), tuple(0 if t is None else t.data_ptr() for t in bufs), bytes(em.c_params()),
+        return (bytes(P.c_particles()), bytes(P.c_scratch()), tuple(0 if t is None else t.data_ptr() for t in bufs),
+                bytes(em.c_params()),
                 em.seed, ps.method, ps.precond, ps.warmStart, ps.pcgTol, ps.pcgMaxIter, id(ps.cnn))
 
     def _capture(self):
@@ -339,6 +342,7 @@ class Buildup:
         C.write_reference_outputs(directory, P.getParticleData(), hist_w[:-1], hist_n[:-1])
         store = {k: D.to_numpy(P.soa()[k][:n]) for k in C.STORE_FIELDS}
         arrays = {"rho_fix": D.to_numpy(P._rho_fix), "wscale": D.to_numpy(P._wscale),
+                  "array_len": D.to_numpy(P._array_len),
                   "status": D.to_numpy(P._status), "step": D.to_numpy(self.step_dev),
                   "hist_n": D.to_numpy(self.hist_n), "hist_w": D.to_numpy(self.hist_w),
                   "phi": D.to_numpy(ps.phi),
@@ -360,6 +364,10 @@ class Buildup:
         for k in C.STORE_FIELDS:
             P.soa()[k][:n].copy_(torch.from_numpy(store[k]))
         P._count.fill_(n)
+        if "array_len" in arrays:
+            P._array_len.copy_(torch.from_numpy(arrays["array_len"]))
+        else:
+            P._array_len.fill_(n)
         P._rho_fix.copy_(torch.from_numpy(arrays["rho_fix"]))
         P._wscale.copy_(torch.from_numpy(arrays["wscale"]))
         P._status.copy_(torch.from_numpy(arrays["status"]))

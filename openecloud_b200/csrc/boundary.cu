@@ -162,7 +162,7 @@ struct WallConst {
 };
 
 // AbsorbRectangular.calculateInteractionPoint + calculateNormalVectors.
-__device__ void wall_rect(const WallConst &c, double *r, double *nrm) {
+__device__ bool wall_rect(const WallConst &c, double *r, double *nrm) {
     const double hx = c.rect_hx, hy = c.rect_hy;
     int xs = 1, ys = 1;
     if (r[0] > hx) xs = 2; else if (r[0] < -hx) xs = 0;
@@ -185,26 +185,52 @@ __device__ void wall_rect(const WallConst &c, double *r, double *nrm) {
         else where = (tx > ty) ? 2 : 3;
         t = (tx > ty) ? tx : ty;
     }
-    r[0] = __dsub_rn(r[0], __dmul_rn(t, r[2]));
-    r[1] = __dsub_rn(r[1], __dmul_rn(t, r[3]));
+    bool found = true;
+    if (isfinite(t)) {
+        r[0] = __dsub_rn(r[0], __dmul_rn(t, r[2]));
+        r[1] = __dsub_rn(r[1], __dmul_rn(t, r[3]));
+    } else {
+        // no velocity across the crossed side (the back step divides by a
+        // zero component and the reference's point is NaN): the point is
+        // clamped onto the wall instead
+        r[0] = fmin(fmax(r[0], -hx), hx);
+        r[1] = fmin(fmax(r[1], -hy), hy);
+        found = false;
+    }
     nrm[0] = where == 0 ? 1. : (where == 1 ? -1. : 0.);
     nrm[1] = where == 2 ? 1. : (where == 3 ? -1. : 0.);
+    return found;
 }
 
 // AbsorbElliptical.calculateInteractionPoint + calculateNormalVectors.
-__device__ void wall_ellipse(const WallConst &c, double *r, double *nrm) {
+__device__ bool wall_ellipse(const WallConst &c, double *r, double *nrm) {
     const double ax = c.ell_ax, ay = c.ell_ay;
     double cc = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(r[0], r[0]), ax), __dmul_rn(__dmul_rn(r[1], r[1]), ay)), -1.);
     double b = __dadd_rn(__dmul_rn(__dmul_rn(r[0], r[2]), ax), __dmul_rn(__dmul_rn(r[1], r[3]), ay));
     double a = __dadd_rn(__dmul_rn(__dmul_rn(r[2], r[2]), ax), __dmul_rn(__dmul_rn(r[3], r[3]), ay));
-    double t = __ddiv_rn(__dsub_rn(b, __dsqrt_rn(__dsub_rn(__dmul_rn(b, b), __dmul_rn(a, cc)))), a);
-    r[0] = __dsub_rn(r[0], __dmul_rn(t, r[2]));
-    r[1] = __dsub_rn(r[1], __dmul_rn(t, r[3]));
+    const double disc = __dsub_rn(__dmul_rn(b, b), __dmul_rn(a, cc));
+    bool found = true;
+    if (disc >= 0. && a > 0.) {
+        double t = __ddiv_rn(__dsub_rn(b, __dsqrt_rn(disc)), a);
+        r[0] = __dsub_rn(r[0], __dmul_rn(t, r[2]));
+        r[1] = __dsub_rn(r[1], __dmul_rn(t, r[3]));
+    } else {
+        // the back step along the velocity misses the wall (or there is no
+        // transverse velocity) and the reference's point is NaN: the point
+        // is projected radially onto the wall instead
+        const double s = __dsqrt_rn(__dadd_rn(cc, 1.));
+        if (s > 0.) {
+            r[0] = __ddiv_rn(r[0], s);
+            r[1] = __ddiv_rn(r[1], s);
+        }
+        found = false;
+    }
     const double nx2 = c.ell_nx2, ny2 = c.ell_ny2, nx4 = c.ell_nx4, ny4 = c.ell_ny4;
     double inv = __ddiv_rn(1., __dsqrt_rn(__dadd_rn(__dmul_rn(__dmul_rn(r[0], r[0]), nx4),
                                                     __dmul_rn(__dmul_rn(r[1], r[1]), ny4))));
     nrm[0] = __dmul_rn(__dmul_rn(-r[0], nx2), inv);
     nrm[1] = __dmul_rn(__dmul_rn(-r[1], ny2), inv);
+    return found;
 }
 
 __device__ __forceinline__ int cell_of(const WallConst &c, double x, double y) {
@@ -269,17 +295,46 @@ __global__ void k_wall(WallConst c, double *__restrict__ rows, const int32_t *n_
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += gridDim.x * blockDim.x) {
         double *r = rows + 6 * (int64_t)i;
         double *nrm = normals + 2 * (int64_t)i;
+        bool found;
         if (c.kind == OEC_BOUNDARY_RECT)
-            wall_rect(c, r, nrm);
+            found = wall_rect(c, r, nrm);
         else if (c.kind == OEC_BOUNDARY_ELLIPSE)
-            wall_ellipse(c, r, nrm);
-        else if (!wall_cutcell(c, r, nrm, G))
-            ++missing;
+            found = wall_ellipse(c, r, nrm);
+        else
+            found = wall_cutcell(c, r, nrm, G);
+        if (!found) ++missing;
     }
     if (missing) atomicAdd(&status->n_not_found, missing);
 }
 
 // ------------------------------------------------------------- add/remove
+//
+// addAndRemoveParticles (particles.pyx:94-121) places the particles by one
+// of four rules, chosen from the counts (N old particles, A holes = removed
+// particles, S added rows, K = N - A kept, N_new = K + S):
+//  * remove only (S = 0, particles.pyx:254-269): each hole below N_new, in
+//    ascending order, takes the LAST kept particle not yet moved, so the
+//    kept particles of the tail [N_new, N) land in descending order;
+//  * a larger array (S > 0 and N_new above the row count of the reference's
+//    particle array, particles.pyx:109-116, :201-219): the kept particles in
+//    order, then the added rows; the array then holds int(1.1 N_new) rows;
+//  * in place with S >= A (particles.pyx:224-232, :245-252): added row k
+//    fills hole k, the rest are appended after N;
+//  * in place with S < A (particles.pyx:224-244): added row k fills hole k
+//    for k < S, then every kept particle after hole S-1 shifts down over the
+//    A - S holes left, in order.
+// The order matters beyond bookkeeping: the reference's Furman emission
+// reads the yields of the last absorbed particle of the store for every
+// single-secondary split (particleEmitter.pyx:245-246), so the same store
+// order gives the same physics.  The row count of the reference's array is
+// emulated in a device integer (array_len); without one the larger-array
+// rule is never taken.
+//
+// The two shifting rules move a region [r0, N) whose kept particles land at
+// r0 + rank; they go through a scratch store (gather, then scatter back),
+// since destinations overlap sources.  The remove-only rule moves tail
+// particles into holes below N_new, disjoint from the sources, directly.
+enum ArMode : int { kArNothing = 0, kArRemove = 1, kArFillAppend = 2, kArShift = 3, kArNewArray = 4 };
 
 __device__ __forceinline__ void copy_particle(oec_particles_t &p, int dst, int src) {
     p.cell[dst] = p.cell[src];
@@ -289,6 +344,16 @@ __device__ __forceinline__ void copy_particle(oec_particles_t &p, int dst, int s
     p.vy[dst] = p.vy[src];
     p.vz[dst] = p.vz[src];
     p.w[dst] = p.w[src];
+}
+
+__device__ __forceinline__ void copy_across(oec_particles_t &d, int dst, const oec_particles_t &s, int src) {
+    d.cell[dst] = s.cell[src];
+    d.ox[dst] = s.ox[src];
+    d.oy[dst] = s.oy[src];
+    d.vx[dst] = s.vx[src];
+    d.vy[dst] = s.vy[src];
+    d.vz[dst] = s.vz[src];
+    d.w[dst] = s.w[src];
 }
 
 // Row [x,y,vx,vy,vz,w] (f64) -> SoA slot k.
@@ -308,51 +373,20 @@ __device__ __forceinline__ void store_row(oec_particles_t &p, int k, const doubl
 
 struct AddArgs {
     oec_particles_t p;
+    oec_particles_t tmp;       // scratch store for the shifting rules
     const int32_t *holes;      // ascending absorbed indices
     const int32_t *n_holes;
     int holes_cap;
     const double *add_rows;    // (n_add, 6)
     const int32_t *n_add;
     int add_cap;
+    int32_t *array_len;        // emulated row count of the reference's array (optional)
     int nx, ny;
     double dxi, dyi, lxh, lyh;
     unsigned long long *rho;   // optional deposit of the added rows
     const double *wscale;
     oec_status_t *status;
-    int32_t *scratch;          // [0]: old count
 };
-
-// Place the added rows: k < holes -> hole k, else appended after the old count.
-__global__ void k_place_added(AddArgs a) {
-    const int N = *a.p.count;
-    const int A = min(*a.n_holes, a.holes_cap);
-    const int S = min(*a.n_add, a.add_cap);
-    if (blockIdx.x == 0 && threadIdx.x == 0) a.scratch[0] = N;
-    int dropped = 0;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += gridDim.x * blockDim.x) {
-        int dst = (k < A) ? a.holes[k] : N + (k - A);
-        if (dst >= a.p.capacity) {
-            ++dropped;
-            continue;
-        }
-        const double *r = a.add_rows + 6 * (int64_t)k;
-        store_row(a.p, dst, r, a.nx, a.ny, a.dxi, a.dyi, a.lxh, a.lyh);
-        if (a.rho && OEC_IN_BOUNDS(a.p.cell[dst] + a.nx + 1, a.nx * a.ny)) {
-            int c = a.p.cell[dst];
-            double q = (double)llrint((double)a.p.w[dst] * *a.wscale);
-            double gx = (double)a.p.ox[dst], gy = (double)a.p.oy[dst];
-            long long v0 = llrint(q * ((1.0 - gx) * (1.0 - gy)));
-            long long v1 = llrint(q * (gx * (1.0 - gy)));
-            long long v2 = llrint(q * ((1.0 - gx) * gy));
-            long long v3 = (long long)q - v0 - v1 - v2;
-            atomicAdd(a.rho + c, (unsigned long long)v0);
-            atomicAdd(a.rho + c + 1, (unsigned long long)v1);
-            atomicAdd(a.rho + c + a.nx, (unsigned long long)v2);
-            atomicAdd(a.rho + c + a.nx + 1, (unsigned long long)v3);
-        }
-    }
-    if (dropped) atomicAdd(&a.status->n_capacity_drop, dropped);
-}
 
 // First index in the ascending holes[0, n) that is >= v.
 __device__ __forceinline__ int holes_lower_bound(const int32_t *__restrict__ holes, int n, int v) {
@@ -365,45 +399,132 @@ __device__ __forceinline__ int holes_lower_bound(const int32_t *__restrict__ hol
     return lo;
 }
 
-// Fewer added rows than holes: the kept particles of the tail region
-// [N_new, N) move, in order, into the remaining holes below N_new
-// (particles.pyx:254-269 fills holes from the end the same way).  The rank
-// of a kept tail particle p is the count of kept positions in [N_new, p):
-// (p - N_new) minus the holes among them, which a CTA takes for its chunk's
+// The rule and the region of one call, computed alike by every thread of
+// every launch (the count changes only in the last launch).
+struct ArPlan {
+    int N, A, S, Nnew;
+    int mode;
+    int r0;     // start of the region whose kept particles move
+    int kept;   // kept particles in [r0, N)
+    int below;  // holes below r0
+};
+
+__device__ __forceinline__ ArPlan ar_plan(const AddArgs &a) {
+    ArPlan q;
+    q.N = *a.p.count;
+    q.A = min(*a.n_holes, a.holes_cap);
+    q.S = min(*a.n_add, a.add_cap);
+    const int K = q.N - q.A;
+    q.Nnew = K + q.S;
+    q.mode = kArFillAppend;
+    q.r0 = q.kept = q.below = 0;
+    if (q.S == 0) {
+        // the kept tail [N_new, N) holds as many particles as there are holes below N_new
+        q.mode = q.A == 0 ? kArNothing : kArRemove;
+        q.r0 = q.Nnew;
+        q.below = holes_lower_bound(a.holes, q.A, q.Nnew);
+        q.kept = q.below;
+    } else if (a.array_len && q.Nnew > *a.array_len) {
+        q.mode = kArNewArray;
+        q.kept = K;
+    } else if (q.S < q.A) {
+        q.mode = kArShift;
+        q.r0 = a.holes[q.S];  // the first hole left open: everything below it stays
+        q.below = q.S;
+        q.kept = q.N - q.r0 - (q.A - q.S);
+    }
+    return q;
+}
+
+// Added row k -> slot dst, with its deposit when rho is given.  Slots at or
+// beyond the capacity are dropped (counted by the caller).
+__device__ __forceinline__ bool place_row(AddArgs &a, int dst, int k) {
+    if (dst >= a.p.capacity) return false;
+    store_row(a.p, dst, a.add_rows + 6 * (int64_t)k, a.nx, a.ny, a.dxi, a.dyi, a.lxh, a.lyh);
+    if (a.rho && OEC_IN_BOUNDS(a.p.cell[dst] + a.nx + 1, a.nx * a.ny)) {
+        const int c = a.p.cell[dst];
+        const double q = (double)llrint((double)a.p.w[dst] * *a.wscale);
+        const double gx = (double)a.p.ox[dst], gy = (double)a.p.oy[dst];
+        const long long v0 = llrint(q * ((1.0 - gx) * (1.0 - gy)));
+        const long long v1 = llrint(q * (gx * (1.0 - gy)));
+        const long long v2 = llrint(q * ((1.0 - gx) * gy));
+        const long long v3 = (long long)q - v0 - v1 - v2;
+        atomicAdd(a.rho + c, (unsigned long long)v0);
+        atomicAdd(a.rho + c + 1, (unsigned long long)v1);
+        atomicAdd(a.rho + c + a.nx, (unsigned long long)v2);
+        atomicAdd(a.rho + c + a.nx + 1, (unsigned long long)v3);
+    }
+    return true;
+}
+
+// In-place rules: added row k fills hole k (k < A), the rest are appended
+// after the old count.  With S < A only holes are filled.
+__global__ void k_place_added(AddArgs a) {
+    const ArPlan q = ar_plan(a);
+    if (q.mode != kArFillAppend && q.mode != kArShift) return;
+    int dropped = 0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < q.S; k += gridDim.x * blockDim.x) {
+        const int dst = (k < q.A) ? a.holes[k] : q.N + (k - q.A);
+        if (!place_row(a, dst, k)) ++dropped;
+    }
+    if (dropped) atomicAdd(&a.status->n_capacity_drop, dropped);
+}
+
+// The kept particles of the region [r0, N), each with its rank among them:
+// (p - r0) minus the holes in [r0, p), which a CTA takes for its chunk's
 // start from the ascending holes array (one binary search) and within the
-// chunk from a scan of the absorbed bits, so the chunks move independently
-// (a merge of 2e6 electrons leaves a tail of ~2e5 positions).  Sources are
-// all >= N_new and destinations < N_new: no move overlaps another.
-__global__ void __launch_bounds__(1024) k_fill_holes(AddArgs a, const uint32_t *__restrict__ mask) {
+// chunk from a scan of the absorbed bits, so the chunks run independently.
+// Remove-only: rank r goes to hole kept-1-r (descending into ascending
+// holes, all below N_new <= r0).  Shifting rules: rank r goes to tmp[r].
+__global__ void __launch_bounds__(1024) k_region_gather(AddArgs a, const uint32_t *__restrict__ mask) {
     __shared__ int sh[32];
-    __shared__ int holes_before;  // holes in [N_new, chunk start)
-    const int N = a.scratch[0];
-    const int A = min(*a.n_holes, a.holes_cap);
-    const int S = min(*a.n_add, a.add_cap);
-    if (S >= A) return;
-    const int Nnew = N - A + S;
-    if (Nnew + (int)blockIdx.x * (int)blockDim.x >= N) return;  // whole CTA, before any barrier
-    const int h0 = holes_lower_bound(a.holes, A, Nnew);
-    for (int c0 = Nnew + blockIdx.x * blockDim.x; c0 < N; c0 += gridDim.x * blockDim.x) {
-        if (threadIdx.x == 0) holes_before = holes_lower_bound(a.holes, A, c0) - h0;
+    __shared__ int holes_before;  // holes in [r0, chunk start)
+    const ArPlan q = ar_plan(a);
+    const int mode = q.mode, N = q.N, r0 = q.r0, kept = q.kept, below = q.below, Nnew = q.Nnew, A = q.A;
+    if (mode != kArRemove && mode != kArShift && mode != kArNewArray) return;
+    if (r0 + (int)blockIdx.x * (int)blockDim.x >= N) return;  // whole CTA, before any barrier
+    for (int c0 = r0 + blockIdx.x * blockDim.x; c0 < N; c0 += gridDim.x * blockDim.x) {
+        if (threadIdx.x == 0) holes_before = holes_lower_bound(a.holes, A, c0) - below;
         const int p = c0 + threadIdx.x;
         const int absorbed = p < N ? (int)((mask[p >> 5] >> (p & 31)) & 1u) : 1;
         const int before = block_excl_scan(absorbed, nullptr, sh);  // its barriers publish holes_before
         if (!absorbed) {
-            const int k = S + (p - Nnew) - (holes_before + before);
-            if (k < A && OEC_IN_BOUNDS(a.holes[k], Nnew)) copy_particle(a.p, a.holes[k], p);
+            const int r = (p - r0) - (holes_before + before);
+            if (r < kept) {
+                if (mode == kArRemove) {
+                    const int dst = a.holes[kept - 1 - r];
+                    if (OEC_IN_BOUNDS(dst, Nnew)) copy_particle(a.p, dst, p);
+                } else {
+                    copy_across(a.tmp, r, a.p, p);
+                }
+            }
         }
         __syncthreads();  // holes_before is rewritten by the next chunk
     }
 }
 
+// Shifting rules, second half: tmp[i] -> slot r0 + i; for the larger-array
+// rule the added rows follow the kept particles (slot K + k = r0 + kept + k).
+__global__ void k_region_scatter(AddArgs a) {
+    const ArPlan q = ar_plan(a);
+    if (q.mode != kArShift && q.mode != kArNewArray) return;
+    const int r0 = q.r0, kept = q.kept;
+    const int items = kept + (q.mode == kArNewArray ? q.S : 0);
+    int dropped = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < items; i += gridDim.x * blockDim.x) {
+        if (i < kept) copy_across(a.p, r0 + i, a.tmp, i);
+        else if (!place_row(a, r0 + i, i - kept)) ++dropped;
+    }
+    if (dropped) atomicAdd(&a.status->n_capacity_drop, dropped);
+}
+
 __global__ void k_set_count(AddArgs a) {
-    const int N = a.scratch[0];
-    const int A = min(*a.n_holes, a.holes_cap);
-    const int S = min(*a.n_add, a.add_cap);
-    long long nn = (long long)N - A + S;
+    const ArPlan q = ar_plan(a);
+    long long nn = q.Nnew;
     if (nn > a.p.capacity) nn = a.p.capacity;
     *a.p.count = (int32_t)nn;
+    // numpy.empty((<unsigned int> (newParticleCount*1.1), nCoords)): truncation
+    if (q.mode == kArNewArray) *a.array_len = (int32_t)(uint32_t)((double)q.Nnew * 1.1);
 }
 
 __global__ void k_mask_from_keep(const uint16_t *__restrict__ keep, int n, uint32_t *__restrict__ mask, int nwords) {
@@ -425,9 +546,11 @@ OEC_BOUND_QUERY(bound_violations_boundary)
 
 using namespace oec;
 
-static bool vp(const oec_particles_t *p) {
-    return p && p->cell && p->ox && p->oy && p->vx && p->vy && p->vz && p->w && p->count && p->capacity > 0;
+static bool vstore(const oec_particles_t *p) {
+    return p && p->cell && p->ox && p->oy && p->vx && p->vy && p->vz && p->w && p->capacity > 0;
 }
+
+static bool vp(const oec_particles_t *p) { return vstore(p) && p->count; }
 
 extern "C" int oec_absorbed_index(const oec_particles_t *p, const uint32_t *absorbed_mask_dev, int32_t *index_dev,
                                   int32_t index_cap, int32_t *n_abs_dev, int32_t *scratch_dev,
@@ -499,34 +622,37 @@ extern "C" int oec_wall_interaction(const oec_grid_t *grid, const oec_boundary_t
     return OEC_OK;
 }
 
-extern "C" int oec_add_remove(const oec_grid_t *grid, oec_particles_t *p, const uint32_t *absorbed_mask_dev,
-                              const int32_t *holes_dev, const int32_t *n_holes_dev, int32_t holes_cap,
-                              const double *add_rows_dev, const int32_t *n_add_dev, int32_t add_cap,
-                              int64_t *rho_fix_dev, const double *wscale_dev, int32_t *scratch_dev,
+extern "C" int oec_add_remove(const oec_grid_t *grid, oec_particles_t *p, oec_particles_t *tmp,
+                              const uint32_t *absorbed_mask_dev, const int32_t *holes_dev, const int32_t *n_holes_dev,
+                              int32_t holes_cap, const double *add_rows_dev, const int32_t *n_add_dev, int32_t add_cap,
+                              int32_t *array_len_dev, int64_t *rho_fix_dev, const double *wscale_dev,
                               oec_status_t *status_dev, void *stream) {
-    if (!grid || !vp(p) || !absorbed_mask_dev || !holes_dev || !n_holes_dev || !n_add_dev || !scratch_dev ||
-        !status_dev || holes_cap < 0 || add_cap < 0 || (add_cap > 0 && !add_rows_dev))
+    if (!grid || !vp(p) || !vstore(tmp) || tmp->capacity < p->capacity || !absorbed_mask_dev || !holes_dev ||
+        !n_holes_dev || !n_add_dev || !status_dev || holes_cap < 0 || add_cap < 0 ||
+        (add_cap > 0 && !add_rows_dev))
         return OEC_ERR_INVALID;
     if (rho_fix_dev && !wscale_dev) return OEC_ERR_INVALID;
     GridConst gc = make_grid_const(*grid);
     AddArgs a{};
     a.p = *p;
+    a.tmp = *tmp;
     a.holes = holes_dev;
     a.n_holes = n_holes_dev;
     a.holes_cap = holes_cap;
     a.add_rows = add_rows_dev;
     a.n_add = n_add_dev;
     a.add_cap = add_cap;
+    a.array_len = array_len_dev;
     a.nx = gc.nx; a.ny = gc.ny;
     a.dxi = gc.dxi; a.dyi = gc.dyi; a.lxh = gc.lxh; a.lyh = gc.lyh;
     a.rho = reinterpret_cast<unsigned long long *>(rho_fix_dev);
     a.wscale = wscale_dev;
     a.status = status_dev;
-    a.scratch = scratch_dev;
     cudaStream_t s = as_stream(stream);
-    int cap = add_cap > 0 ? add_cap : 1;
-    k_place_added<<<persistent_grid((cap + 255) / 256, 4), 256, 0, s>>>(a);
-    k_fill_holes<<<persistent_grid(((int64_t)p->capacity + 1023) / 1024, 2), 1024, 0, s>>>(a, absorbed_mask_dev);
+    const int64_t cap = p->capacity;
+    k_place_added<<<persistent_grid((add_cap + 255) / 256 + 1, 4), 256, 0, s>>>(a);
+    k_region_gather<<<persistent_grid((cap + 1023) / 1024, 2), 1024, 0, s>>>(a, absorbed_mask_dev);
+    k_region_scatter<<<persistent_grid((cap + add_cap + 255) / 256, 4), 256, 0, s>>>(a);
     k_set_count<<<1, 1, 0, s>>>(a);
     OEC_LAUNCH_CHECK();
     return OEC_OK;

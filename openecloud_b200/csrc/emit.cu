@@ -26,6 +26,14 @@ struct Rec {
     int nsec;
 };
 
+// An absorbed row emits only with a finite position, energy and wall normal.
+// A non-finite one (the reference would draw ten secondaries from NaN
+// yields, each as non-finite, and so on at every step) emits nothing and is
+// counted in status->n_emit_skipped.
+__device__ __forceinline__ bool row_emits(const double *r, double e0, double n0, double n1) {
+    return isfinite(r[0]) && isfinite(r[1]) && isfinite(e0) && isfinite(n0) && isfinite(n1);
+}
+
 __device__ __forceinline__ double clip(double x, double lo, double hi) {
     // particleEmitter.pyx:33-39 -- a NaN falls through to `hi`
     if (x <= hi && x >= lo) return x;
@@ -44,11 +52,18 @@ __global__ void k_furman_pass1(oec_furman_t f, const double *__restrict__ rows, 
     double lfac[11];  // lgamma(j + 1), j <= m <= 10, by the threads that have work
     if ((int)(blockIdx.x * blockDim.x + threadIdx.x) < na)
         for (int j = 0; j <= f.m; ++j) lfac[j] = sf::lgam((double)j + 1.0);
+    int skipped = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += gridDim.x * blockDim.x) {
         const double *r = rows + 6 * (int64_t)i;
         const double n0 = normals[2 * i], n1 = normals[2 * i + 1];
         double v0 = sqrt(r[2] * r[2] + r[3] * r[3] + r[4] * r[4]);
         double e0 = eFactor * v0 * v0;
+        if (!row_emits(r, e0, n0, n1)) {
+            rec[i] = Rec{0., 0., 0., 1., 0};
+            nsec[i] = 0;
+            ++skipped;
+            continue;
+        }
         double th = acos((r[2] * n0 + r[3] * n1) / v0);
         if (th > 0.5 * sf::kPi) th = sf::kPi - th;
         th = clip(th, 0., f.theta0max);
@@ -104,6 +119,7 @@ __global__ void k_furman_pass1(oec_furman_t f, const double *__restrict__ rows, 
     }
     if (wd) atomicAdd(&status->warn_derm, wd);
     if (wt) atomicAdd(&status->warn_tsprime, wt);
+    if (skipped) atomicAdd(&status->n_emit_skipped, skipped);
 }
 
 // Pass 2a: the costly inverses of the joint energy split of a multi-secondary
@@ -344,11 +360,17 @@ __global__ void k_secelec_pass1(oec_secelec_t f, const double *__restrict__ rows
     const int na = min(*n_abs, cap);
     const double mass = f.model == 1 ? 9.10938291e-31 : f.particle_mass;
     const double eF = 0.5 * mass / 1.602176565e-19;
-    int capped = 0;
+    int capped = 0, skipped = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += gridDim.x * blockDim.x) {
         const double *r = rows + 6 * (int64_t)i;
         const double v0 = sqrt(r[2] * r[2] + r[3] * r[3] + r[4] * r[4]);
         const double e0 = eF * v0 * v0;
+        if (!row_emits(r, e0, normals[2 * i], normals[2 * i + 1])) {
+            rec[i] = SRec{0., 0, 0, 0, 0};
+            nsec[i] = 0;
+            ++skipped;
+            continue;
+        }
         double dE, dR, dTS;
         if (f.model == 1) {
             const double s = 1.813, eHat = 310;
@@ -387,6 +409,7 @@ __global__ void k_secelec_pass1(oec_secelec_t f, const double *__restrict__ rows
         nsec[i] = nE + nR + nT;
     }
     if (capped) atomicAdd(&status->warn_tsprime, capped);
+    if (skipped) atomicAdd(&status->n_emit_skipped, skipped);
 }
 
 __device__ __forceinline__ void put_row(double *q, const double *r, double vx, double vy, double vz) {

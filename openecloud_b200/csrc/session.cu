@@ -84,6 +84,8 @@ struct oec_run {
     oec_run_desc_t d{};
     oec_boundary_t bnd{};
     oec_particles_t p{};
+    oec_particles_t tmp{};      // scratch store of the shifting add/remove rules
+    int32_t *array_len = nullptr;  // row count of the reference's particle array
     uint32_t *mask = nullptr;
     int64_t mask_words = 0;
     int64_t *rho_fix = nullptr;
@@ -94,7 +96,7 @@ struct oec_run {
     std::vector<int8_t> l_lanes, u_lanes;
     int32_t *e_ptr = nullptr, *e_idx = nullptr;
     double *e_val = nullptr;
-    int32_t *index = nullptr, *n_abs = nullptr, *abs_scratch = nullptr, *scan_scratch = nullptr;
+    int32_t *index = nullptr, *n_abs = nullptr, *abs_scratch = nullptr;
     double *rows = nullptr, *normals = nullptr;
     void *em_work = nullptr;
     double *em_out = nullptr;
@@ -129,8 +131,8 @@ int launch_step(oec_run *r) {
     OEC_TRY(oec_wall_interaction(&d.grid, &r->bnd, d.dt, r->rows, r->n_abs, d.abs_cap, r->normals, st, s));
     OEC_TRY(oec_furman_emit(&d.furman, r->rows, r->normals, r->n_abs, d.abs_cap, r->index, d.emit_seed, 0, r->step,
                             nullptr, r->em_work, r->em_out, r->em_out_cap, r->n_out, st, s));
-    OEC_TRY(oec_add_remove(&d.grid, &r->p, r->mask, r->index, r->n_abs, (int32_t)d.capacity, r->em_out, r->n_out,
-                           r->em_out_cap, r->rho_fix, r->wscale, r->scan_scratch, st, s));
+    OEC_TRY(oec_add_remove(&d.grid, &r->p, &r->tmp, r->mask, r->index, r->n_abs, (int32_t)d.capacity, r->em_out,
+                           r->n_out, r->em_out_cap, r->array_len, r->rho_fix, r->wscale, st, s));
     OEC_TRY(oec_step_advance(r->step, s));
     OEC_TRY(oec_history(&r->p, r->step, d.table_len, r->hist_w, r->hist_n, r->hist_scratch, s));
     return OEC_OK;
@@ -177,8 +179,8 @@ int manage(oec_run *r) {
     }
     OEC_CUDA_TRY(cudaMemcpyAsync(r->n_add, &n_add, sizeof(int32_t), cudaMemcpyHostToDevice, s));
     OEC_TRY(oec_absorbed_index(&r->p, r->mask, r->index, (int32_t)d.capacity, r->n_abs, r->abs_scratch, nullptr, s));
-    OEC_TRY(oec_add_remove(&d.grid, &r->p, r->mask, r->index, r->n_abs, (int32_t)d.capacity, r->clone_rows,
-                           r->n_add, d.target, nullptr, nullptr, r->scan_scratch, r->ctx->status, s));
+    OEC_TRY(oec_add_remove(&d.grid, &r->p, &r->tmp, r->mask, r->index, r->n_abs, (int32_t)d.capacity,
+                           r->clone_rows, r->n_add, d.target, r->array_len, nullptr, nullptr, r->ctx->status, s));
     OEC_CUDA_TRY(cudaStreamSynchronize(s));  // n_add lives on this stack frame
     return prepare_deposit(r);
 }
@@ -231,6 +233,12 @@ int create_run(oec_ctx *c, const oec_run_desc_t *d, oec_run *r) {
     for (float **a : f) OEC_TRY(ctx_array(c, cap, a));
     OEC_TRY(ctx_array(c, 1, &r->p.count));
     r->p.capacity = cap;
+    OEC_TRY(ctx_array(c, cap, &r->tmp.cell));
+    float **ft[] = {&r->tmp.ox, &r->tmp.oy, &r->tmp.vx, &r->tmp.vy, &r->tmp.vz, &r->tmp.w};
+    for (float **a : ft) OEC_TRY(ctx_array(c, cap, a));
+    r->tmp.count = r->p.count;
+    r->tmp.capacity = cap;
+    OEC_TRY(ctx_array(c, 1, &r->array_len));
     r->mask_words = cap / 32;
     OEC_TRY(ctx_array(c, r->mask_words, &r->mask));
     OEC_TRY(ctx_array(c, G, &r->rho_fix));
@@ -295,7 +303,6 @@ int create_run(oec_ctx *c, const oec_run_desc_t *d, oec_run *r) {
     OEC_TRY(ctx_array(c, cap, &r->index));
     OEC_TRY(ctx_array(c, 1, &r->n_abs));
     OEC_TRY(ctx_array(c, 1024, &r->abs_scratch));
-    OEC_TRY(ctx_array(c, 1024, &r->scan_scratch));
     OEC_TRY(ctx_array(c, 6 * (size_t)d->abs_cap, &r->rows));
     OEC_TRY(ctx_array(c, 2 * (size_t)d->abs_cap, &r->normals));
     const int64_t wb = oec_furman_work_bytes(d->abs_cap);
@@ -315,11 +322,13 @@ int create_run(oec_ctx *c, const oec_run_desc_t *d, oec_run *r) {
     OEC_TRY(ctx_array(c, 1, &r->fails));
     OEC_TRY(ctx_array(c, 6 * (size_t)d->target, &r->clone_rows));
     // the initial particles (setParticleData), their deposit, the first history entry
+    const int32_t n_rows = (int32_t)d->n_rows;  // read by the copy below before the synchronize
     if (d->n_rows > 0) {
         double *aos;
         OEC_TRY(ctx_upload(c, d->rows, 6 * (size_t)d->n_rows, &aos));
         OEC_TRY(oec_particles_from_aos(&d->grid, aos, d->n_rows, &r->p, c->stream));
     }
+    OEC_CUDA_TRY(cudaMemcpyAsync(r->array_len, &n_rows, sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
     OEC_TRY(prepare_deposit(r));
     OEC_TRY(oec_history(&r->p, r->step, d->table_len, r->hist_w, r->hist_n, r->hist_scratch, c->stream));
     OEC_CUDA_TRY(cudaStreamSynchronize(c->stream));  // the host arrays may go once this returns

@@ -246,3 +246,4 @@ def homoLoader(gridObj, particlesObj, partBoundObj, macroParticleCount, weightIn
               float(vsigma), int(randomizeWeight), int(seed) & 0xffffffffffffffff, failed.data_ptr(), D.stream())
     if int(failed.item()):
         raise RuntimeError("homoLoader: rejection sampling found no inside point for some particles")
+    P._array_len.fill_(n)  # the reference stores the loaded rows with setParticleData

@@ -65,6 +65,8 @@ class Particles:
         self._soa, self._cap = soa, cap
         if self._count is None:
             self._count = D.zeros(1, torch.int32)
+            # row count of the reference's particle array (particles.pyx:109-116)
+            self._array_len = D.zeros(1, torch.int32)
             self._status = D.zeros(_lib.STATUS_WORDS, torch.int32)
             self._wscale = D.zeros(1, torch.float64)
         mask = D.zeros(cap // 32, torch.int32)
@@ -100,6 +102,7 @@ class Particles:
         self.ensure_capacity(n)
         p = self.c_particles()
         _lib.call("oec_particles_from_aos", self._grid.c_grid(), aos.data_ptr() if n else None, n, p, D.stream())
+        self._array_len.fill_(n)
 
     def soa(self):
         return self._soa
@@ -181,17 +184,24 @@ class Particles:
             col = 6  # x, y: the cell-major order is the position order used on the device
         if col not in (2, 3, 4, 5, 6):
             raise ValueError("column must be 0..5 (or 6 for cells)")
+        tmp = self.c_scratch()
+        if getattr(self, "_sort_work", None) is None or self._sort_work_cap != self._cap:
+            self._sort_work = D.empty(int(_lib.lib().oec_sort_work_bytes(self._cap)), torch.uint8)
+            self._sort_work_cap = self._cap
+        _lib.call("oec_sort_particles", self.c_particles(), tmp, col, self._sort_work.data_ptr(), D.stream())
+        self._soa, self._sort_tmp = self._sort_tmp, self._soa
+
+    def c_scratch(self):
+        """A second store of the same capacity: the sort's output (swapped in
+        afterwards) and the staging area of the shifting add/remove rules."""
         if getattr(self, "_sort_tmp", None) is None or self._sort_tmp["cell"].shape[0] != self._cap:
             self._sort_tmp = {"cell": D.empty(self._cap, torch.int32)}
             for k in ("ox", "oy", "vx", "vy", "vz", "w"):
                 self._sort_tmp[k] = D.empty(self._cap, torch.float32)
-            self._sort_work = D.empty(int(_lib.lib().oec_sort_work_bytes(self._cap)), torch.uint8)
         t = self._sort_tmp
-        tmp = _lib.Particles_t(t["cell"].data_ptr(), t["ox"].data_ptr(), t["oy"].data_ptr(), t["vx"].data_ptr(),
-                               t["vy"].data_ptr(), t["vz"].data_ptr(), t["w"].data_ptr(), self._count.data_ptr(),
-                               self._cap)
-        _lib.call("oec_sort_particles", self.c_particles(), tmp, col, self._sort_work.data_ptr(), D.stream())
-        self._soa, self._sort_tmp = t, self._soa
+        return _lib.Particles_t(t["cell"].data_ptr(), t["ox"].data_ptr(), t["oy"].data_ptr(), t["vx"].data_ptr(),
+                                t["vy"].data_ptr(), t["vz"].data_ptr(), t["w"].data_ptr(), self._count.data_ptr(),
+                                self._cap)
 
     def calcGridWeights(self, gridObj):
         """particles.pyx:52-56 -> inCell and the four CIC weights (device)."""
@@ -304,10 +314,10 @@ class Particles:
         insert the rows of addParticleData (device tensor or numpy (n, 6)).
 
         keepParticles: u16 per particle (1 = keep), or None to use the
-        absorbed bits of the last inside test already on the device.  Added
-        rows fill the holes in index order, extra rows are appended, and
-        remaining holes take the kept particles of the tail in order (the
-        set of particles equals the reference's; the order may differ)."""
+        absorbed bits of the last inside test already on the device.  Every
+        particle lands in the slot the reference gives it (oec_add_remove
+        follows the reference's three placement rules, with the row count of
+        its array tracked on the device)."""
         n_old = self.getMacroParticleCount()
         if keepParticles is not None:
             keep = D.to_device(np.asarray(keepParticles, dtype=np.uint16).astype(np.int16), torch.int16)
@@ -337,9 +347,10 @@ class Particles:
         if deposit:
             self._deposit_buffers(self._grid)
             rho, wsc = self._rho_fix.data_ptr(), self._wscale.data_ptr()
-        _lib.call("oec_add_remove", self._grid.c_grid(), p, self._mask.data_ptr(), self._holes.data_ptr(),
-                  self._n_holes.data_ptr(), self._holes.shape[0], add_dev.data_ptr(), self._n_add.data_ptr(),
-                  max(n_add, 0), rho, wsc, self._scan_scratch.data_ptr(), self._status.data_ptr(), s)
+        _lib.call("oec_add_remove", self._grid.c_grid(), p, self.c_scratch(), self._mask.data_ptr(),
+                  self._holes.data_ptr(), self._n_holes.data_ptr(), self._holes.shape[0], add_dev.data_ptr(),
+                  self._n_add.data_ptr(), max(n_add, 0), self._array_len.data_ptr(), rho, wsc,
+                  self._status.data_ptr(), s)
         self.eAtParticles = None
         self.bAtParticles = None
 

@@ -332,6 +332,24 @@ def _manage_declared():
     return L
 
 
+def add_and_remove(pd, add, keep, array_len):
+    """addAndRemoveParticles (particles.pyx:94-121, :201-269) on a particle
+    array of `array_len` rows holding the rows of `pd`: returns the rows
+    after the call and the array's row count (int(1.1 * count) when the
+    call allocated a new array)."""
+    L = _manage_declared()
+    pd = np.asarray(pd, np.float64).reshape(-1, 6)
+    add = np.ascontiguousarray(add, np.float64).reshape(-1, 6)
+    keep = np.ascontiguousarray(keep, np.uint16)
+    n, m = pd.shape[0], add.shape[0]
+    a = np.zeros((max(n, int(keep[:n].sum()) + m, 1), 6))
+    a[:n] = pd
+    k = L.orc_add_and_remove(_p(a), int(array_len), n, _p(add) if m else None, m, _p(keep))
+    if m and k > array_len:
+        array_len = int(k * 1.1)
+    return a[:k].copy(), int(array_len)
+
+
 def sort_by_column(pd, col=5, seed=None):
     """sortByColumn (particles.pyx:49-50, :431-459) with the MT stream."""
     L = _manage_declared()

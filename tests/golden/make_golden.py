@@ -511,3 +511,59 @@ def buildup_cc_golden(n_seeds=8, n_steps=1160):
 if __name__ == "__main__" and "--buildup-cc" in sys.argv:
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     buildup_cc_golden()
+
+
+# one reference Particles object through a sequence of addAndRemoveParticles
+# calls that takes each of its placement rules: (label, keep fraction, rows added)
+ADD_REMOVE_OPS = [
+    ("remove", 0.8, 0),        # _removeParticles
+    ("fill_append", 0.9, 500),  # in place, more rows than holes
+    ("shift", 0.85, 100),      # in place, fewer rows than holes
+    ("new_array", 0.95, 1500),  # above the array's rows: new array of 1.1 x count
+    ("fill_append", 0.99, 120),  # in place inside the new array's room
+    ("shift", 0.7, 50),
+    ("nothing", 1.0, 0),
+    ("remove", 0.6, 0),
+    ("shift", 0.98, 1),
+    ("new_array", 1.0, 3000),
+]
+
+
+def add_remove_golden(n0=3000):
+    """Reference addAndRemoveParticles (particles.pyx:94-121, :201-269) over
+    ADD_REMOVE_OPS.  Every row carries a unique id in its weight column
+    (the initial rows 0..n0-1, then each call's added rows in turn), so the
+    placement is recorded as the id sequence after each call, with the keep
+    bits and the row count of the reference's array (getFullParticleData);
+    the other columns play no part in the placement."""
+    grid, particles, particleBoundary, poissonSolver, randomGen = _import_reference()
+    rng = np.random.default_rng(123)
+    next_id = [0]
+
+    def rows(n):
+        r = make_particles(rng, n, 0.04, 0.04, 1, 3e5) if n else np.zeros((0, 6))
+        r[:, 5] = np.arange(next_id[0], next_id[0] + n, dtype=np.float64)
+        next_id[0] += n
+        return r
+
+    P = particles.Particles("electrons", "variableWeight")
+    pd0 = rows(n0)
+    P.setParticleData(pd0.copy())
+    out = {"n0": np.array(n0)}
+    for k, (label, frac, n_add) in enumerate(ADD_REMOVE_OPS):
+        n = P.getMacroParticleCount()
+        keep = (rng.random(n) < frac).astype(np.uint16)
+        add = rows(n_add)
+        P.addAndRemoveParticles(add if n_add else np.zeros((0, 6)), keep)
+        out[f"keep{k}"] = np.packbits(keep.astype(bool))
+        out[f"nadd{k}"] = np.array(n_add)
+        out[f"ids{k}"] = np.asarray(P.getParticleData())[:, 5].astype(np.int32)
+        out[f"len{k}"] = np.array(np.asarray(P.getFullParticleData()).shape[0])
+        print(label, n, "->", P.getMacroParticleCount(), "array rows", int(out[f"len{k}"]))
+    path = os.path.join(HERE, "add_remove.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path))
+
+
+if __name__ == "__main__" and "--add-remove" in sys.argv:
+    add_remove_golden()

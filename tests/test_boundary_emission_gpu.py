@@ -8,7 +8,8 @@
   rows within 1e-10 (different libm); with Philox draws: the energy and angle
   spectra pass a two-sample KS test against the reference's secondaries;
 * add/remove: the resulting particle set equals the kept rows plus the added
-  rows (order not compared).
+  rows, and every particle sits in the slot the reference's placement rules
+  give it (against the compiled reference's id sequences and the oracle).
 """
 import numpy as np
 import pytest
@@ -165,56 +166,76 @@ def test_add_remove_set_semantics(gpu):
         assert np.array_equal(key(after), key(expect))
 
 
-def _placement_model(before, add_stored, keep):
-    """particles.pyx:254-269 restated on the host: added rows fill the holes
-    in index order and extra rows are appended; with fewer added rows than
-    holes the kept particles of the tail [N_new, N) move, in order, into the
-    remaining holes below N_new."""
-    n = before.shape[0]
-    holes = np.nonzero(keep == 0)[0]
-    A, S = holes.size, add_stored.shape[0]
-    out = before.copy()
-    if S >= A:
-        out[holes] = add_stored[:A]
-        return np.concatenate([out, add_stored[A:]])
-    out[holes[:S]] = add_stored
-    n_new = n - A + S
-    tail = np.arange(n_new, n)
-    kept_tail = tail[keep[n_new:] == 1]
-    out[holes[S:S + kept_tail.size]] = before[kept_tail]
-    return out[:n_new]
+def _stored(g, rows):
+    """rows as the device store holds them (FP32 cell offsets, velocities
+    and weights), read back as f64 rows."""
+    from openecloud_b200.particles import Particles
+    P2 = Particles("electrons", "variableWeight")
+    P2.setParticleData(rows if rows.shape[0] else np.zeros((1, 6)))
+    P2._bind(g)
+    return P2.getParticleData()[:rows.shape[0]]
+
+
+def _rows(rng, ids):
+    r = np.empty((ids.size, 6))
+    r[:, :2] = rng.uniform(-0.019, 0.019, (ids.size, 2))
+    r[:, 2:5] = rng.normal(0, 1e5, (ids.size, 3))
+    r[:, 5] = ids
+    return r
+
+
+def test_add_remove_replays_reference_placement(gpu):
+    """Slot by slot against the compiled reference: a sequence of calls on one
+    store that takes every placement rule (remove only, in place with more and
+    with fewer added rows than holes, a new larger array and the room it
+    leaves); every row's id rides in its weight (exact in FP32)."""
+    from openecloud_b200.grid import Grid
+    from openecloud_b200.particles import Particles
+    z = golden("add_remove.npz")
+    rng = np.random.default_rng(1)
+    g = Grid(64, 64, 0.04, 0.04, 0)
+    n0 = int(z["n0"])
+    P = Particles("electrons", "variableWeight")
+    P.setParticleData(_rows(rng, np.arange(n0, dtype=np.float64)))
+    P._bind(g)
+    next_id, k = n0, 0
+    while f"ids{k}" in z.files:
+        n, m = P.getMacroParticleCount(), int(z[f"nadd{k}"])
+        keep = np.unpackbits(z[f"keep{k}"])[:n].astype(np.uint16)
+        add = _rows(rng, np.arange(next_id, next_id + m, dtype=np.float64))
+        next_id += m
+        P.addAndRemoveParticles(add, keep)
+        assert np.array_equal(P.getParticleData()[:, 5].astype(np.int32), z[f"ids{k}"]), k
+        assert int(P._array_len.item()) == int(z[f"len{k}"]), k
+        k += 1
+    assert k == 10
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n,n_add,frac_keep", [(60000, 2000, 0.7), (200000, 100, 0.95), (50000, 0, 0.5),
-                                               (30000, 9000, 0.7)])
-def test_add_remove_exact_placement(gpu, n, n_add, frac_keep):
-    """The device placement, particle by particle, against the host model over
-    tails of many 1024-position chunks (the fill runs chunk-parallel)."""
+@pytest.mark.parametrize("n,ops", [
+    (60000, [(0.7, 2000), (1.0, 20000), (0.99, 3000), (0.5, 0), (0.7, 9000)]),
+    (200000, [(0.95, 100), (0.999, 30000), (0.99, 5000), (0.6, 0), (0.98, 4000), (0.9, 0)]),
+])
+def test_add_remove_exact_placement(gpu, n, ops):
+    """Full rows, slot by slot, against the oracle's addAndRemoveParticles
+    over stores of many 1024-position chunks (the moves run chunk-parallel),
+    with the row count of the reference's array carried along."""
     from openecloud_b200.grid import Grid
     from openecloud_b200.particles import Particles
-    rng = np.random.default_rng(n + n_add)
+    rng = np.random.default_rng(n)
     g = Grid(64, 64, 0.04, 0.04, 0)
-    pd = np.empty((n, 6))
-    pd[:, :2] = rng.uniform(-0.019, 0.019, (n, 2))
-    pd[:, 2:5] = rng.normal(0, 1e5, (n, 3))
-    pd[:, 5] = rng.uniform(1, 2, n)
-    add = np.empty((n_add, 6))
-    add[:, :2] = rng.uniform(-0.019, 0.019, (n_add, 2))
-    add[:, 2:5] = rng.normal(0, 1e5, (n_add, 3))
-    add[:, 5] = rng.uniform(3, 4, n_add)
-    keep = (rng.random(n) < frac_keep).astype(np.uint16)
+    pd = _rows(rng, rng.uniform(1, 2, n))
     P = Particles("electrons", "variableWeight")
     P.setParticleData(pd)
     P._bind(g)
-    before = P.getParticleData()
-    P.addAndRemoveParticles(add, keep)
-    after = P.getParticleData()
-    P2 = Particles("electrons", "variableWeight")
-    P2.setParticleData(add if n_add else np.zeros((1, 6)))
-    P2._bind(g)
-    add_stored = P2.getParticleData()[:n_add]
-    assert np.array_equal(after, _placement_model(before, add_stored, keep))
+    expect, array_len = P.getParticleData(), n
+    for frac_keep, n_add in ops:
+        add = _rows(rng, rng.uniform(3, 4, n_add))
+        keep = (rng.random(expect.shape[0]) < frac_keep).astype(np.uint16)
+        P.addAndRemoveParticles(add, keep)
+        expect, array_len = O.add_and_remove(expect, _stored(g, add), keep, array_len)
+        assert np.array_equal(P.getParticleData(), expect)
+        assert int(P._array_len.item()) == array_len
 
 
 def test_homo_loader_uniform_inside(gpu):
