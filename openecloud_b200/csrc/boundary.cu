@@ -457,30 +457,29 @@ __device__ __forceinline__ bool place_row(AddArgs &a, int dst, int k) {
     return true;
 }
 
-// In-place rules: added row k fills hole k (k < A), the rest are appended
-// after the old count.  With S < A only holes are filled.
-__global__ void k_place_added(AddArgs a) {
-    const ArPlan q = ar_plan(a);
-    if (q.mode != kArFillAppend && q.mode != kArShift) return;
-    int dropped = 0;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < q.S; k += gridDim.x * blockDim.x) {
-        const int dst = (k < q.A) ? a.holes[k] : q.N + (k - q.A);
-        if (!place_row(a, dst, k)) ++dropped;
-    }
-    if (dropped) atomicAdd(&a.status->n_capacity_drop, dropped);
-}
-
-// The kept particles of the region [r0, N), each with its rank among them:
-// (p - r0) minus the holes in [r0, p), which a CTA takes for its chunk's
-// start from the ascending holes array (one binary search) and within the
-// chunk from a scan of the absorbed bits, so the chunks run independently.
-// Remove-only: rank r goes to hole kept-1-r (descending into ascending
-// holes, all below N_new <= r0).  Shifting rules: rank r goes to tmp[r].
-__global__ void __launch_bounds__(1024) k_region_gather(AddArgs a, const uint32_t *__restrict__ mask) {
+// One launch, two loops.  First the in-place rules' added rows: row k fills
+// hole k (k < A), the rest are appended after the old count (with S < A only
+// holes are filled, all below r0).  Then the kept particles of the region
+// [r0, N), each with its rank among them: (p - r0) minus the holes in
+// [r0, p), which a CTA takes for its chunk's start from the ascending holes
+// array (one binary search) and within the chunk from a scan of the absorbed
+// bits, so the chunks run independently.  Remove-only: rank r goes to hole
+// kept-1-r (descending into ascending holes, all below N_new <= r0).
+// Shifting rules: rank r goes to tmp[r].  The two loops touch disjoint
+// slots (holes below r0 or slots from N on, against [r0, N)).
+__global__ void __launch_bounds__(1024) k_place_gather(AddArgs a, const uint32_t *__restrict__ mask) {
     __shared__ int sh[32];
     __shared__ int holes_before;  // holes in [r0, chunk start)
     const ArPlan q = ar_plan(a);
     const int mode = q.mode, N = q.N, r0 = q.r0, kept = q.kept, below = q.below, Nnew = q.Nnew, A = q.A;
+    if (mode == kArFillAppend || mode == kArShift) {
+        int dropped = 0;
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < q.S; k += gridDim.x * blockDim.x) {
+            const int dst = (k < A) ? a.holes[k] : N + (k - A);
+            if (!place_row(a, dst, k)) ++dropped;
+        }
+        if (dropped) atomicAdd(&a.status->n_capacity_drop, dropped);
+    }
     if (mode != kArRemove && mode != kArShift && mode != kArNewArray) return;
     if (r0 + (int)blockIdx.x * (int)blockDim.x >= N) return;  // whole CTA, before any barrier
     for (int c0 = r0 + blockIdx.x * blockDim.x; c0 < N; c0 += gridDim.x * blockDim.x) {
@@ -650,8 +649,8 @@ extern "C" int oec_add_remove(const oec_grid_t *grid, oec_particles_t *p, oec_pa
     a.status = status_dev;
     cudaStream_t s = as_stream(stream);
     const int64_t cap = p->capacity;
-    k_place_added<<<persistent_grid((add_cap + 255) / 256 + 1, 4), 256, 0, s>>>(a);
-    k_region_gather<<<persistent_grid((cap + 1023) / 1024, 2), 1024, 0, s>>>(a, absorbed_mask_dev);
+    const int64_t span = cap > (int64_t)add_cap ? cap : (int64_t)add_cap;
+    k_place_gather<<<persistent_grid((span + 1023) / 1024, 2), 1024, 0, s>>>(a, absorbed_mask_dev);
     k_region_scatter<<<persistent_grid((cap + add_cap + 255) / 256, 4), 256, 0, s>>>(a);
     k_set_count<<<1, 1, 0, s>>>(a);
     OEC_LAUNCH_CHECK();
