@@ -615,7 +615,8 @@ def component_rooflines(peak, n=1 << 24, n_merge=2_000_000):
     W.setParticleData(pd[:4096])
     W._bind(g)
     W.addAndRemoveParticles(pd[:16], (np.arange(4096) % 3 != 0).astype(np.uint16))
-    ms = timed(lambda: _lib.call("oec_add_remove", cg, cp, P.c_scratch(), P._mask.data_ptr(), bd._index.data_ptr(),
+    tmp = P.c_scratch()  # the scratch store is allocated before the timed call
+    ms = timed(lambda: _lib.call("oec_add_remove", cg, cp, tmp, P._mask.data_ptr(), bd._index.data_ptr(),
                                  bd._n_abs.data_ptr(), bd._index.shape[0], em._out.data_ptr(), em._n_out.data_ptr(),
                                  em._out.shape[0], P._array_len.data_ptr(), rho, wsc, st, sh), reps=1, warm=0)
     out.append(line("refill and compaction (oec_add_remove)", n / 8 + (48 + 28 + 16) * n_sec + 112 * moved, ms,

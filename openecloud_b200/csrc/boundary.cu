@@ -462,14 +462,18 @@ __device__ __forceinline__ bool place_row(AddArgs &a, int dst, int k) {
 // holes are filled, all below r0).  Then the kept particles of the region
 // [r0, N), each with its rank among them: (p - r0) minus the holes in
 // [r0, p), which a CTA takes for its chunk's start from the ascending holes
-// array (one binary search) and within the chunk from a scan of the absorbed
-// bits, so the chunks run independently.  Remove-only: rank r goes to hole
+// array (a binary search; the 32 warps search the starts of 32 successive
+// chunk iterations at once, so the dependent loads of one search are paid
+// once per 32 chunks) and within the chunk from a scan of the absorbed bits,
+// so the chunks run independently.  Remove-only: rank r goes to hole
 // kept-1-r (descending into ascending holes, all below N_new <= r0).
 // Shifting rules: rank r goes to tmp[r].  The two loops touch disjoint
 // slots (holes below r0 or slots from N on, against [r0, N)).
-__global__ void __launch_bounds__(1024) k_place_gather(AddArgs a, const uint32_t *__restrict__ mask) {
+constexpr int kGatherThreads = 1024;  // 32 warps: one hole search per warp
+
+__global__ void __launch_bounds__(kGatherThreads) k_place_gather(AddArgs a, const uint32_t *__restrict__ mask) {
     __shared__ int sh[32];
-    __shared__ int holes_before;  // holes in [r0, chunk start)
+    __shared__ int holes_before[32];  // holes in [r0, chunk start) of 32 successive chunk iterations
     const ArPlan q = ar_plan(a);
     const int mode = q.mode, N = q.N, r0 = q.r0, kept = q.kept, below = q.below, Nnew = q.Nnew, A = q.A;
     if (mode == kArFillAppend || mode == kArShift) {
@@ -482,13 +486,20 @@ __global__ void __launch_bounds__(1024) k_place_gather(AddArgs a, const uint32_t
     }
     if (mode != kArRemove && mode != kArShift && mode != kArNewArray) return;
     if (r0 + (int)blockIdx.x * (int)blockDim.x >= N) return;  // whole CTA, before any barrier
-    for (int c0 = r0 + blockIdx.x * blockDim.x; c0 < N; c0 += gridDim.x * blockDim.x) {
-        if (threadIdx.x == 0) holes_before = holes_lower_bound(a.holes, A, c0) - below;
+    const int stride = gridDim.x * blockDim.x;
+    int iter = 0;
+    for (int c0 = r0 + blockIdx.x * blockDim.x; c0 < N; c0 += stride, ++iter) {
+        if ((iter & 31) == 0 && (threadIdx.x & 31) == 0) {
+            // warp w: the start of chunk iteration iter + w (rewritten only
+            // after the barrier that ends iteration iter - 1)
+            const int cw = c0 + (threadIdx.x >> 5) * stride;
+            holes_before[threadIdx.x >> 5] = cw < N ? holes_lower_bound(a.holes, A, cw) - below : 0;
+        }
         const int p = c0 + threadIdx.x;
         const int absorbed = p < N ? (int)((mask[p >> 5] >> (p & 31)) & 1u) : 1;
         const int before = block_excl_scan(absorbed, nullptr, sh);  // its barriers publish holes_before
         if (!absorbed) {
-            const int r = (p - r0) - (holes_before + before);
+            const int r = (p - r0) - (holes_before[iter & 31] + before);
             if (r < kept) {
                 if (mode == kArRemove) {
                     const int dst = a.holes[kept - 1 - r];
@@ -498,7 +509,7 @@ __global__ void __launch_bounds__(1024) k_place_gather(AddArgs a, const uint32_t
                 }
             }
         }
-        __syncthreads();  // holes_before is rewritten by the next chunk
+        __syncthreads();  // holes_before is rewritten 32 chunk iterations later
     }
 }
 
@@ -650,7 +661,8 @@ extern "C" int oec_add_remove(const oec_grid_t *grid, oec_particles_t *p, oec_pa
     cudaStream_t s = as_stream(stream);
     const int64_t cap = p->capacity;
     const int64_t span = cap > (int64_t)add_cap ? cap : (int64_t)add_cap;
-    k_place_gather<<<persistent_grid((span + 1023) / 1024, 2), 1024, 0, s>>>(a, absorbed_mask_dev);
+    k_place_gather<<<persistent_grid((span + kGatherThreads - 1) / kGatherThreads, 2), kGatherThreads, 0, s>>>(
+        a, absorbed_mask_dev);
     k_region_scatter<<<persistent_grid((cap + add_cap + 255) / 256, 4), 256, 0, s>>>(a);
     k_set_count<<<1, 1, 0, s>>>(a);
     OEC_LAUNCH_CHECK();
