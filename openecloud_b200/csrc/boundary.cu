@@ -492,8 +492,8 @@ __global__ void __launch_bounds__(kGatherThreads) k_place_gather(AddArgs a, cons
         if ((iter & 31) == 0 && (threadIdx.x & 31) == 0) {
             // warp w: the start of chunk iteration iter + w (rewritten only
             // after the barrier that ends iteration iter - 1)
-            const int cw = c0 + (threadIdx.x >> 5) * stride;
-            holes_before[threadIdx.x >> 5] = cw < N ? holes_lower_bound(a.holes, A, cw) - below : 0;
+            const int64_t cw = (int64_t)c0 + (int64_t)(threadIdx.x >> 5) * stride;
+            holes_before[threadIdx.x >> 5] = cw < N ? holes_lower_bound(a.holes, A, (int)cw) - below : 0;
         }
         const int p = c0 + threadIdx.x;
         const int absorbed = p < N ? (int)((mask[p >> 5] >> (p & 31)) & 1u) : 1;
