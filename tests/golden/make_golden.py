@@ -567,3 +567,71 @@ def add_remove_golden(n0=3000):
 
 if __name__ == "__main__" and "--add-remove" in sys.argv:
     add_remove_golden()
+
+
+# a fixed inward field (the electrons are pushed outward) on the 32x32 circle:
+# E = -k (x, y) at the nodes, so the wall sees impacts of up to ~2 keV and
+# the refill takes every placement rule over the run
+LOOP_RUN = dict(grid="circle_32", n0=800, k=1e7, dt=1e-11, steps=300, seed=5, sey=1.6)
+
+
+def loop_field(xm, ym, k):
+    X, Y = np.meshgrid(xm, ym)
+    return np.concatenate([(-k * X).reshape(-1), (-k * Y).reshape(-1)])
+
+
+def loop_checksums(pd):
+    """Per-column sums and the slot-weighted sums of x and vx (which change
+    when the same rows sit in other slots)."""
+    i = np.arange(pd.shape[0], dtype=np.float64)
+    return np.concatenate([pd.sum(0), [np.dot(i, pd[:, 0]), np.dot(i, pd[:, 2])]])
+
+
+def loop_golden():
+    """The reference's particle loop without the Poisson solve (example01's
+    calcGridWeights, eFieldToParticles, borisPush, indexInside, saveAbsorbed,
+    calculateInteractionPoint, calculateNormalVectors, generateSecondaries,
+    addAndRemoveParticles; example01_basic.py:66-97) in the fixed field of
+    loop_field, LOOP_RUN['steps'] steps: per step the count, the row count of
+    the particle array and the checksums, and the rows at the end."""
+    grid, particles, particleBoundary, poissonSolver, randomGen = _import_reference()
+    import particleEmitter
+    r = LOOP_RUN
+    nx, ny, lx, ly, bt = GRIDS[r["grid"]]
+    g = grid.Grid(nx, ny, lx, ly, bt)
+    E = loop_field(np.asarray(g.getXMesh()), np.asarray(g.getYMesh()), r["k"])
+    rng = np.random.default_rng(77)
+    pd0 = make_particles(rng, r["n0"], lx, ly, bt, 3e5)
+    P = particles.Particles("electrons", "variableWeight")
+    P.setParticleData(pd0.copy())
+    bd = particleBoundary.AbsorbElliptical(g, P)
+    em = particleEmitter.FurmanEmitter(bd, P, seyMax=r["sey"])
+    randomGen.seed(r["seed"])
+    counts, lens, sums, absorbed = [], [], [], []
+    for _ in range(r["steps"]):
+        P.calcGridWeights(g)
+        P.eFieldToParticles(g, E)
+        P.borisPush(r["dt"], 0)
+        bd.indexInside()
+        bd.saveAbsorbed()
+        na = bd.getAbsorbedMacroParticleCount()
+        absorbed.append(na)
+        if na > 0:
+            bd.calculateInteractionPoint()
+            bd.calculateNormalVectors()
+            P.addAndRemoveParticles(em.generateSecondaries(), P.getIsInside())
+        pd = np.asarray(P.getParticleData())
+        counts.append(pd.shape[0])
+        lens.append(np.asarray(P.getFullParticleData()).shape[0])
+        sums.append(loop_checksums(pd))
+    out = {"pd0": pd0, "counts": np.array(counts), "array_len": np.array(lens), "absorbed": np.array(absorbed),
+           "checksums": np.array(sums), "final": np.asarray(P.getParticleData()).copy(),
+           "params": np.array([nx, ny, lx, ly, bt], np.float64), "k": np.array(r["k"]), "dt": np.array(r["dt"]),
+           "seed": np.array(r["seed"]), "sey": np.array(r["sey"])}
+    path = os.path.join(HERE, "loop_circle_32.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "final count", counts[-1], "absorbed", sum(absorbed))
+
+
+if __name__ == "__main__" and "--loop" in sys.argv:
+    loop_golden()
