@@ -587,13 +587,16 @@ def loop_checksums(pd):
     return np.concatenate([pd.sum(0), [np.dot(i, pd[:, 0]), np.dot(i, pd[:, 2])]])
 
 
-def loop_golden():
-    """The reference's particle loop without the Poisson solve (example01's
-    calcGridWeights, eFieldToParticles, borisPush, indexInside, saveAbsorbed,
+def loop_golden(space_charge=False):
+    """The reference's particle loop (example01's calcGridWeights,
+    eFieldToParticles, borisPush, indexInside, saveAbsorbed,
     calculateInteractionPoint, calculateNormalVectors, generateSecondaries,
     addAndRemoveParticles; example01_basic.py:66-97) in the fixed field of
     loop_field, LOOP_RUN['steps'] steps: per step the count, the row count of
-    the particle array and the checksums, and the rows at the end."""
+    the particle array and the checksums, and the rows at the end.  With
+    space_charge the electrons' own field is added every step (chargeToGrid,
+    PoissonSolver.solve; example01_basic.py:71-81 without the beam) and
+    their weights are 1e4 times larger, so that it matters."""
     grid, particles, particleBoundary, poissonSolver, randomGen = _import_reference()
     import particleEmitter
     r = LOOP_RUN
@@ -602,15 +605,22 @@ def loop_golden():
     E = loop_field(np.asarray(g.getXMesh()), np.asarray(g.getYMesh()), r["k"])
     rng = np.random.default_rng(77)
     pd0 = make_particles(rng, r["n0"], lx, ly, bt, 3e5)
+    if space_charge:
+        pd0[:, 5] *= 1e4
     P = particles.Particles("electrons", "variableWeight")
     P.setParticleData(pd0.copy())
     bd = particleBoundary.AbsorbElliptical(g, P)
     em = particleEmitter.FurmanEmitter(bd, P, seyMax=r["sey"])
+    ps = poissonSolver.PoissonSolver(g)
     randomGen.seed(r["seed"])
     counts, lens, sums, absorbed = [], [], [], []
     for _ in range(r["steps"]):
         P.calcGridWeights(g)
-        P.eFieldToParticles(g, E)
+        if space_charge:
+            P.chargeToGrid(g)
+            P.eFieldToParticles(g, np.asarray(ps.solve(np.asarray(P.getChargeOnGrid()))) + E)
+        else:
+            P.eFieldToParticles(g, E)
         P.borisPush(r["dt"], 0)
         bd.indexInside()
         bd.saveAbsorbed()
@@ -627,11 +637,32 @@ def loop_golden():
     out = {"pd0": pd0, "counts": np.array(counts), "array_len": np.array(lens), "absorbed": np.array(absorbed),
            "checksums": np.array(sums), "final": np.asarray(P.getParticleData()).copy(),
            "params": np.array([nx, ny, lx, ly, bt], np.float64), "k": np.array(r["k"]), "dt": np.array(r["dt"]),
-           "seed": np.array(r["seed"]), "sey": np.array(r["sey"])}
-    path = os.path.join(HERE, "loop_circle_32.npz")
+           "seed": np.array(r["seed"]), "sey": np.array(r["sey"]), "space_charge": np.array(int(space_charge))}
+    path = os.path.join(HERE, "loop_sc_circle_32.npz" if space_charge else "loop_circle_32.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path), "final count", counts[-1], "absorbed", sum(absorbed))
 
 
 if __name__ == "__main__" and "--loop" in sys.argv:
     loop_golden()
+    loop_golden(space_charge=True)
+
+
+def e2n_csc_golden():
+    """Adds to each grid_*.npz the grid's edge-to-node matrix exactly as the
+    reference returns it (CSC, its own index order: the order in which the
+    phi -> E product sums), so that a restated solve gives the same E bit for
+    bit; the CSR copy already stored is sorted."""
+    grid, particles, particleBoundary, poissonSolver, randomGen = _import_reference()
+    for gname, (nx, ny, lx, ly, bt) in GRIDS.items():
+        path = os.path.join(HERE, f"grid_{gname}.npz")
+        arrays = dict(np.load(path))
+        e2n = grid.Grid(nx, ny, lx, ly, bt).getEdgeToNode().tocsc()
+        arrays["e2n_csc_indptr"], arrays["e2n_csc_indices"], arrays["e2n_csc_data"] = \
+            e2n.indptr.copy(), e2n.indices.copy(), e2n.data.copy()
+        np.savez_compressed(path, **arrays)
+        print("wrote", path, os.path.getsize(path))
+
+
+if __name__ == "__main__" and "--e2n-csc" in sys.argv:
+    e2n_csc_golden()
