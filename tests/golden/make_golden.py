@@ -666,3 +666,81 @@ def e2n_csc_golden():
 
 if __name__ == "__main__" and "--e2n-csc" in sys.argv:
     e2n_csc_golden()
+
+
+EXAMPLE01_RUN = dict(n_particles=2000, steps=1200, load_seed=3, seed=11)
+
+
+def example01_golden():
+    """example01_basic.py's loop as written (32x32 circle, LHCBeam, Furman
+    emitter with its defaults, globalRandom every 50 steps outside +-5 %,
+    dt = 2.155172413795e-11), with 2000 instead of 1e5 macro-particles, over
+    its first 1200 steps (the first bunch passage).  The loaded rows are
+    recorded and the MT stream re-seeded before the loop, so the oracle can
+    start from them; the beam charge of each step is recorded as its scalar
+    factor times the transverse profile (checked to be the reference's
+    getCharge bit for bit).  Per step: count, array rows, absorbed count,
+    whether globalRandom ran, checksums; the rows at the end."""
+    grid, particles, particleBoundary, poissonSolver, randomGen = _import_reference()
+    import particleEmitter
+    import particleManagement
+    from beam import LHCBeam
+    r = EXAMPLE01_RUN
+    N = r["n_particles"]
+    g = grid.Grid(32, 32, 0.04, 0.04, 1)
+    dt = 2.155172413795e-11
+    beam = LHCBeam(g, dt)
+    P = particles.Particles("electrons", "variableWeight")
+    bd = particleBoundary.AbsorbElliptical(g, P)
+    em = particleEmitter.FurmanEmitter(bd, P)
+    ps = poissonSolver.PoissonSolver(g)
+    randomGen.seed(r["load_seed"])
+    particleEmitter.homoLoader(g, P, bd, N, 1.e9 / N)
+    pd0 = np.asarray(P.getParticleData()).copy()
+    profile = np.asarray(beam.getTransversalProfile()).copy()
+    randomGen.seed(r["seed"])
+    counts, lens, absorbed, managed, sums, beam_scale = [], [], [], [], [], []
+    for ii in range(r["steps"]):
+        n = P.getMacroParticleCount()
+        man = ii > 0 and ii % 50 == 0 and (n > 1.05 * N or n < 0.95 * N)
+        if man:
+            particleManagement.globalRandom(g, P, N)
+        managed.append(int(man))
+        P.calcGridWeights(g)
+        P.chargeToGrid(g)
+        qb = beam.getCharge(ii * dt)
+        saved, beam.qTransversalProfile = beam.qTransversalProfile, np.float64(1.0)
+        scale = beam.getCharge(ii * dt)
+        beam.qTransversalProfile = saved
+        if np.isscalar(qb) and qb == 0:
+            beam_scale.append(np.nan)  # no bunch: the reference adds the integer 0
+        else:
+            assert np.array_equal(float(scale) * profile, qb)
+            beam_scale.append(float(scale))
+        ps.solve(np.asarray(P.getChargeOnGrid()) + qb)
+        P.eFieldToParticles(g, ps.getEAtGridPoints())
+        P.borisPush(dt, 0)
+        bd.indexInside()
+        bd.saveAbsorbed()
+        na = bd.getAbsorbedMacroParticleCount()
+        absorbed.append(na)
+        if na > 0:
+            bd.calculateInteractionPoint()
+            bd.calculateNormalVectors()
+            P.addAndRemoveParticles(em.generateSecondaries(), P.getIsInside())
+        pd = np.asarray(P.getParticleData())
+        counts.append(pd.shape[0])
+        lens.append(np.asarray(P.getFullParticleData()).shape[0])
+        sums.append(loop_checksums(pd))
+    out = {"pd0": pd0, "profile": profile, "beam_scale": np.array(beam_scale), "counts": np.array(counts),
+           "array_len": np.array(lens), "absorbed": np.array(absorbed), "managed": np.array(managed),
+           "checksums": np.array(sums), "final": np.asarray(P.getParticleData()).copy(), "dt": np.array(dt),
+           "seed": np.array(r["seed"]), "target": np.array(N)}
+    path = os.path.join(HERE, "example01_circle_32.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "final count", counts[-1], "absorbed", sum(absorbed),
+          "management events", sum(managed), "beam steps", int(np.isfinite(out["beam_scale"]).sum()))
+
+
+if __name__ == "__main__" and "--example01" in sys.argv:
+    example01_golden()

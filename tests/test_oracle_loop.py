@@ -64,3 +64,44 @@ def test_oracle_particle_loop_replays_reference(fixture):
         assert np.array_equal(checksums(pd), z["checksums"][s]), s
     assert rules == {"remove", "new array", "fill/append", "shift"}, rules
     assert np.array_equal(pd, z["final"])
+
+
+def test_oracle_replays_example01():
+    """example01_basic.py's loop as written -- deposit, beam, solve, gather,
+    push, boundary, Furman emission, refill and globalRandom every 50 steps,
+    all on the one MT stream -- with 2000 macro-particles over its first
+    1200 steps (the first bunch passage; make_golden.py --example01): the
+    oracle replays the compiled reference bit for bit at every step."""
+    z = golden("example01_circle_32.npz")
+    solver = from_golden(golden("grid_circle_32.npz"))
+    g = O.GridGeom(32, 32, 0.04, 0.04)
+    f = O.furman("copper")
+    target, dt = int(z["target"]), float(z["dt"])
+    pd = z["pd0"].copy()
+    array_len = pd.shape[0]
+    O.seed(int(z["seed"]))
+    for s in range(z["counts"].shape[0]):
+        n = pd.shape[0]
+        if s > 0 and s % 50 == 0 and (n > 1.05 * target or n < 0.95 * target):
+            assert z["managed"][s], s
+            pd = O.global_random(pd, target)
+            if pd.shape[0] > n and pd.shape[0] > array_len:  # cloned rows in a new array
+                array_len = int(pd.shape[0] * 1.1)
+        else:
+            assert not z["managed"][s], s
+        q = O.charge_to_grid(pd, g, QE)
+        if np.isfinite(z["beam_scale"][s]):
+            q = q + z["beam_scale"][s] * z["profile"]
+        e = O.field_to_particles(pd, g, solver.solve(q)[1], 2)
+        pd = O.boris_push(pd, e, dt, QM, 0)
+        inside, pd = O.index_inside(pd, g, 1)
+        ab = O.save_absorbed(pd, inside)
+        assert ab.shape[0] == z["absorbed"][s], s
+        if ab.shape[0]:
+            wall, normals, _ = O.interaction(ab, g, 1)
+            pd, array_len = O.add_and_remove(pd, O.furman_emit(f, wall, normals, mode=0), inside, array_len)
+        assert pd.shape[0] == z["counts"][s], s
+        assert array_len == z["array_len"][s], s
+        assert np.array_equal(checksums(pd), z["checksums"][s]), s
+    assert z["managed"].sum() >= 3
+    assert np.array_equal(pd, z["final"])
