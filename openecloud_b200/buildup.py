@@ -15,8 +15,9 @@ replayed.  Per step:
                                                              oec_save_absorbed,
                                                              oec_wall_interaction)
   6. Furman emission                                        (oec_furman_emit)
-  7. holes <- secondaries, tail compaction, deposit of the
-     secondaries for the next step                          (oec_add_remove)
+  7. refill in the reference's slot order (secondaries into
+     holes, shift or append), deposit of the secondaries
+     for the next step                                      (oec_add_remove)
   8. history (count, sum w) and ++step                      (oec_history, oec_step_advance)
 
 Particle management (globalRandom / localRandom) runs between graph replays
@@ -26,8 +27,10 @@ scale.
 Particle order is physics here: the reference's Furman emitter gives a lone
 secondary the elastic / rediffused / true-secondary split of the LAST
 absorbed particle of the step (particleEmitter.pyx:245-246), so which particle
-is last matters.  The driver keeps the reference's order (holes refilled by
-secondaries, extras appended, tail compaction) and does not sort by default.
+is last matters.  The refill puts every particle in the slot the reference's
+array gives it (all three placement routines of particles.pyx, with the
+array's row count tracked on the device), and the driver does not sort by
+default.
 Periodic cell sorting (`sort_every`) helps the deposit's warp aggregation but
 is only order-neutral with the emitter's `compat` switch off.
 """

@@ -1,5 +1,5 @@
 // boundary.cu -- absorbed particles, wall intersection and wall normals,
-// and the removal/insertion of particles (compaction with hole filling).
+// and the removal/insertion of particles in the reference's slot order.
 //
 // Reference: particleBoundary.pyx (saveAbsorbed :38-65, AbsorbRectangular
 // :99-221, AbsorbElliptical :252-297, AbsorbArbitraryCutCell :373-481) and
