@@ -374,21 +374,27 @@ def global_random(pd, target, seed=None):
 
 
 def local_random(pd, target, g, kind=1, seed=None, threshold=2., lambda_factor=1., dis_limit=1., scheme=0,
-                 leaf=10):
-    """localRandom (particleManagement.pyx:74-238) with the MT stream; the
-    particle array starts with capacity n, as after setParticleData."""
+                 leaf=10, array_len=None):
+    """localRandom (particleManagement.pyx:74-238) with the MT stream.  The
+    particle array holds n rows, as after setParticleData, or array_len rows
+    when given; then the array's row count after the call is returned too
+    (int(1.1 * count) when the refill needed a new array)."""
     L = _manage_declared()
     if seed is not None:
         L.orc_seed(int(seed))
     n = pd.shape[0]
+    cap = n if array_len is None else int(array_len)
     room = 2 * n + 10
     a = np.zeros((room, 6))
     a[:n] = pd
     scratch = np.zeros((n + 10, 6))
-    k = L.orc_local_random_ellipse(_p(a), n, n, int(target), g.dx, g.dy, g.lx, g.ly, 1 if kind == 0 else 0,
+    k = L.orc_local_random_ellipse(_p(a), cap, n, int(target), g.dx, g.dy, g.lx, g.ly, 1 if kind == 0 else 0,
                                    float(threshold), float(lambda_factor), float(dis_limit), int(scheme),
                                    int(leaf), _p(scratch))
-    return a[:k].copy()
+    if array_len is None:
+        return a[:k].copy()
+    # more rows than the array holds can only come from added (split) rows
+    return a[:k].copy(), (int(k * 1.1) if k > cap else cap)
 
 
 # ------------------------------------------------- fixed-point deposit

@@ -744,3 +744,114 @@ def example01_golden():
 
 if __name__ == "__main__" and "--example01" in sys.argv:
     example01_golden()
+
+
+# examples 02-05 as written, each with 1000 macro-particles over its first
+# 600 steps (the first bunch and the start of the decay): what differs from
+# example01 is the magnetic field, the management and the chamber
+EXAMPLES = {
+    "02": dict(grid=(32, 32, 0.04, 0.04, 1), type_b=1, bconst=(0., 0.1, 0.), management="global"),
+    "03": dict(grid=(32, 32, 0.04, 0.04, 1), type_b=0, management="local"),
+    "04": dict(grid=(32, 32, 0.04, 0.04, 1), type_b=2, multipole=(0., 5., 0., 0.01), management="local"),
+    "05": dict(grid=(44, 36, CC_LX, CC_LY, 3), type_b=0, management="global_over_1.2"),
+}
+EXAMPLE_RUN = dict(n_particles=1000, steps=600, load_seed=3, seed=11)
+
+
+def example_golden(name):
+    """exampleNN's loop as written (the managements: globalRandom every 50
+    steps outside +-5 % (02), localRandom with its kd-tree likewise (03,
+    04), globalRandom whenever the count reaches 1.2x (05); B: constant
+    (0, 0.1, 0) T (02), a quadrupole with an error from multipoleExpansion
+    gathered per particle (04); chamber: example05's cut-cell boundary from
+    its boundFunc) recorded like example01_golden; the grid arrays the
+    oracle needs for the 44x36 chamber are stored with it."""
+    grid, particles, particleBoundary, poissonSolver, randomGen = _import_reference()
+    import particleEmitter
+    import particleManagement
+    import magneticField
+    from beam import LHCBeam
+    spec, r = EXAMPLES[name], EXAMPLE_RUN
+    N = r["n_particles"]
+    nx, ny, lx, ly, bt = spec["grid"]
+    g = grid.Grid(nx, ny, lx, ly, bt, boundFunc=lhc_bound) if bt == 3 else grid.Grid(nx, ny, lx, ly, bt)
+    dt = 2.155172413795e-11
+    beam = LHCBeam(g, dt)
+    P = particles.Particles("electrons", "variableWeight")
+    bd = (particleBoundary.AbsorbArbitraryCutCell if bt == 3 else particleBoundary.AbsorbElliptical)(g, P)
+    em = particleEmitter.FurmanEmitter(bd, P)
+    ps = poissonSolver.PoissonSolver(g)
+    randomGen.seed(r["load_seed"])
+    particleEmitter.homoLoader(g, P, bd, N, 1.e9 / N)
+    b_nodes = None
+    if spec["type_b"] == 1:
+        P.setBConst(np.array(spec["bconst"]))
+    elif spec["type_b"] == 2:
+        b_nodes = np.asarray(magneticField.multipoleExpansion(g, list(spec["multipole"]))).copy()
+    out = {"pd0": np.asarray(P.getParticleData()).copy(), "params": np.array([nx, ny, lx, ly, bt], np.float64)}
+    profile = np.asarray(beam.getTransversalProfile()).copy()
+    randomGen.seed(r["seed"])
+    counts, lens, absorbed, managed, sums, beam_scale = [], [], [], [], [], []
+    for ii in range(r["steps"]):
+        n = P.getMacroParticleCount()
+        if spec["management"] == "global_over_1.2":
+            man = ii > 0 and n >= 1.2 * N
+        else:
+            man = ii > 0 and ii % 50 == 0 and (n > 1.05 * N or n < 0.95 * N)
+        if man and spec["management"] == "local":
+            particleManagement.localRandom(g, P, bd, N)
+        elif man:
+            particleManagement.globalRandom(g, P, N)
+        managed.append(int(man))
+        P.calcGridWeights(g)
+        P.chargeToGrid(g)
+        qb = beam.getCharge(ii * dt)
+        saved, beam.qTransversalProfile = beam.qTransversalProfile, np.float64(1.0)
+        scale = beam.getCharge(ii * dt)
+        beam.qTransversalProfile = saved
+        if np.isscalar(qb) and qb == 0:
+            beam_scale.append(np.nan)
+        else:
+            assert np.array_equal(float(scale) * profile, qb)
+            beam_scale.append(float(scale))
+        ps.solve(np.asarray(P.getChargeOnGrid()) + qb)
+        P.eFieldToParticles(g, ps.getEAtGridPoints())
+        if b_nodes is not None:
+            P.bFieldToParticles(g, b_nodes)
+        P.borisPush(dt, spec["type_b"])
+        bd.indexInside()
+        bd.saveAbsorbed()
+        na = bd.getAbsorbedMacroParticleCount()
+        absorbed.append(na)
+        if na > 0:
+            bd.calculateInteractionPoint()
+            bd.calculateNormalVectors()
+            P.addAndRemoveParticles(em.generateSecondaries(), P.getIsInside())
+        pd = np.asarray(P.getParticleData())
+        counts.append(pd.shape[0])
+        lens.append(np.asarray(P.getFullParticleData()).shape[0])
+        sums.append(loop_checksums(pd))
+    out.update({"profile": profile, "beam_scale": np.array(beam_scale), "counts": np.array(counts),
+                "array_len": np.array(lens), "absorbed": np.array(absorbed), "managed": np.array(managed),
+                "checksums": np.array(sums), "final": np.asarray(P.getParticleData()).copy(), "dt": np.array(dt),
+                "seed": np.array(r["seed"]), "target": np.array(N), "type_b": np.array(spec["type_b"]),
+                "bconst": np.array(spec.get("bconst", (0., 0., 0.))),
+                "management": np.array(spec["management"])})
+    if b_nodes is not None:
+        out["b_nodes"] = b_nodes
+    if bt == 3:
+        arrays = grid_arrays(g)
+        for k in ("insidePoints", "Dsi", "Dst", "insideFaces", "boundaryPoints", "cutCellPointsInd",
+                  "cutCellNormalVectors"):
+            out[k] = arrays[k]
+        e2n = g.getEdgeToNode().tocsc()
+        out["e2n_csc_indptr"], out["e2n_csc_indices"], out["e2n_csc_data"] = e2n.indptr, e2n.indices, e2n.data
+    path = os.path.join(HERE, f"example{name}_loop.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "final count", counts[-1], "absorbed", sum(absorbed),
+          "management events", sum(managed), "beam steps", int(np.isfinite(out["beam_scale"]).sum()))
+
+
+if __name__ == "__main__" and "--examples" in sys.argv:
+    for _name in EXAMPLES:
+        example_golden(_name)
