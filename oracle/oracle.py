@@ -332,6 +332,24 @@ def _manage_declared():
     return L
 
 
+def homo_loader(kind, lx, ly, n, w0, vsigma=10000. * 2.2250738585072014e-308, randomize=0, seed=None):
+    """homoLoader (particleEmitter.pyx:41-72) with the MT stream: n rows
+    uniform inside the rectangle (kind 0) or the ellipse (kind 1) of the
+    particle boundary, Gaussian velocities of deviation vsigma (the
+    reference's default: 1e4 times the smallest normal double), weight w0
+    (or w0 (0.5 + U) with randomize)."""
+    L = lib()
+    if not getattr(L, "_homo_declared", False):
+        L.orc_homo_loader.restype = None
+        L.orc_homo_loader.argtypes = [_I, _D, _D, _I64, _D, _D, _I, _P]
+        L._homo_declared = True
+    if seed is not None:
+        L.orc_seed(int(seed))
+    pd = np.zeros((int(n), 6))
+    L.orc_homo_loader(int(kind), float(lx), float(ly), int(n), float(w0), float(vsigma), int(randomize), _p(pd))
+    return pd
+
+
 def add_and_remove(pd, add, keep, array_len):
     """addAndRemoveParticles (particles.pyx:94-121, :201-269) on a particle
     array of `array_len` rows holding the rows of `pd`: returns the rows

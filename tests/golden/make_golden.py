@@ -735,7 +735,7 @@ def example01_golden():
     out = {"pd0": pd0, "profile": profile, "beam_scale": np.array(beam_scale), "counts": np.array(counts),
            "array_len": np.array(lens), "absorbed": np.array(absorbed), "managed": np.array(managed),
            "checksums": np.array(sums), "final": np.asarray(P.getParticleData()).copy(), "dt": np.array(dt),
-           "seed": np.array(r["seed"]), "target": np.array(N)}
+           "seed": np.array(r["seed"]), "target": np.array(N), "load_seed": np.array(r["load_seed"])}
     path = os.path.join(HERE, "example01_circle_32.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path), "final count", counts[-1], "absorbed", sum(absorbed),
@@ -835,6 +835,7 @@ def example_golden(name):
                 "array_len": np.array(lens), "absorbed": np.array(absorbed), "managed": np.array(managed),
                 "checksums": np.array(sums), "final": np.asarray(P.getParticleData()).copy(), "dt": np.array(dt),
                 "seed": np.array(r["seed"]), "target": np.array(N), "type_b": np.array(spec["type_b"]),
+                "load_seed": np.array(r["load_seed"]),
                 "bconst": np.array(spec.get("bconst", (0., 0., 0.))),
                 "management": np.array(spec["management"])})
     if b_nodes is not None:

@@ -77,6 +77,8 @@ def test_oracle_replays_example01():
     g = O.GridGeom(32, 32, 0.04, 0.04)
     f = O.furman("copper")
     target, dt = int(z["target"]), float(z["dt"])
+    # homoLoader's rows from the same MT seed
+    assert np.array_equal(O.homo_loader(1, 0.04, 0.04, target, 1.e9 / target, seed=int(z["load_seed"])), z["pd0"])
     pd = z["pd0"].copy()
     array_len = pd.shape[0]
     O.seed(int(z["seed"]))
@@ -129,6 +131,8 @@ def test_oracle_replays_examples(name):
     f = O.furman("copper")
     target, dt, type_b = int(z["target"]), float(z["dt"]), int(z["type_b"])
     management = str(z["management"])
+    if not cut:  # homoLoader's rows from the same MT seed (the oracle's loader has no cut-cell predicate)
+        assert np.array_equal(O.homo_loader(1, lx, ly, target, 1.e9 / target, seed=int(z["load_seed"])), z["pd0"])
     pd = z["pd0"].copy()
     array_len = pd.shape[0]
     worst = 0.0
